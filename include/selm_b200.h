@@ -1,0 +1,158 @@
+/*
+ * selm_b200.h - C ABI of libselm_b200.so, the B200-native SELM
+ * fluctuating-hydrodynamics step (monomers coupled to a periodic Stokes
+ * fluid through the Peskin 4-point kernel).
+ *
+ * The reference (yaohong99/monomers2026, data/src/selm-main/src/cuda) is an
+ * executable whose plugin surface is a C++ lifecycle:
+ *   Selm{initial, run, compute_f, final}            cuda/SELM.cuh:22-27
+ *   Eulerian{initial, compute_f, run, final}        cuda/SELM_Eulerian.cuh:23-27
+ *   Lagrangian{initial, compute_f, run, final}      cuda/SELM_Lagrangian.cuh:41-47
+ * with state shared through public pointers (d_u, d_f, dim, dx, d_x, d_v,
+ * d_f, d_m, lo, hi).  This header is that surface as plain C: an opaque
+ * handle, FP64 host buffers that are copied (never aliased), and int status
+ * codes instead of exit(-1) (cuda/check.cuh:6-10).
+ *
+ * Conventions: particles are AoS [M][3] doubles; grid fields are planar
+ * [3][Nz][Ny][Nx] doubles with n = (k*Ny + j)*Nx + i, exactly the
+ * reference's layout.  All calls return SELM_OK (0) on success; on failure
+ * selm_last_error() describes the most recent error of the calling thread.
+ */
+#ifndef SELM_B200_H
+#define SELM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SELM_OK 0
+#define SELM_ERR_INVALID 1   /* bad argument or size */
+#define SELM_ERR_CUDA 2      /* CUDA runtime error */
+#define SELM_ERR_STATE 3     /* call out of lifecycle order */
+#define SELM_ERR_NOMEM 4     /* device allocation failed or over budget */
+#define SELM_ERR_IO 5        /* input file missing or malformed */
+#define SELM_ERR_NUMERIC 6   /* the device error word is non-zero */
+
+/* form of the step */
+#define SELM_FORM_PLAIN64 0  /* reference structure, FP64 (drop-in) */
+#define SELM_FORM_FUSED64 1  /* spectral state, fused pencil FFT kernels, FP64 */
+#define SELM_FORM_FUSED32 2  /* same in FP32 with FP64 positions, zero mode and noise prefactor */
+
+#define SELM_INTEGRATOR_INERTIAL 0     /* reference scheme (cuda/SELM_Kernel.cu:155-195,302-373) */
+#define SELM_INTEGRATOR_QUASI_STEADY 1 /* overdamped: u = P f / (mu |k_h|^2), x += Gamma u dt */
+
+#define SELM_NOISE_REF_COMPAT 0 /* reference draw: x=0 and x=Nx/2 planes Hermitian-averaged by the c2r */
+#define SELM_NOISE_EXACT 1      /* Hermitian-correct draw: full variance on those planes */
+
+/* device error word bits (selm_status) */
+#define SELM_STATUS_NONFINITE 0x1u
+#define SELM_STATUS_DISPLACEMENT 0x2u /* |v dt| > L/2: the reference only prints (cuda/SELM_Kernel.cu:363) */
+#define SELM_STATUS_FENE_STRETCH 0x4u
+#define SELM_STATUS_FENE_BROKEN 0x8u
+
+/* Model.SELM keys (cuda/SELM.cu:17-48) plus the box and dt that the
+ * reference takes from LAMMPS (domain->boxlo/hi, update->dt). */
+typedef struct selm_params {
+  int num_mesh_pts[3];       /* numMeshPtsPerDir (all equal, as the reference assumes) */
+  double box_lo, box_hi;     /* cubic periodic box; dx = (hi - lo)/Nx */
+  double rho, mu, KB, T, dt; /* rho mu KB T, timestep */
+  int flag_stochastic;       /* flagStochasticDriving */
+  unsigned long long seed;   /* SELM_Seed */
+  int form;                  /* SELM_FORM_* */
+  int integrator;            /* SELM_INTEGRATOR_* */
+  int noise_mode;            /* SELM_NOISE_* */
+} selm_params;
+
+/* Force field of the LAMMPS-script subset the inputs use
+ * (bond_style harmonic|fene, angle_style harmonic, pair_style lj/cut,
+ * special_bonds lj weights, a uniform body force). Atom indices 0-based,
+ * types 1-based as in LAMMPS data files. */
+#define SELM_BOND_NONE 0
+#define SELM_BOND_HARMONIC 1 /* coeff per type: K r0            (E = K (r-r0)^2) */
+#define SELM_BOND_FENE 2     /* coeff per type: K R0 eps sigma  (LAMMPS bond_style fene) */
+#define SELM_ANGLE_NONE 0
+#define SELM_ANGLE_HARMONIC 1 /* coeff per type: K theta0(deg) (E = K (theta-theta0)^2) */
+#define SELM_PAIR_NONE 0
+#define SELM_PAIR_LJCUT 1 /* coeff per type pair (i,j) at (i*(ntypes+1)+j)*3: eps sigma rc */
+
+typedef struct selm_topology {
+  int natoms, ntypes;
+  const int* type;            /* [natoms] */
+  int nbonds, bond_style, nbondtypes;
+  const int* bonds;           /* [nbonds][3] = type, i, j */
+  const double* bond_coeff;   /* [(nbondtypes+1)][4] */
+  int nangles, angle_style, nangletypes;
+  const int* angles;          /* [nangles][4] = type, i, j(center), k */
+  const double* angle_coeff;  /* [(nangletypes+1)][2] */
+  int pair_style;
+  const double* pair_coeff;   /* [(ntypes+1)^2][3] */
+  double special_lj[3];       /* 1-2, 1-3, 1-4 weights (LAMMPS default 0 0 0) */
+  double body_force[3];
+} selm_topology;
+
+typedef struct selm_sim selm_sim;
+
+/* Host force provider, the role LAMMPS plays in the reference
+ * (Lagrangian_LAMMPS::compute_f, cuda/SELM_Lagrangian_LAMMPS.cu:107-130):
+ * called once per step with the new positions/velocities; writes f. */
+typedef int (*selm_force_fn)(void* user, int natoms, const double* x, const double* v, double* f);
+
+/* ---- lifecycle (Selm::Selm / initial / run / final) ---- */
+/* replaces Selm::Selm() + Eulerian_Period::initial allocations (cuda/SELM.cu:17-48,
+ * cuda/SELM_Eulerian_Period.cu:14-76) */
+int selm_create(const selm_params* params, selm_sim** out);
+/* replaces Selm::Selm() reading Model.SELM + LAMMPS script/data from a case
+ * directory (cuda/SELM.cu:20, cuda/SELM_Lagrangian_LAMMPS.cu:21-28) */
+int selm_create_from_files(const char* case_dir, selm_sim** out);
+/* monomer state: replaces Lagrangian_LAMMPS::initial uploads (cuda/SELM_Lagrangian_LAMMPS.cu:71-93) */
+int selm_set_particles(selm_sim* s, int natoms, const double* x, const double* v, const double* mass);
+/* device force field (replaces the per-step LAMMPS round trip) */
+int selm_set_topology(selm_sim* s, const selm_topology* topo);
+/* host force provider instead of the device force field */
+int selm_set_force_callback(selm_sim* s, selm_force_fn fn, void* user);
+/* Selm::initial (cuda/SELM.cu:55-58): initial forces, u = 0, first noise */
+int selm_initial(selm_sim* s);
+/* nsteps iterations of the body of Selm::run (cuda/SELM.cu:73-90) */
+int selm_step(selm_sim* s, int nsteps);
+/* Selm::final + destructor (cuda/SELM.cu:50-63) */
+int selm_destroy(selm_sim* s);
+
+/* ---- state access (the reference's public pointers, copied) ---- */
+int selm_get_particles(selm_sim* s, double* x, double* v, double* f); /* any may be NULL */
+#define SELM_FIELD_U 0 /* Eulerian::d_u[cur_u] */
+#define SELM_FIELD_F 1 /* Eulerian::d_f (forcing for the next fluid update) */
+int selm_get_field(selm_sim* s, int which, double* out);       /* [3][Nz][Ny][Nx] */
+int selm_set_field(selm_sim* s, int which, const double* in);
+int selm_get_info(selm_sim* s, int* natoms, int dims[3], unsigned long long* step);
+int selm_status(selm_sim* s, unsigned int* error_word);
+
+/* ---- streams and timing ---- */
+int selm_set_stream(selm_sim* s, void* cuda_stream); /* NULL = library-owned stream */
+void* selm_get_stream(selm_sim* s);
+int selm_synchronize(selm_sim* s);
+/* per-kernel CUDA-event timing on the library stream */
+int selm_profile_enable(selm_sim* s, int enable);
+int selm_profile_read(selm_sim* s, const char* kernel, double* total_ms, long* launches);
+
+/* ---- operator entry points on host buffers (unit-level parity) ---- */
+/* gamma(): cuda/SELM_Kernel.cu:375-422 with the staggering of :328-338 */
+int selm_op_interp(int precision, const int dims[3], double lo, double dx, const double* u, int natoms,
+                   const double* x, double* out);
+/* lambda(): cuda/SELM_Kernel.cu:424-470; fgrid -= Lambda(tf) */
+int selm_op_spread(int precision, const int dims[3], double lo, double dx, double* fgrid, int natoms,
+                   const double* x, const double* tf);
+/* cufftExecD2Z / cufftExecZ2D (cuda/SELM_Eulerian_Period.cu:113,117), unnormalised;
+ * precision 64 or 32; half spectrum as interleaved complex doubles */
+int selm_op_fft3_r2c(int precision, const int dims[3], const double* in, double* out);
+int selm_op_fft3_c2r(int precision, const int dims[3], const double* in, double* out);
+
+/* ---- errors ---- */
+const char* selm_last_error(void);
+const char* selm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SELM_B200_H */

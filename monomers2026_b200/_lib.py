@@ -1,0 +1,102 @@
+"""ctypes binding of libselm_b200.so (the C ABI declared in include/selm_b200.h).
+
+The library is built in-tree (``monomers2026_b200/lib/``).  There is no
+fallback: if the shared object is missing, importing the binding raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libselm_b200.so")
+
+# symbols declared in include/selm_b200.h (checked by the CPU test suite)
+EXPORTED = [
+    "selm_create", "selm_create_from_files", "selm_set_particles", "selm_set_topology",
+    "selm_set_force_callback", "selm_initial", "selm_step", "selm_destroy", "selm_get_particles",
+    "selm_get_field", "selm_set_field", "selm_get_info", "selm_status", "selm_set_stream",
+    "selm_get_stream", "selm_synchronize", "selm_profile_enable", "selm_profile_read",
+    "selm_op_interp", "selm_op_spread", "selm_op_fft3_r2c", "selm_op_fft3_c2r", "selm_last_error",
+    "selm_version",
+]
+
+SELM_OK = 0
+
+
+class SelmParams(C.Structure):
+    _fields_ = [
+        ("num_mesh_pts", C.c_int * 3),
+        ("box_lo", C.c_double), ("box_hi", C.c_double),
+        ("rho", C.c_double), ("mu", C.c_double), ("KB", C.c_double), ("T", C.c_double), ("dt", C.c_double),
+        ("flag_stochastic", C.c_int),
+        ("seed", C.c_ulonglong),
+        ("form", C.c_int), ("integrator", C.c_int), ("noise_mode", C.c_int),
+    ]
+
+
+class SelmTopology(C.Structure):
+    _fields_ = [
+        ("natoms", C.c_int), ("ntypes", C.c_int), ("type", C.c_void_p),
+        ("nbonds", C.c_int), ("bond_style", C.c_int), ("nbondtypes", C.c_int),
+        ("bonds", C.c_void_p), ("bond_coeff", C.c_void_p),
+        ("nangles", C.c_int), ("angle_style", C.c_int), ("nangletypes", C.c_int),
+        ("angles", C.c_void_p), ("angle_coeff", C.c_void_p),
+        ("pair_style", C.c_int), ("pair_coeff", C.c_void_p),
+        ("special_lj", C.c_double * 3), ("body_force", C.c_double * 3),
+    ]
+
+
+FORCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                       C.POINTER(C.c_double))
+
+_lib = None
+
+
+def load():
+    """Load libselm_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libselm_b200.so not built ({LIB_PATH}); run monomers2026_b200.build.build()")
+    L = C.CDLL(LIB_PATH)
+    vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)
+    L.selm_create.argtypes = [C.POINTER(SelmParams), C.POINTER(vp)]
+    L.selm_create_from_files.argtypes = [C.c_char_p, C.POINTER(vp)]
+    L.selm_set_particles.argtypes = [vp, C.c_int, dp, dp, dp]
+    L.selm_set_topology.argtypes = [vp, C.POINTER(SelmTopology)]
+    L.selm_set_force_callback.argtypes = [vp, FORCE_FN, vp]
+    L.selm_initial.argtypes = [vp]
+    L.selm_step.argtypes = [vp, C.c_int]
+    L.selm_destroy.argtypes = [vp]
+    L.selm_get_particles.argtypes = [vp, dp, dp, dp]
+    L.selm_get_field.argtypes = [vp, C.c_int, dp]
+    L.selm_set_field.argtypes = [vp, C.c_int, dp]
+    L.selm_get_info.argtypes = [vp, ip, ip, C.POINTER(C.c_ulonglong)]
+    L.selm_status.argtypes = [vp, C.POINTER(C.c_uint)]
+    L.selm_set_stream.argtypes = [vp, vp]
+    L.selm_get_stream.argtypes = [vp]
+    L.selm_get_stream.restype = vp
+    L.selm_synchronize.argtypes = [vp]
+    L.selm_profile_enable.argtypes = [vp, C.c_int]
+    L.selm_profile_read.argtypes = [vp, C.c_char_p, dp, C.POINTER(C.c_long)]
+    L.selm_op_interp.argtypes = [C.c_int, ip, C.c_double, C.c_double, dp, C.c_int, dp, dp]
+    L.selm_op_spread.argtypes = [C.c_int, ip, C.c_double, C.c_double, dp, C.c_int, dp, dp]
+    L.selm_op_fft3_r2c.argtypes = [C.c_int, ip, dp, dp]
+    L.selm_op_fft3_c2r.argtypes = [C.c_int, ip, dp, dp]
+    L.selm_last_error.restype = C.c_char_p
+    L.selm_version.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+class SelmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"selm error {code}: {msg}")
+        self.code = code
+
+
+def check(rc: int) -> None:
+    if rc != SELM_OK:
+        raise SelmError(rc, load().selm_last_error().decode(errors="replace"))

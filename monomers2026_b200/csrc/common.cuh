@@ -1,0 +1,194 @@
+// common.cuh - device helpers shared by every SELM kernel (sm_100a).
+//
+// Philox4x32-10 is the published counter-based generator of Salmon, Moraes,
+// Dror and Shaw (SC'11).  Counter layout (one call per use):
+//   fluid noise   : {mode q, component d (0..2), step lo, step hi}
+//   monomer noise : {monomer p, 4 + component d, step lo, step hi}
+//   key           : {seed lo, seed hi}
+// Normals are Box-Muller pairs of two 52-bit open-interval uniforms, so the
+// draws are a pure function of (seed, step, index) and do not depend on the
+// launch shape, the batch a job runs in, or the number of jobs.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace selm {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// error word bits (per job, device resident, read back by the host)
+enum : uint32_t {
+  ERR_NONFINITE = 1u << 0,        // NaN/Inf in a monomer state
+  ERR_DISPLACEMENT = 1u << 1,     // |v dt| > L/2 (reference warns, cuda/SELM_Kernel.cu:363)
+  ERR_FENE_STRETCH = 1u << 2,     // FENE bond past 0.9 R0^2, clamped
+  ERR_FENE_BROKEN = 1u << 3,      // FENE bond past the LAMMPS error limit
+  ERR_BUCKET_OVERFLOW = 1u << 4,  // candidate list longer than the kernel bound
+};
+
+template <typename T> struct cpx_t;
+template <> struct cpx_t<float> { using type = float2; };
+template <> struct cpx_t<double> { using type = double2; };
+template <typename T> using cpx = typename cpx_t<T>::type;
+
+template <typename C> __device__ __forceinline__ C cmk(decltype(C::x) a, decltype(C::x) b) {
+  C c; c.x = a; c.y = b; return c;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return cmk<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return cmk<C>(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  return cmk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return cmk<C>(a.x * s, a.y * s); }
+
+// ---------------------------------------------------------------- Philox
+__host__ __device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                       uint32_t k0, uint32_t k1, uint32_t out[4]) {
+#ifdef __CUDA_ARCH__
+#pragma unroll
+#endif
+  for (int r = 0; r < 10; r++) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    c0 = hi1 ^ c1 ^ k0;
+    c1 = lo1;
+    c2 = hi0 ^ c3 ^ k1;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+__device__ __forceinline__ double u01_52(uint32_t a, uint32_t b) {
+  const uint64_t x = ((((uint64_t)a) << 32) | b) >> 12;
+  return ((double)x + 0.5) * (1.0 / 4503599627370496.0);
+}
+
+// Box-Muller pair from one Philox block
+__device__ __forceinline__ void philox_normal2(uint64_t seed, uint32_t c0, uint32_t c1, uint64_t step,
+                                               double& z0, double& z1) {
+  uint32_t o[4];
+  philox4x32_10(c0, c1, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)seed, (uint32_t)(seed >> 32), o);
+  const double u1 = u01_52(o[0], o[1]), u2 = u01_52(o[2], o[3]);
+  const double r = sqrt(-2.0 * log(u1));
+  double s, c;
+  sincos(2.0 * kPi * u2, &s, &c);
+  z0 = r * c;
+  z1 = r * s;
+}
+
+// ---------------------------------------------------------------- Peskin
+// phi(r) of cuda/SELM_Kernel.cu:391-395 for r = |distance| (grid units)
+template <typename T> __device__ __forceinline__ T peskin4(T r) {
+  if (r < T(1)) return (T(3) - T(2) * r + sqrt(T(1) + T(4) * r * (T(1) - r))) / T(8);
+  if (r < T(2)) return (T(5) - T(2) * r - sqrt(T(-7) + T(4) * r * (T(3) - r))) / T(8);
+  return T(0);
+}
+
+__device__ __forceinline__ int wrapi(int p, int n) {
+  p %= n;
+  return p < 0 ? p + n : p;
+}
+
+// ---------------------------------------------------------------- FFT plans
+// Radix schedule of a line FFT (same factorisation order as the oracle:
+// 4 first, then 2, 3, 5, 7, larger odd primes).
+struct FftRadix {
+  int n;
+  int nstage;
+  int radix[12];
+};
+
+inline FftRadix make_radix(int n) {
+  FftRadix r{};
+  r.n = n;
+  int m = n, ns = 0;
+  while (m > 1 && ns < 12) {
+    int p;
+    if (m % 4 == 0) p = 4;
+    else if (m % 2 == 0) p = 2;
+    else if (m % 3 == 0) p = 3;
+    else if (m % 5 == 0) p = 5;
+    else { p = 7; while (m % p) p += 2; }
+    r.radix[ns++] = p;
+    m /= p;
+  }
+  r.nstage = ns;
+  return r;
+}
+
+// One Stockham decimation-in-time stage for many lines held in shared memory.
+// Element t of line b lives at  b*sb + t*st  (sb, st in elements).
+//   Y[k][q + Ls v] = sum_s w_p^{s v} ( w_L^{s q} Y*[k + s r][q] )
+// Y* (input) at  q*rs + k  ,  Y (output) at  q*r + k ,  L = p*Ls, r = n/L.
+// w[t] = exp(sign*2*pi*i*t/n) for t < n.
+template <typename C>
+__device__ __forceinline__ void stockham_stage(const C* __restrict__ a, C* __restrict__ b, const C* __restrict__ w,
+                                               int n, int p, int Ls, int nlines, int sb, int st, bool line_fast,
+                                               int sign, int tid, int nthr) {
+  using T = decltype(C::x);
+  const int L = Ls * p, r = n / L, rs = n / Ls;
+  const int nbf = nlines * r * Ls;  // butterflies
+  for (int it = tid; it < nbf; it += nthr) {
+    int line, k, q;
+    if (line_fast) {
+      line = it % nlines;
+      const int rest = it / nlines;
+      k = rest % r;
+      q = rest / r;
+    } else {
+      k = it % r;
+      const int rest = it / r;
+      q = rest % Ls;
+      line = rest / Ls;
+    }
+    const C* ai = a + line * sb;
+    C* bo = b + line * sb;
+    C c[8];
+#pragma unroll 1
+    for (int s = 0; s < p; s++) {
+      C y = ai[(q * rs + k + s * r) * st];
+      c[s] = (s == 0 || q == 0) ? y : cmul(y, w[s * q * r]);
+    }
+    if (p == 4) {
+      const C s02p = cadd(c[0], c[2]), s02m = csub(c[0], c[2]);
+      const C s13p = cadd(c[1], c[3]), s13m = csub(c[1], c[3]);
+      const C js = cmk<C>(-T(sign) * s13m.y, T(sign) * s13m.x);
+      bo[(q * r + k) * st] = cadd(s02p, s13p);
+      bo[((q + Ls) * r + k) * st] = cadd(s02m, js);
+      bo[((q + 2 * Ls) * r + k) * st] = csub(s02p, s13p);
+      bo[((q + 3 * Ls) * r + k) * st] = csub(s02m, js);
+    } else if (p == 2) {
+      bo[(q * r + k) * st] = cadd(c[0], c[1]);
+      bo[((q + Ls) * r + k) * st] = csub(c[0], c[1]);
+    } else {
+      const int np = n / p;
+      for (int v = 0; v < p; v++) {
+        C acc = c[0];
+        for (int s = 1; s < p; s++) acc = cadd(acc, cmul(c[s], w[((s * v) % p) * np]));
+        bo[((q + v * Ls) * r + k) * st] = acc;
+      }
+    }
+  }
+}
+
+// Full line FFT over all stages; ping-pongs between bufA and bufB and returns
+// the buffer that holds the result.  Caller synchronises before the call.
+template <typename C>
+__device__ C* line_fft(C* bufA, C* bufB, const C* w, const FftRadix& R, int nlines, int sb, int st,
+                       bool line_fast, int sign) {
+  C* a = bufA;
+  C* b = bufB;
+  int Ls = 1;
+  for (int s = 0; s < R.nstage; s++) {
+    stockham_stage(a, b, w, R.n, R.radix[s], Ls, nlines, sb, st, line_fast, sign, threadIdx.x, blockDim.x);
+    __syncthreads();
+    C* t = a; a = b; b = t;
+    Ls *= R.radix[s];
+  }
+  return a;
+}
+
+}  // namespace selm

@@ -1,0 +1,461 @@
+// coupling.cu - monomer <-> grid coupling on sm_100a.
+//
+//  * bin_particles  : counting sort of monomers into buckets (grid tiles for
+//                     the coupling, force cells for the pair list).  Bucket
+//                     contents are ordered by monomer index, so every later
+//                     traversal has a fixed order.
+//  * interp_update  : Peskin 4-point interpolation of the staggered velocity
+//                     (gamma(), cuda/SELM_Kernel.cu:375-422) fused with the
+//                     drag/noise impulse and the explicit monomer update of
+//                     lagrangian_update() (cuda/SELM_Kernel.cu:302-373).
+//  * spread_gather  : the spreading lambda() (cuda/SELM_Kernel.cu:424-470)
+//                     written as a gather: one block per 8x8x8 tile stages the
+//                     monomers whose stencils reach the tile (from the 27
+//                     neighbouring buckets) in shared memory, and every grid
+//                     value is summed by one thread in a fixed order.  No
+//                     floating-point atomics; results do not depend on
+//                     scheduling.
+#include "common.cuh"
+#include "selm_kernels.h"
+
+namespace selm {
+
+// ================================================================ binning
+__device__ __forceinline__ int axis_bucket(double x, int a, const BinSpec& bs) {
+  int c;
+  if (bs.mode == 0) {
+    c = (int)floor((x - bs.lo) / bs.dx);
+    c = wrapi(c, bs.n[a]);
+    return c / bs.tile[a];
+  }
+  c = (int)floor((x - bs.lo) / bs.L * bs.n[a]);
+  return wrapi(c, bs.n[a]);
+}
+
+__global__ void k_bin_count(const double* __restrict__ x, int M, BinSpec bs, int* __restrict__ bucket_of,
+                            int* __restrict__ counts) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= M) return;
+  int b3[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double xa = x[3 * p + a];
+    b3[a] = isfinite(xa) ? axis_bucket(xa, a, bs) : 0;
+  }
+  const int b = (b3[2] * bs.nb[1] + b3[1]) * bs.nb[0] + b3[0];
+  bucket_of[p] = b;
+  atomicAdd(&counts[b], 1);
+}
+
+__global__ void k_bin_scatter(const int* __restrict__ bucket_of, int M, int* __restrict__ cursor,
+                              int* __restrict__ unsorted) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= M) return;
+  const int pos = atomicAdd(&cursor[bucket_of[p]], 1);
+  unsorted[pos] = p;
+}
+
+// One warp per bucket: rank of every member by monomer index.
+__global__ void k_bucket_sort(const int* __restrict__ offsets, int nbuckets, const int* __restrict__ unsorted,
+                              int* __restrict__ sorted) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= nbuckets) return;
+  const int s = offsets[warp], e = offsets[warp + 1];
+  const int n = e - s;
+  for (int i = lane; i < n; i += 32) {
+    const int id = unsorted[s + i];
+    int rank = 0;
+    for (int j = 0; j < n; j++) rank += (unsorted[s + j] < id);
+    sorted[s + rank] = id;
+  }
+}
+
+// ---- exclusive scan over n ints (two levels of 4096-element blocks)
+constexpr int kScanThreads = 1024, kScanIpt = 4, kScanBlock = kScanThreads * kScanIpt;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* sh_warp, int& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) sh_warp[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int w = (lane < (int)(blockDim.x >> 5)) ? sh_warp[lane] : 0;
+    int wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    sh_warp[lane] = wi - w;  // exclusive warp offsets
+    if (lane == 31) sh_warp[32] = wi;
+  }
+  __syncthreads();
+  total = sh_warp[32];
+  const int r = sh_warp[wid] + incl - v;
+  __syncthreads();
+  return r;
+}
+
+__global__ void k_scan_block(const int* __restrict__ in, int* __restrict__ out, long n, int* __restrict__ bsum) {
+  __shared__ int sh[33];
+  const long base = (long)blockIdx.x * kScanBlock + (long)threadIdx.x * kScanIpt;
+  int v[kScanIpt];
+  int s = 0;
+#pragma unroll
+  for (int q = 0; q < kScanIpt; q++) {
+    v[q] = (base + q < n) ? in[base + q] : 0;
+    s += v[q];
+  }
+  int total;
+  int run = block_exclusive_scan(s, sh, total);
+#pragma unroll
+  for (int q = 0; q < kScanIpt; q++) {
+    if (base + q < n) out[base + q] = run;
+    run += v[q];
+  }
+  if (threadIdx.x == 0 && bsum) bsum[blockIdx.x] = total;
+}
+
+__global__ void k_scan_add(int* __restrict__ out, long n, const int* __restrict__ boff) {
+  const long base = (long)blockIdx.x * kScanBlock;
+  const int add = boff[blockIdx.x];
+  for (int t = threadIdx.x; t < kScanBlock; t += blockDim.x)
+    if (base + t < n) out[base + t] += add;
+}
+
+long scan_tmp_size(long n) {
+  const long nb = (n + kScanBlock - 1) / kScanBlock;
+  return 2 * nb + 2;
+}
+
+static cudaError_t exclusive_scan(const int* in, int* out, long n, int* tmp, cudaStream_t st) {
+  const long nb = (n + kScanBlock - 1) / kScanBlock;
+  if (nb > kScanBlock) return cudaErrorInvalidValue;
+  if (nb == 1) {
+    k_scan_block<<<1, kScanThreads, 0, st>>>(in, out, n, nullptr);
+    return cudaGetLastError();
+  }
+  int* bsum = tmp;
+  int* boff = tmp + nb;
+  k_scan_block<<<(unsigned)nb, kScanThreads, 0, st>>>(in, out, n, bsum);
+  k_scan_block<<<1, kScanThreads, 0, st>>>(bsum, boff, nb, nullptr);
+  k_scan_add<<<(unsigned)nb, 256, 0, st>>>(out, n, boff);
+  return cudaGetLastError();
+}
+
+cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBuffers& bb, cudaStream_t st) {
+  const long nbk = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
+  cudaError_t e = cudaMemsetAsync(bb.counts, 0, sizeof(int) * (nbk + 1), st);
+  if (e != cudaSuccess) return e;
+  if (M > 0) k_bin_count<<<(M + 255) / 256, 256, 0, st>>>(x, M, bs, bb.bucket_of, bb.counts);
+  if ((e = exclusive_scan(bb.counts, bb.offsets, nbk + 1, bb.scan_tmp, st)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(bb.cursor, bb.offsets, sizeof(int) * nbk, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+    return e;
+  if (M > 0) {
+    k_bin_scatter<<<(M + 255) / 256, 256, 0, st>>>(bb.bucket_of, M, bb.cursor, bb.unsorted);
+    k_bucket_sort<<<(unsigned)((nbk * 32 + 255) / 256), 256, 0, st>>>(bb.offsets, (int)nbk, bb.unsorted, bb.sorted);
+  }
+  return cudaGetLastError();
+}
+
+// ================================================================ Peskin weights
+// Weight factor of the reference's loop nest for a distance r (grid units):
+// the branches of cuda/SELM_Kernel.cu:391-395; a distance of exactly 2 (a
+// coordinate on a grid node) leaves the factor at 1.0 there, which is kept.
+// The branch is taken on the FP64 distance so that the FP32 form never rounds
+// a distance just below 2 onto the edge case.
+template <typename T> __device__ __forceinline__ T ref_weight(double rd) {
+  const T r = (T)rd;
+  if (rd < 1.0) return (T(3) - T(2) * r + sqrt(T(1) + T(4) * r * (T(1) - r))) / T(8);
+  if (rd < 2.0) return (T(5) - T(2) * r - sqrt(T(-7) + T(4) * r * (T(3) - r))) / T(8);
+  return T(1);
+}
+
+// gamma() of cuda/SELM_Kernel.cu:375-422 (same loop and product order)
+template <typename T>
+__device__ __forceinline__ T interp_one(double rx, double ry, double rz, int Nx, int Ny, int Nz,
+                                        const T* __restrict__ u) {
+  const int p0 = (int)floor(rx) - 1, p1 = (int)floor(ry) - 1, p2 = (int)floor(rz) - 1;
+  T wx[4], wy[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    wx[i] = ref_weight<T>(fabs(rx - (double)(p0 + i)));
+    wy[i] = ref_weight<T>(fabs(ry - (double)(p1 + i)));
+  }
+  int ix[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) ix[i] = wrapi(p0 + i, Nx);
+  T rv = T(0);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const T dk = T(1) * ref_weight<T>(fabs(rz - (double)(p2 + k)));
+    const long zoff = (long)wrapi(p2 + k, Nz) * Ny;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const T dj = dk * wy[j];
+      const T* row = u + (zoff + wrapi(p1 + j, Ny)) * Nx;
+#pragma unroll
+      for (int i = 0; i < 4; i++) rv += __ldg(row + ix[i]) * (dj * wx[i]);
+    }
+  }
+  return rv;
+}
+
+// lagrangian_update() of cuda/SELM_Kernel.cu:302-373, one thread per
+// (monomer, component); the spread part lives in k_spread_gather.
+template <typename T>
+__global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, const double* __restrict__ x_old,
+                                                       double* __restrict__ x_new, double* __restrict__ v,
+                                                       double* __restrict__ f, const double* __restrict__ m,
+                                                       double* __restrict__ tf_out, const int* __restrict__ order,
+                                                       CouplingArgs a, uint32_t* __restrict__ err) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 3L * a.M) return;
+  const int s = (int)(gid / 3), d = (int)(gid % 3);
+  const int p = order ? order[s] : s;
+  const long g = 3L * p + d;
+  const long N = (long)a.nx * a.ny * a.nz;
+  const double gx = (x_old[3L * p] - a.lo) / a.dx, gy = (x_old[3L * p + 1] - a.lo) / a.dx,
+               gz = (x_old[3L * p + 2] - a.lo) / a.dx;
+  T val;
+  if (d == 0) val = interp_one<T>(gx, gy - 0.5, gz - 0.5, a.nx, a.ny, a.nz, u);
+  else if (d == 1) val = interp_one<T>(gx - 0.5, gy, gz - 0.5, a.nx, a.ny, a.nz, u + N);
+  else val = interp_one<T>(gx - 0.5, gy - 0.5, gz, a.nx, a.ny, a.nz, u + 2 * N);
+  const double vg = v[g];
+  double t_f = -a.upsilon * (vg - (double)val) * a.dt;
+  if (a.stochastic) {
+    double z0, z1;
+    philox_normal2(a.seed, (uint32_t)p, 4u + (uint32_t)d, a.step, z0, z1);
+    t_f += z0 * a.coef;
+  }
+  tf_out[g] = t_f;
+  t_f += a.dt * f[g];
+  f[g] = t_f / a.dt;
+  const double tmp = vg * a.dt;
+  const double L = a.hi - a.lo;
+  if (fabs(tmp) > L / 2) atomicOr(err, ERR_DISPLACEMENT);
+  double tx = x_old[g] + tmp;
+  if (tx > a.hi) tx -= L;
+  else if (tx < a.lo) tx += L;
+  x_new[g] = tx;
+  const double vn = vg + t_f / m[p];
+  v[g] = vn;
+  if (!isfinite(vn) || !isfinite(tx)) atomicOr(err, ERR_NONFINITE);
+}
+
+// Pure interpolation (operator entry point): out[p][d] = Gamma_d u (x_p)
+template <typename T>
+__global__ void k_interp_only(const T* __restrict__ u, const double* __restrict__ x, int M, int nx, int ny, int nz,
+                              double lo, double dx, double* __restrict__ out) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 3L * M) return;
+  const int p = (int)(gid / 3), d = (int)(gid % 3);
+  const long N = (long)nx * ny * nz;
+  const double gx = (x[3L * p] - lo) / dx, gy = (x[3L * p + 1] - lo) / dx, gz = (x[3L * p + 2] - lo) / dx;
+  T val;
+  if (d == 0) val = interp_one<T>(gx, gy - 0.5, gz - 0.5, nx, ny, nz, u);
+  else if (d == 1) val = interp_one<T>(gx - 0.5, gy, gz - 0.5, nx, ny, nz, u + N);
+  else val = interp_one<T>(gx - 0.5, gy - 0.5, gz, nx, ny, nz, u + 2 * N);
+  out[gid] = (double)val;
+}
+
+template <typename T>
+cudaError_t interp_only(const T* u, const double* x, int M, int nx, int ny, int nz, double lo, double dx, double* out,
+                        cudaStream_t st) {
+  if (M <= 0) return cudaSuccess;
+  k_interp_only<T><<<(unsigned)((3L * M + 255) / 256), 256, 0, st>>>(u, x, M, nx, ny, nz, lo, dx, out);
+  return cudaGetLastError();
+}
+template cudaError_t interp_only<double>(const double*, const double*, int, int, int, int, double, double, double*,
+                                         cudaStream_t);
+template cudaError_t interp_only<float>(const float*, const double*, int, int, int, int, double, double, double*,
+                                        cudaStream_t);
+
+template <typename T>
+cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double* v, double* f, const double* m,
+                          double* tf, const int* order, const CouplingArgs& a, uint32_t* err, cudaStream_t st) {
+  if (a.M <= 0) return cudaSuccess;
+  const long nt = 3L * a.M;
+  k_interp_update<T><<<(unsigned)((nt + 383) / 384), 384, 0, st>>>(u, x_old, x_new, v, f, m, tf, order, a, err);
+  return cudaGetLastError();
+}
+
+// ================================================================ spread (gather)
+constexpr int kTile = 8;
+constexpr int kSpreadThreads = 3 * kTile * kTile;  // one thread per (component, y row, z row)
+constexpr int kSpreadCap = 256;                    // staged candidates per accumulation round
+
+template <typename T> struct SpreadCand {
+  int rb[3][2];     // base of the 4-point stencil relative to the tile, wrapped: [axis][unshifted, shifted]
+  T w[3][2][4];     // weight factors [axis][unshifted, shifted][point]
+  T tf[3];          // impulse per component
+};
+
+template <typename T>
+__device__ __forceinline__ void spread_accumulate(const SpreadCand<T>* __restrict__ cand, int ncand, int d, int ry,
+                                                  int rz, int nx, int ny, int nz, T (&acc)[kTile]) {
+  const int sx = (d == 0) ? 0 : 1, sy = (d == 1) ? 0 : 1, sz = (d == 2) ? 0 : 1;
+  for (int c = 0; c < ncand; c++) {
+    const SpreadCand<T>& C = cand[c];
+    int kz0 = rz - C.rb[2][sz];
+    if (kz0 < 0) kz0 += nz;
+    if (kz0 >= 4) continue;
+    int jy0 = ry - C.rb[1][sy];
+    if (jy0 < 0) jy0 += ny;
+    if (jy0 >= 4) continue;
+    const T tfd = C.tf[d];
+    const int rbx = C.rb[0][sx];
+    for (int kz = kz0; kz < 4; kz += nz) {
+      const T dk = T(1) * C.w[2][sz][kz];
+      for (int jy = jy0; jy < 4; jy += ny) {
+        const T dj = dk * C.w[1][sy][jy];
+#pragma unroll
+        for (int cx = 0; cx < kTile; cx++) {
+          int ix = cx - rbx;
+          if (ix < 0) ix += nx;
+          for (; ix < 4; ix += nx) acc[cx] -= tfd * (dj * C.w[0][sx][ix]);
+        }
+      }
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSpreadThreads) k_spread_gather(T* __restrict__ fgrid, int accumulate,
+                                                                  const double* __restrict__ x_old,
+                                                                  const double* __restrict__ tf, BinSpec bs,
+                                                                  const int* __restrict__ offsets,
+                                                                  const int* __restrict__ sorted, CouplingArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SpreadCand<T>* cand = reinterpret_cast<SpreadCand<T>*>(smem_raw);
+  __shared__ int wtot[kSpreadThreads / 32];
+  __shared__ int s_ncand;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int tb = blockIdx.x;
+  const int tbx = tb % bs.nb[0], tby = (tb / bs.nb[0]) % bs.nb[1], tbz = tb / (bs.nb[0] * bs.nb[1]);
+  const int t0[3] = {tbx * kTile, tby * kTile, tbz * kTile};
+  const int ext[3] = {min(kTile, nx - t0[0]), min(kTile, ny - t0[1]), min(kTile, nz - t0[2])};
+  const int nn[3] = {nx, ny, nz};
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int d = tid / (kTile * kTile), r = tid % (kTile * kTile), ry = r % kTile, rz = r / kTile;
+  const long N = (long)nx * ny * nz;
+  const bool row_ok = (ry < ext[1]) && (rz < ext[2]);
+  T* row = fgrid + d * N + ((long)(t0[2] + rz) * ny + (t0[1] + ry)) * nx + t0[0];
+  T acc[kTile];
+#pragma unroll
+  for (int cx = 0; cx < kTile; cx++) acc[cx] = (accumulate && row_ok && cx < ext[0]) ? row[cx] : T(0);
+  if (tid == 0) s_ncand = 0;
+  __syncthreads();
+  // distinct neighbouring buckets along each axis (fewer than 3 on tiny grids)
+  int noff[3], offs[3][3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ax++) {
+    const int nb = bs.nb[ax];
+    const int tcur = (ax == 0) ? tbx : (ax == 1) ? tby : tbz;
+    if (nb >= 3) {
+      noff[ax] = 3;
+      offs[ax][0] = wrapi(tcur - 1, nb); offs[ax][1] = tcur; offs[ax][2] = wrapi(tcur + 1, nb);
+    } else if (nb == 2) {
+      noff[ax] = 2;
+      offs[ax][0] = 0; offs[ax][1] = 1;
+    } else {
+      noff[ax] = 1;
+      offs[ax][0] = 0;
+    }
+  }
+  for (int oz = 0; oz < noff[2]; oz++)
+    for (int oy = 0; oy < noff[1]; oy++)
+      for (int ox = 0; ox < noff[0]; ox++) {
+        const int b = (offs[2][oz] * bs.nb[1] + offs[1][oy]) * bs.nb[0] + offs[0][ox];
+        const int s = offsets[b], e = offsets[b + 1];
+        for (int base = s; base < e; base += kSpreadThreads) {
+          const int q = base + tid;
+          bool take = false;
+          SpreadCand<T> mine;
+          if (q < e) {
+            const int p = sorted[q];
+            double g[3];
+#pragma unroll
+            for (int ax = 0; ax < 3; ax++) g[ax] = (x_old[3L * p + ax] - a.lo) / a.dx;
+            take = true;
+#pragma unroll
+            for (int ax = 0; ax < 3; ax++) {
+              const double gs = g[ax] - 0.5;
+              const int b0 = (int)floor(g[ax]) - 1, b1 = (int)floor(gs) - 1;
+              const int r0 = wrapi(b0 - t0[ax], nn[ax]), r1 = wrapi(b1 - t0[ax], nn[ax]);
+              mine.rb[ax][0] = r0;
+              mine.rb[ax][1] = r1;
+              bool hit = false;
+              for (int c = 0; c < 5; c++) hit |= (((r1 + c) % nn[ax]) < ext[ax]);
+              take = take && hit;
+#pragma unroll
+              for (int i = 0; i < 4; i++) {
+                mine.w[ax][0][i] = ref_weight<T>(fabs(g[ax] - (double)(b0 + i)));
+                mine.w[ax][1][i] = ref_weight<T>(fabs(gs - (double)(b1 + i)));
+              }
+            }
+#pragma unroll
+            for (int dd = 0; dd < 3; dd++) mine.tf[dd] = (T)tf[3L * p + dd];
+          }
+          const unsigned bal = __ballot_sync(0xffffffffu, take);
+          if (lane == 0) wtot[wid] = __popc(bal);
+          __syncthreads();
+          int wbase = 0, tot = 0;
+#pragma unroll
+          for (int w = 0; w < kSpreadThreads / 32; w++) {
+            if (w < wid) wbase += wtot[w];
+            tot += wtot[w];
+          }
+          const int n0 = s_ncand;
+          if (take) cand[n0 + wbase + __popc(bal & ((1u << lane) - 1u))] = mine;
+          __syncthreads();
+          if (tid == 0) s_ncand = n0 + tot;
+          __syncthreads();
+          if (s_ncand >= kSpreadCap) {
+            if (row_ok) spread_accumulate(cand, s_ncand, d, ry, rz, nx, ny, nz, acc);
+            __syncthreads();
+            if (tid == 0) s_ncand = 0;
+            __syncthreads();
+          }
+        }
+      }
+  if (row_ok) spread_accumulate(cand, s_ncand, d, ry, rz, nx, ny, nz, acc);
+  if (row_ok) {
+#pragma unroll
+    for (int cx = 0; cx < kTile; cx++)
+      if (cx < ext[0]) row[cx] = acc[cx];
+  }
+}
+
+template <typename T>
+cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const double* tf, const BinSpec& bs,
+                          const int* offsets, const int* sorted, const CouplingArgs& a, cudaStream_t st) {
+  const int ntiles = bs.nb[0] * bs.nb[1] * bs.nb[2];
+  if (!accumulate && a.M == 0) {
+    return cudaMemsetAsync(fgrid, 0, sizeof(T) * 3L * a.nx * a.ny * a.nz, st);
+  }
+  const size_t sm = sizeof(SpreadCand<T>) * (kSpreadCap + kSpreadThreads);
+  cudaError_t e = cudaFuncSetAttribute((const void*)k_spread_gather<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm);
+  if (e != cudaSuccess) return e;
+  k_spread_gather<T><<<ntiles, kSpreadThreads, sm, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets, sorted,
+                                                        a);
+  return cudaGetLastError();
+}
+
+template cudaError_t interp_update<double>(const double*, const double*, double*, double*, double*, const double*,
+                                           double*, const int*, const CouplingArgs&, uint32_t*, cudaStream_t);
+template cudaError_t interp_update<float>(const float*, const double*, double*, double*, double*, const double*,
+                                          double*, const int*, const CouplingArgs&, uint32_t*, cudaStream_t);
+template cudaError_t spread_gather<double>(double*, bool, const double*, const double*, const BinSpec&, const int*,
+                                           const int*, const CouplingArgs&, cudaStream_t);
+template cudaError_t spread_gather<float>(float*, bool, const double*, const double*, const BinSpec&, const int*,
+                                          const int*, const CouplingArgs&, cudaStream_t);
+
+}  // namespace selm

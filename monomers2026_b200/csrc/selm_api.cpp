@@ -1,0 +1,838 @@
+// selm_api.cpp - host engine and C ABI of libselm_b200.so.
+//
+// The engine keeps the reference's object split (cuda/SELM.cu Selm driver,
+// cuda/SELM_Eulerian_Period.cu fluid, cuda/SELM_Lagrangian_LAMMPS.cu
+// monomers) but all state stays resident on the device: one stream, no host
+// synchronisation inside a step, device forces instead of the LAMMPS round
+// trip.  Errors are returned as status codes (the reference prints and calls
+// exit(-1), cuda/check.cuh:6-10).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/selm_b200.h"
+#include "selm_engine.h"
+#include "selm_kernels.h"
+
+using namespace selm;
+
+static thread_local std::string g_err;
+
+int selm_fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CU(x)                                                                                   \
+  do {                                                                                          \
+    cudaError_t e_ = (x);                                                                       \
+    if (e_ != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ================================================================ allocation
+template <typename T> static int dalloc(selm_sim* s, T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return selm_fail(SELM_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+  }
+  s->allocs.push_back(*p);
+  return SELM_OK;
+}
+
+static void free_all(std::vector<void*>& v) {
+  for (void* p : v) cudaFree(p);
+  v.clear();
+}
+
+// ================================================================ FFT tables
+static bool smooth7(int n) {
+  if (n < 1) return false;
+  for (int p : {2, 3, 5, 7})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+template <typename C> static std::vector<C> twiddles(int n, int sign) {
+  std::vector<C> w(n);
+  for (int t = 0; t < n; t++) {
+    const double a = 2.0 * M_PI * (double)t / (double)n;
+    w[t].x = (decltype(C::x))cos(a);
+    w[t].y = (decltype(C::x))(sign * sin(a));
+  }
+  return w;
+}
+
+template <typename T>
+static int make_tables(std::vector<void*>& allocs, const int dims[3], FftTables<T>& tb) {
+  using C = cpx<T>;
+  const int n[3] = {dims[0], dims[1], dims[2]};
+  const C* ptr[6];
+  for (int a = 0; a < 3; a++) {
+    for (int sgn = 0; sgn < 2; sgn++) {
+      auto w = twiddles<C>(n[a], sgn == 0 ? -1 : 1);
+      C* d = nullptr;
+      if (cudaMalloc((void**)&d, sizeof(C) * n[a]) != cudaSuccess) return SELM_ERR_NOMEM;
+      allocs.push_back(d);
+      if (cudaMemcpy(d, w.data(), sizeof(C) * n[a], cudaMemcpyHostToDevice) != cudaSuccess) return SELM_ERR_CUDA;
+      ptr[2 * a + sgn] = d;
+    }
+  }
+  tb.rx = make_radix(n[0]);
+  tb.ry = make_radix(n[1]);
+  tb.rz = make_radix(n[2]);
+  tb.wx_f = ptr[0]; tb.wx_b = ptr[1];
+  tb.wy_f = ptr[2]; tb.wy_b = ptr[3];
+  tb.wz_f = ptr[4]; tb.wz_b = ptr[5];
+  return SELM_OK;
+}
+
+// ================================================================ profiling
+void prof_mark(selm_sim* s, const char* name, bool begin) {
+  if (!s->prof) return;
+  if (begin) {
+    ProfEvent ev;
+    ev.name = name;
+    cudaEventCreate(&ev.a);
+    cudaEventCreate(&ev.b);
+    cudaEventRecord(ev.a, s->st);
+    s->pending.push_back(ev);
+  } else if (!s->pending.empty()) {
+    for (auto it = s->pending.rbegin(); it != s->pending.rend(); ++it)
+      if (it->name == name && !it->closed) {
+        cudaEventRecord(it->b, s->st);
+        it->closed = true;
+        break;
+      }
+  }
+}
+
+static void prof_collect(selm_sim* s) {
+  if (s->pending.empty()) return;
+  cudaStreamSynchronize(s->st);
+  for (auto& ev : s->pending) {
+    float ms = 0.f;
+    if (ev.closed) cudaEventElapsedTime(&ms, ev.a, ev.b);
+    auto& acc = s->prof_acc[ev.name];
+    acc.first += ms;
+    acc.second += 1;
+    cudaEventDestroy(ev.a);
+    cudaEventDestroy(ev.b);
+  }
+  s->pending.clear();
+}
+
+// ================================================================ creation
+static int validate(const selm_params* p) {
+  if (!p) return selm_fail(SELM_ERR_INVALID, "params is NULL");
+  for (int a = 0; a < 3; a++)
+    if (p->num_mesh_pts[a] < 4 || p->num_mesh_pts[a] > 1024 || !smooth7(p->num_mesh_pts[a]))
+      return selm_fail(SELM_ERR_INVALID, "numMeshPtsPerDir must be in [4,1024] with prime factors 2,3,5,7");
+  if (p->num_mesh_pts[0] != p->num_mesh_pts[1] || p->num_mesh_pts[0] != p->num_mesh_pts[2])
+    return selm_fail(SELM_ERR_INVALID, "numMeshPtsPerDir must be equal in every dimension (cubic box)");
+  if (!(p->box_hi > p->box_lo)) return selm_fail(SELM_ERR_INVALID, "box_hi must exceed box_lo");
+  if (!(p->rho > 0) || !(p->dt > 0) || !(p->mu >= 0))
+    return selm_fail(SELM_ERR_INVALID, "rho, dt must be positive and mu non-negative");
+  if (p->form < SELM_FORM_PLAIN64 || p->form > SELM_FORM_FUSED32) return selm_fail(SELM_ERR_INVALID, "unknown form");
+  if (p->integrator != SELM_INTEGRATOR_INERTIAL && p->integrator != SELM_INTEGRATOR_QUASI_STEADY)
+    return selm_fail(SELM_ERR_INVALID, "unknown integrator");
+  if (p->integrator == SELM_INTEGRATOR_QUASI_STEADY && p->form == SELM_FORM_PLAIN64)
+    return selm_fail(SELM_ERR_INVALID, "the quasi-steady integrator runs in the fused forms only");
+  if (p->noise_mode != SELM_NOISE_REF_COMPAT && p->noise_mode != SELM_NOISE_EXACT)
+    return selm_fail(SELM_ERR_INVALID, "unknown noise mode");
+  return SELM_OK;
+}
+
+extern "C" int selm_create(const selm_params* params, selm_sim** out) {
+  if (!out) return selm_fail(SELM_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  int rc = validate(params);
+  if (rc) return rc;
+  selm_sim* s = new selm_sim();
+  s->prm = *params;
+  s->nx = params->num_mesh_pts[0];
+  s->ny = params->num_mesh_pts[1];
+  s->nz = params->num_mesh_pts[2];
+  s->N = (long)s->nx * s->ny * s->nz;
+  s->N2 = (long)(s->nx / 2 + 1) * s->ny * s->nz;
+  s->lo = params->box_lo;
+  s->hi = params->box_hi;
+  s->dx = (s->hi - s->lo) / s->nx;  // cuda/SELM_Eulerian_Period.cu:18
+  if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete s;
+    return selm_fail(SELM_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  s->own_st = true;
+  rc = engine_allocate_grid(s);
+  if (rc) {
+    selm_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return SELM_OK;
+}
+
+int engine_allocate_grid(selm_sim* s) {
+  int rc;
+  const long N = s->N, N2 = s->N2;
+  if ((rc = dalloc(s, &s->err, 1))) return rc;
+  CU(cudaMemset(s->err, 0, sizeof(uint32_t)));
+  if ((rc = make_tables<double>(s->allocs, s->prm.num_mesh_pts, s->tb64))) return selm_fail(rc, "FFT tables");
+  if ((rc = make_tables<float>(s->allocs, s->prm.num_mesh_pts, s->tb32))) return selm_fail(rc, "FFT tables");
+  if (s->prm.form == SELM_FORM_PLAIN64) {
+    if ((rc = dalloc(s, &s->u64[0], 3 * N))) return rc;
+    if ((rc = dalloc(s, &s->u64[1], 3 * N))) return rc;
+    if ((rc = dalloc(s, &s->fg64, 3 * N))) return rc;
+    if ((rc = dalloc(s, &s->p64, N))) return rc;
+    if ((rc = dalloc(s, &s->work64, 6 * N2))) return rc;  // 3 components x N2 complex
+    if ((rc = dalloc(s, &s->partial, 3 * kSumParts))) return rc;
+    if ((rc = dalloc(s, &s->sum, 3))) return rc;
+    CU(cudaMemset(s->u64[0], 0, sizeof(double) * 3 * N));
+    CU(cudaMemset(s->u64[1], 0, sizeof(double) * 3 * N));
+    CU(cudaMemset(s->fg64, 0, sizeof(double) * 3 * N));
+  } else {
+    rc = fused_allocate(s);
+    if (rc) return rc;
+  }
+  // coupling tiles (8^3 cells)
+  BinSpec& t = s->tiles;
+  t.mode = 0;
+  t.lo = s->lo;
+  t.dx = s->dx;
+  t.L = s->hi - s->lo;
+  const int nn[3] = {s->nx, s->ny, s->nz};
+  for (int a = 0; a < 3; a++) {
+    t.n[a] = nn[a];
+    t.tile[a] = 8;
+    t.nb[a] = (nn[a] + 7) / 8;
+  }
+  return SELM_OK;
+}
+
+static int alloc_bins(selm_sim* s, const BinSpec& bs, BinBuffers& bb, int M) {
+  const long nbk = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
+  int rc;
+  if ((rc = dalloc(s, &bb.counts, nbk + 1))) return rc;
+  if ((rc = dalloc(s, &bb.offsets, nbk + 1))) return rc;
+  if ((rc = dalloc(s, &bb.cursor, nbk))) return rc;
+  if ((rc = dalloc(s, &bb.bucket_of, M))) return rc;
+  if ((rc = dalloc(s, &bb.unsorted, M))) return rc;
+  if ((rc = dalloc(s, &bb.sorted, M))) return rc;
+  if ((rc = dalloc(s, &bb.scan_tmp, scan_tmp_size(nbk + 1)))) return rc;
+  return SELM_OK;
+}
+
+extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const double* v, const double* mass) {
+  if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  if (M < 0 || (M > 0 && (!x || !mass))) return selm_fail(SELM_ERR_INVALID, "bad particle arrays");
+  if (s->M != 0 && M != s->M) return selm_fail(SELM_ERR_STATE, "monomer count is fixed once set");
+  for (long i = 0; i < 3L * M; i++)
+    if (!std::isfinite(x[i])) return selm_fail(SELM_ERR_INVALID, "non-finite position");
+  for (int i = 0; i < M; i++)
+    if (!(mass[i] > 0)) return selm_fail(SELM_ERR_INVALID, "masses must be positive");
+  int rc;
+  if (s->M == 0 && M > 0) {
+    s->M = M;
+    if ((rc = dalloc(s, &s->x[0], 3L * M))) return rc;
+    if ((rc = dalloc(s, &s->x[1], 3L * M))) return rc;
+    if ((rc = dalloc(s, &s->v, 3L * M))) return rc;
+    if ((rc = dalloc(s, &s->f, 3L * M))) return rc;
+    if ((rc = dalloc(s, &s->m, M))) return rc;
+    if ((rc = dalloc(s, &s->tf, 3L * M))) return rc;
+    if ((rc = alloc_bins(s, s->tiles, s->tbb, M))) return rc;
+    CU(cudaMemsetAsync(s->f, 0, sizeof(double) * 3 * M, s->st));
+  }
+  if (M == 0) return SELM_OK;
+  CU(cudaMemcpyAsync(s->x[s->cx], x, sizeof(double) * 3 * M, cudaMemcpyHostToDevice, s->st));
+  if (v) CU(cudaMemcpyAsync(s->v, v, sizeof(double) * 3 * M, cudaMemcpyHostToDevice, s->st));
+  else CU(cudaMemsetAsync(s->v, 0, sizeof(double) * 3 * M, s->st));
+  CU(cudaMemcpyAsync(s->m, mass, sizeof(double) * M, cudaMemcpyHostToDevice, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  return SELM_OK;
+}
+
+// ---------------------------------------------------------------- topology
+extern "C" int selm_set_topology(selm_sim* s, const selm_topology* tp) {
+  if (!s || !tp) return selm_fail(SELM_ERR_INVALID, "NULL argument");
+  if (tp->natoms != s->M) return selm_fail(SELM_ERR_INVALID, "topology natoms differs from the monomer count");
+  const int M = tp->natoms, nt = tp->ntypes;
+  if (nt < 1 || !tp->type) return selm_fail(SELM_ERR_INVALID, "need ntypes >= 1 and types");
+  for (int i = 0; i < M; i++)
+    if (tp->type[i] < 1 || tp->type[i] > nt) return selm_fail(SELM_ERR_INVALID, "atom type out of range");
+  // CSR of incident bonds, in bond order
+  std::vector<int> boff(M + 1, 0), bnbr, btyp;
+  for (int b = 0; b < tp->nbonds; b++) {
+    const int t = tp->bonds[3 * b], i = tp->bonds[3 * b + 1], j = tp->bonds[3 * b + 2];
+    if (i < 0 || i >= M || j < 0 || j >= M || i == j || t < 1 || t > tp->nbondtypes)
+      return selm_fail(SELM_ERR_INVALID, "bad bond");
+    boff[i + 1]++;
+    boff[j + 1]++;
+  }
+  for (int i = 0; i < M; i++) boff[i + 1] += boff[i];
+  bnbr.resize(boff[M]);
+  btyp.resize(boff[M]);
+  {
+    std::vector<int> fill(M, 0);
+    for (int b = 0; b < tp->nbonds; b++) {
+      const int t = tp->bonds[3 * b], i = tp->bonds[3 * b + 1], j = tp->bonds[3 * b + 2];
+      bnbr[boff[i] + fill[i]] = j; btyp[boff[i] + fill[i]++] = t;
+      bnbr[boff[j] + fill[j]] = i; btyp[boff[j] + fill[j]++] = t;
+    }
+  }
+  // CSR of incident angles (entries copied per member atom, in angle order)
+  std::vector<int> aoff(M + 1, 0), aat;
+  for (int a = 0; a < tp->nangles; a++) {
+    const int* A = tp->angles + 4 * a;
+    if (A[0] < 1 || A[0] > tp->nangletypes) return selm_fail(SELM_ERR_INVALID, "bad angle type");
+    for (int r = 1; r <= 3; r++) {
+      if (A[r] < 0 || A[r] >= M) return selm_fail(SELM_ERR_INVALID, "bad angle atom");
+    }
+    aoff[A[1] + 1]++;
+    if (A[2] != A[1]) aoff[A[2] + 1]++;
+    if (A[3] != A[1] && A[3] != A[2]) aoff[A[3] + 1]++;
+  }
+  for (int i = 0; i < M; i++) aoff[i + 1] += aoff[i];
+  aat.resize(4 * (size_t)aoff[M]);
+  {
+    std::vector<int> fill(M, 0);
+    for (int a = 0; a < tp->nangles; a++) {
+      const int* A = tp->angles + 4 * a;
+      int members[3] = {A[1], A[2], A[3]};
+      for (int r = 0; r < 3; r++) {
+        bool dup = false;
+        for (int q = 0; q < r; q++) dup |= (members[q] == members[r]);
+        if (dup) continue;
+        const int at = members[r];
+        std::memcpy(&aat[4 * (size_t)(aoff[at] + fill[at]++)], A, 4 * sizeof(int));
+      }
+    }
+  }
+  // special neighbours (1-2, 1-3, 1-4 through the bond graph; closest wins)
+  std::vector<int> soff(M + 1, 0), snbr;
+  std::vector<double> sw;
+  {
+    std::vector<std::vector<int>> adj(M);
+    for (int b = 0; b < tp->nbonds; b++) {
+      adj[tp->bonds[3 * b + 1]].push_back(tp->bonds[3 * b + 2]);
+      adj[tp->bonds[3 * b + 2]].push_back(tp->bonds[3 * b + 1]);
+    }
+    for (int i = 0; i < M; i++) {
+      std::vector<int> lst, lvl;
+      auto add = [&](int j, int l) {
+        if (j == i) return;
+        for (int q : lst)
+          if (q == j) return;
+        lst.push_back(j);
+        lvl.push_back(l);
+      };
+      for (int j : adj[i]) add(j, 1);
+      size_t f0 = 0;
+      for (int l = 2; l <= 3; l++) {
+        const size_t f1 = lst.size();
+        for (size_t q = f0; q < f1; q++)
+          if (lvl[q] == l - 1)
+            for (int j : adj[lst[q]]) add(j, l);
+        f0 = f1;
+      }
+      for (size_t q = 0; q < lst.size(); q++) {
+        const double w = tp->special_lj[lvl[q] - 1];
+        if (w == 1.0) continue;
+        snbr.push_back(lst[q]);
+        sw.push_back(w);
+      }
+      soff[i + 1] = (int)snbr.size();
+    }
+  }
+  // upload
+  int rc;
+  auto up_i = [&](const std::vector<int>& h, int** d) -> int {
+    int r = dalloc(s, d, h.size());
+    if (r) return r;
+    if (!h.empty() && cudaMemcpy(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return SELM_ERR_CUDA;
+    return SELM_OK;
+  };
+  auto up_d = [&](const double* h, size_t n, double** d) -> int {
+    int r = dalloc(s, d, n);
+    if (r) return r;
+    if (n && h && cudaMemcpy(*d, h, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess) return SELM_ERR_CUDA;
+    return SELM_OK;
+  };
+  ForceTopo& T = s->topo;
+  T = ForceTopo{};
+  T.M = M;
+  T.ntypes = nt;
+  int *d_type, *d_boff, *d_bnbr, *d_btyp, *d_aoff, *d_aat, *d_soff, *d_snbr;
+  double *d_bc, *d_ac, *d_pc, *d_sw;
+  std::vector<int> types(tp->type, tp->type + M);
+  if ((rc = up_i(types, &d_type))) return selm_fail(rc, "upload");
+  if ((rc = up_i(boff, &d_boff)) || (rc = up_i(bnbr, &d_bnbr)) || (rc = up_i(btyp, &d_btyp)))
+    return selm_fail(rc, "upload");
+  if ((rc = up_i(aoff, &d_aoff)) || (rc = up_i(aat, &d_aat))) return selm_fail(rc, "upload");
+  if ((rc = up_i(soff, &d_soff)) || (rc = up_i(snbr, &d_snbr))) return selm_fail(rc, "upload");
+  if ((rc = up_d(sw.data(), sw.size(), &d_sw))) return selm_fail(rc, "upload");
+  if ((rc = up_d(tp->bond_coeff, tp->bond_style ? 4 * (size_t)(tp->nbondtypes + 1) : 0, &d_bc)))
+    return selm_fail(rc, "upload");
+  if ((rc = up_d(tp->angle_coeff, tp->angle_style ? 2 * (size_t)(tp->nangletypes + 1) : 0, &d_ac)))
+    return selm_fail(rc, "upload");
+  const size_t npc = 3 * (size_t)(nt + 1) * (nt + 1);
+  if ((rc = up_d(tp->pair_coeff, tp->pair_style ? npc : 0, &d_pc))) return selm_fail(rc, "upload");
+  T.type = d_type;
+  T.bond_style = tp->nbonds > 0 ? tp->bond_style : 0;
+  T.bond_off = d_boff; T.bond_nbr = d_bnbr; T.bond_typ = d_btyp; T.bond_coeff = d_bc;
+  T.angle_style = tp->nangles > 0 ? tp->angle_style : 0;
+  T.ang_off = d_aoff; T.ang_atoms = d_aat; T.angle_coeff = d_ac;
+  T.pair_style = tp->pair_style;
+  T.pair_coeff = d_pc;
+  T.sp_off = d_soff; T.sp_nbr = d_snbr; T.sp_w = d_sw;
+  for (int a = 0; a < 3; a++) T.body[a] = tp->body_force[a];
+  T.lo = s->lo;
+  T.hi = s->hi;
+  // force cells: as many cells of size >= the largest cutoff as fit (1 if < 3)
+  double rcmax = 0.0;
+  if (tp->pair_style && tp->pair_coeff)
+    for (size_t q = 0; q < (size_t)(nt + 1) * (nt + 1); q++) rcmax = std::max(rcmax, tp->pair_coeff[3 * q + 2]);
+  const double L = s->hi - s->lo;
+  int nc = rcmax > 0 ? (int)std::floor(L / rcmax) : 1;
+  if (nc < 3) nc = 1;
+  if (nc > 1024) nc = 1024;
+  BinSpec& fc = s->fcells;
+  fc.mode = 1;
+  fc.lo = s->lo;
+  fc.dx = s->dx;
+  fc.L = L;
+  for (int a = 0; a < 3; a++) {
+    fc.n[a] = nc;
+    fc.tile[a] = 1;
+    fc.nb[a] = nc;
+  }
+  if (tp->pair_style && M > 1) {
+    if ((rc = alloc_bins(s, s->fcells, s->fbb, M))) return rc;
+  }
+  s->have_topo = true;
+  s->cb = nullptr;
+  return SELM_OK;
+}
+
+extern "C" int selm_set_force_callback(selm_sim* s, selm_force_fn fn, void* user) {
+  if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  s->cb = fn;
+  s->cb_user = user;
+  if (fn) s->have_topo = false;
+  return SELM_OK;
+}
+
+// ---------------------------------------------------------------- forces
+int engine_forces(selm_sim* s) {
+  if (s->M == 0) return SELM_OK;
+  double* x = s->x[s->cx];
+  if (s->have_topo) {
+    prof_mark(s, "forces", true);
+    if (s->topo.pair_style && s->M > 1) {
+      CU(bin_particles(x, s->M, s->fcells, s->fbb, s->st));
+      CU(compute_forces(x, s->f, s->topo, s->fcells, s->fbb.offsets, s->fbb.sorted, s->err, s->st));
+    } else {
+      CU(compute_forces(x, s->f, s->topo, s->fcells, nullptr, nullptr, s->err, s->st));
+    }
+    prof_mark(s, "forces", false);
+    return SELM_OK;
+  }
+  if (s->cb) {
+    // host round trip, as Lagrangian_LAMMPS::compute_f (cuda/SELM_Lagrangian_LAMMPS.cu:107-130)
+    s->hx.resize(3 * (size_t)s->M);
+    s->hv.resize(3 * (size_t)s->M);
+    s->hf.resize(3 * (size_t)s->M);
+    CU(cudaMemcpyAsync(s->hx.data(), x, sizeof(double) * 3 * s->M, cudaMemcpyDeviceToHost, s->st));
+    CU(cudaMemcpyAsync(s->hv.data(), s->v, sizeof(double) * 3 * s->M, cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    const int r = s->cb(s->cb_user, s->M, s->hx.data(), s->hv.data(), s->hf.data());
+    if (r != 0) return selm_fail(SELM_ERR_INVALID, "force callback returned an error");
+    CU(cudaMemcpyAsync(s->f, s->hf.data(), sizeof(double) * 3 * s->M, cudaMemcpyHostToDevice, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    return SELM_OK;
+  }
+  CU(cudaMemsetAsync(s->f, 0, sizeof(double) * 3 * s->M, s->st));
+  return SELM_OK;
+}
+
+// ---------------------------------------------------------------- step (plain form)
+static CouplingArgs coupling_args(selm_sim* s, uint64_t step) {
+  CouplingArgs a{};
+  a.nx = s->nx;
+  a.ny = s->ny;
+  a.nz = s->nz;
+  a.lo = s->lo;
+  a.hi = s->hi;
+  a.dx = s->dx;
+  a.dt = s->prm.dt;
+  a.upsilon = 6.0 * M_PI * 2 * s->dx * s->prm.mu;                       // cuda/SELM_Lagrangian_LAMMPS.cu:138
+  a.coef = sqrt(2.0 * s->prm.KB * s->prm.T * a.upsilon * s->prm.dt);  // :139
+  a.stochastic = s->prm.flag_stochastic;
+  a.seed = s->prm.seed;
+  a.step = step;
+  a.M = s->M;
+  return a;
+}
+
+static int plain_compute_f_step(selm_sim* s, uint64_t noise_step) {
+  prof_mark(s, "noise", true);
+  CU(plain_compute_f(s->fg64, (double2*)s->work64, s->nx, s->ny, s->nz, s->dx, s->prm.KB, s->prm.T, s->prm.dt,
+                     s->prm.mu, s->prm.flag_stochastic != 0, s->prm.seed, noise_step, s->prm.noise_mode, s->tb64,
+                     s->st));
+  prof_mark(s, "noise", false);
+  return SELM_OK;
+}
+
+static int plain_step(selm_sim* s) {
+  const uint64_t n = ++s->step;
+  const CouplingArgs a = coupling_args(s, n);
+  double* xo = s->x[s->cx];
+  double* xn = s->x[s->cx ^ 1];
+  if (s->M > 0) {
+    prof_mark(s, "bin", true);
+    CU(bin_particles(xo, s->M, s->tiles, s->tbb, s->st));
+    prof_mark(s, "bin", false);
+    prof_mark(s, "interp_update", true);
+    CU(interp_update<double>(s->u64[s->cu], xo, xn, s->v, s->f, s->m, s->tf, s->tbb.sorted, a, s->err, s->st));
+    prof_mark(s, "interp_update", false);
+    prof_mark(s, "spread", true);
+    CU(spread_gather<double>(s->fg64, true, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st));
+    prof_mark(s, "spread", false);
+    s->cx ^= 1;
+  }
+  prof_mark(s, "fluid", true);
+  CU(plain_fluid_run(s->u64[s->cu], s->u64[s->cu ^ 1], s->fg64, s->p64, (double2*)s->work64, s->partial, s->sum,
+                     s->nx, s->ny, s->nz, s->dx, s->prm.dt, s->prm.mu, s->prm.rho, s->tb64, s->st));
+  prof_mark(s, "fluid", false);
+  s->cu ^= 1;
+  int rc = plain_compute_f_step(s, n + 1);
+  if (rc) return rc;
+  return engine_forces(s);
+}
+
+extern "C" int selm_initial(selm_sim* s) {
+  if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  s->step = 0;
+  int rc = engine_forces(s);
+  if (rc) return rc;
+  if (s->prm.form == SELM_FORM_PLAIN64) {
+    CU(cudaMemsetAsync(s->u64[0], 0, sizeof(double) * 3 * s->N, s->st));
+    CU(cudaMemsetAsync(s->u64[1], 0, sizeof(double) * 3 * s->N, s->st));
+    s->cu = 0;
+    rc = plain_compute_f_step(s, 1);
+  } else {
+    rc = fused_initial(s);
+  }
+  if (rc) return rc;
+  s->initialized = true;
+  return SELM_OK;
+}
+
+extern "C" int selm_step(selm_sim* s, int nsteps) {
+  if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  if (!s->initialized) return selm_fail(SELM_ERR_STATE, "selm_initial has not been called");
+  if (nsteps < 0) return selm_fail(SELM_ERR_INVALID, "nsteps < 0");
+  for (int i = 0; i < nsteps; i++) {
+    const int rc = (s->prm.form == SELM_FORM_PLAIN64) ? plain_step(s) : fused_step(s);
+    if (rc) return rc;
+  }
+  return SELM_OK;
+}
+
+extern "C" int selm_destroy(selm_sim* s) {
+  if (!s) return SELM_OK;
+  if (s->st) cudaStreamSynchronize(s->st);
+  for (auto& ev : s->pending) {
+    cudaEventDestroy(ev.a);
+    cudaEventDestroy(ev.b);
+  }
+  fused_release(s);
+  free_all(s->allocs);
+  if (s->own_st && s->st) cudaStreamDestroy(s->st);
+  delete s;
+  return SELM_OK;
+}
+
+// ---------------------------------------------------------------- access
+extern "C" int selm_get_particles(selm_sim* s, double* x, double* v, double* f) {
+  if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  if (s->M == 0) return SELM_OK;
+  const size_t b = sizeof(double) * 3 * s->M;
+  if (x) CU(cudaMemcpyAsync(x, s->x[s->cx], b, cudaMemcpyDeviceToHost, s->st));
+  if (v) CU(cudaMemcpyAsync(v, s->v, b, cudaMemcpyDeviceToHost, s->st));
+  if (f) CU(cudaMemcpyAsync(f, s->f, b, cudaMemcpyDeviceToHost, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  return SELM_OK;
+}
+
+extern "C" int selm_get_field(selm_sim* s, int which, double* out) {
+  if (!s || !out) return selm_fail(SELM_ERR_INVALID, "NULL argument");
+  if (which != SELM_FIELD_U && which != SELM_FIELD_F) return selm_fail(SELM_ERR_INVALID, "unknown field");
+  if (s->prm.form == SELM_FORM_PLAIN64) {
+    const double* src = (which == SELM_FIELD_U) ? s->u64[s->cu] : s->fg64;
+    CU(cudaMemcpyAsync(out, src, sizeof(double) * 3 * s->N, cudaMemcpyDeviceToHost, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    return SELM_OK;
+  }
+  return fused_get_field(s, which, out);
+}
+
+extern "C" int selm_set_field(selm_sim* s, int which, const double* in) {
+  if (!s || !in) return selm_fail(SELM_ERR_INVALID, "NULL argument");
+  if (which != SELM_FIELD_U && which != SELM_FIELD_F) return selm_fail(SELM_ERR_INVALID, "unknown field");
+  if (s->prm.form == SELM_FORM_PLAIN64) {
+    double* dst = (which == SELM_FIELD_U) ? s->u64[s->cu] : s->fg64;
+    CU(cudaMemcpyAsync(dst, in, sizeof(double) * 3 * s->N, cudaMemcpyHostToDevice, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    return SELM_OK;
+  }
+  return fused_set_field(s, which, in);
+}
+
+extern "C" int selm_get_info(selm_sim* s, int* natoms, int dims[3], unsigned long long* step) {
+  if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  if (natoms) *natoms = s->M;
+  if (dims) {
+    dims[0] = s->nx;
+    dims[1] = s->ny;
+    dims[2] = s->nz;
+  }
+  if (step) *step = s->step;
+  return SELM_OK;
+}
+
+extern "C" int selm_status(selm_sim* s, unsigned int* word) {
+  if (!s || !word) return selm_fail(SELM_ERR_INVALID, "NULL argument");
+  uint32_t w = 0;
+  CU(cudaMemcpyAsync(&w, s->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  *word = w;
+  return SELM_OK;
+}
+
+extern "C" int selm_set_stream(selm_sim* s, void* stream) {
+  if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  CU(cudaStreamSynchronize(s->st));
+  if (s->own_st) cudaStreamDestroy(s->st);
+  if (stream) {
+    s->st = (cudaStream_t)stream;
+    s->own_st = false;
+  } else {
+    CU(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+    s->own_st = true;
+  }
+  return fused_stream_changed(s);
+}
+
+extern "C" void* selm_get_stream(selm_sim* s) { return s ? (void*)s->st : nullptr; }
+
+extern "C" int selm_synchronize(selm_sim* s) {
+  if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  CU(cudaStreamSynchronize(s->st));
+  return SELM_OK;
+}
+
+extern "C" int selm_profile_enable(selm_sim* s, int enable) {
+  if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  prof_collect(s);
+  s->prof = enable != 0;
+  if (enable) s->prof_acc.clear();
+  return SELM_OK;
+}
+
+extern "C" int selm_profile_read(selm_sim* s, const char* kernel, double* total_ms, long* launches) {
+  if (!s || !kernel) return selm_fail(SELM_ERR_INVALID, "NULL argument");
+  prof_collect(s);
+  auto it = s->prof_acc.find(kernel);
+  if (total_ms) *total_ms = it == s->prof_acc.end() ? 0.0 : it->second.first;
+  if (launches) *launches = it == s->prof_acc.end() ? 0 : it->second.second;
+  return SELM_OK;
+}
+
+extern "C" const char* selm_last_error(void) { return g_err.c_str(); }
+extern "C" const char* selm_version(void) { return "selm_b200 0.1 (sm_100a)"; }
+
+// ================================================================ operators on host buffers
+namespace {
+struct OpScope {
+  std::vector<void*> allocs;
+  cudaStream_t st = nullptr;
+  ~OpScope() {
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+    for (void* p : allocs) cudaFree(p);
+  }
+  template <typename T> T* alloc(size_t n) {
+    T* p = nullptr;
+    if (cudaMalloc((void**)&p, sizeof(T) * (n ? n : 1)) != cudaSuccess) return nullptr;
+    allocs.push_back(p);
+    return p;
+  }
+};
+
+int check_dims(const int dims[3]) {
+  if (!dims) return selm_fail(SELM_ERR_INVALID, "dims is NULL");
+  for (int a = 0; a < 3; a++)
+    if (dims[a] < 4 || dims[a] > 1024 || !smooth7(dims[a]))
+      return selm_fail(SELM_ERR_INVALID, "dims must be in [4,1024] with prime factors 2,3,5,7");
+  return SELM_OK;
+}
+
+template <typename T> int op_interp(const int dims[3], double lo, double dx, const double* u, int M, const double* x,
+                                    double* out) {
+  OpScope o;
+  CU(cudaStreamCreate(&o.st));
+  const long N = (long)dims[0] * dims[1] * dims[2];
+  std::vector<T> hu(3 * N);
+  for (long i = 0; i < 3 * N; i++) hu[i] = (T)u[i];
+  T* du = o.alloc<T>(3 * N);
+  double* dxp = o.alloc<double>(3L * M);
+  double* dout = o.alloc<double>(3L * M);
+  if (!du || !dxp || !dout) return selm_fail(SELM_ERR_NOMEM, "cudaMalloc failed");
+  CU(cudaMemcpy(du, hu.data(), sizeof(T) * 3 * N, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dxp, x, sizeof(double) * 3 * M, cudaMemcpyHostToDevice));
+  CU(interp_only<T>(du, dxp, M, dims[0], dims[1], dims[2], lo, dx, dout, o.st));
+  CU(cudaStreamSynchronize(o.st));
+  CU(cudaMemcpy(out, dout, sizeof(double) * 3 * M, cudaMemcpyDeviceToHost));
+  return SELM_OK;
+}
+
+template <typename T> int op_spread(const int dims[3], double lo, double dx, double* fgrid, int M, const double* x,
+                                    const double* tf) {
+  OpScope o;
+  CU(cudaStreamCreate(&o.st));
+  const long N = (long)dims[0] * dims[1] * dims[2];
+  BinSpec bs{};
+  bs.mode = 0;
+  bs.lo = lo;
+  bs.dx = dx;
+  bs.L = dx * dims[0];
+  for (int a = 0; a < 3; a++) {
+    bs.n[a] = dims[a];
+    bs.tile[a] = 8;
+    bs.nb[a] = (dims[a] + 7) / 8;
+  }
+  const long nbk = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
+  BinBuffers bb{};
+  bb.counts = o.alloc<int>(nbk + 1);
+  bb.offsets = o.alloc<int>(nbk + 1);
+  bb.cursor = o.alloc<int>(nbk);
+  bb.bucket_of = o.alloc<int>(M);
+  bb.unsorted = o.alloc<int>(M);
+  bb.sorted = o.alloc<int>(M);
+  bb.scan_tmp = o.alloc<int>(scan_tmp_size(nbk + 1));
+  std::vector<T> hg(3 * N);
+  for (long i = 0; i < 3 * N; i++) hg[i] = (T)fgrid[i];
+  T* dg = o.alloc<T>(3 * N);
+  double* dxp = o.alloc<double>(3L * M);
+  double* dtf = o.alloc<double>(3L * M);
+  if (!dg || !dxp || !dtf || !bb.scan_tmp) return selm_fail(SELM_ERR_NOMEM, "cudaMalloc failed");
+  CU(cudaMemcpy(dg, hg.data(), sizeof(T) * 3 * N, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dxp, x, sizeof(double) * 3 * M, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dtf, tf, sizeof(double) * 3 * M, cudaMemcpyHostToDevice));
+  CouplingArgs a{};
+  a.nx = dims[0];
+  a.ny = dims[1];
+  a.nz = dims[2];
+  a.lo = lo;
+  a.dx = dx;
+  a.M = M;
+  CU(bin_particles(dxp, M, bs, bb, o.st));
+  CU(spread_gather<T>(dg, true, dxp, dtf, bs, bb.offsets, bb.sorted, a, o.st));
+  CU(cudaStreamSynchronize(o.st));
+  CU(cudaMemcpy(hg.data(), dg, sizeof(T) * 3 * N, cudaMemcpyDeviceToHost));
+  for (long i = 0; i < 3 * N; i++) fgrid[i] = (double)hg[i];
+  return SELM_OK;
+}
+
+template <typename T> int op_fft(const int dims[3], const double* in, double* out, bool forward) {
+  using C = cpx<T>;
+  OpScope o;
+  CU(cudaStreamCreate(&o.st));
+  const long N = (long)dims[0] * dims[1] * dims[2];
+  const long N2 = (long)(dims[0] / 2 + 1) * dims[1] * dims[2];
+  FftTables<T> tb;
+  if (make_tables<T>(o.allocs, dims, tb)) return selm_fail(SELM_ERR_CUDA, "FFT tables");
+  T* dr = o.alloc<T>(N);
+  C* dc = o.alloc<C>(N2);
+  if (!dr || !dc) return selm_fail(SELM_ERR_NOMEM, "cudaMalloc failed");
+  if (forward) {
+    std::vector<T> h(N);
+    for (long i = 0; i < N; i++) h[i] = (T)in[i];
+    CU(cudaMemcpy(dr, h.data(), sizeof(T) * N, cudaMemcpyHostToDevice));
+    CU(fft3_r2c<T>(dr, dc, dims[0], dims[1], dims[2], 1, tb, o.st));
+    CU(cudaStreamSynchronize(o.st));
+    std::vector<C> hc(N2);
+    CU(cudaMemcpy(hc.data(), dc, sizeof(C) * N2, cudaMemcpyDeviceToHost));
+    for (long i = 0; i < N2; i++) {
+      out[2 * i] = hc[i].x;
+      out[2 * i + 1] = hc[i].y;
+    }
+  } else {
+    std::vector<C> hc(N2);
+    for (long i = 0; i < N2; i++) {
+      hc[i].x = (T)in[2 * i];
+      hc[i].y = (T)in[2 * i + 1];
+    }
+    CU(cudaMemcpy(dc, hc.data(), sizeof(C) * N2, cudaMemcpyHostToDevice));
+    CU(fft3_c2r<T>(dc, dr, dims[0], dims[1], dims[2], 1, T(1), tb, o.st));
+    CU(cudaStreamSynchronize(o.st));
+    std::vector<T> h(N);
+    CU(cudaMemcpy(h.data(), dr, sizeof(T) * N, cudaMemcpyDeviceToHost));
+    for (long i = 0; i < N; i++) out[i] = (double)h[i];
+  }
+  return SELM_OK;
+}
+}  // namespace
+
+extern "C" int selm_op_interp(int precision, const int dims[3], double lo, double dx, const double* u, int M,
+                              const double* x, double* out) {
+  int rc = check_dims(dims);
+  if (rc) return rc;
+  if (M < 0 || (M > 0 && (!u || !x || !out))) return selm_fail(SELM_ERR_INVALID, "bad arrays");
+  if (M == 0) return SELM_OK;
+  if (precision == 64) return op_interp<double>(dims, lo, dx, u, M, x, out);
+  if (precision == 32) return op_interp<float>(dims, lo, dx, u, M, x, out);
+  return selm_fail(SELM_ERR_INVALID, "precision must be 64 or 32");
+}
+
+extern "C" int selm_op_spread(int precision, const int dims[3], double lo, double dx, double* fgrid, int M,
+                              const double* x, const double* tf) {
+  int rc = check_dims(dims);
+  if (rc) return rc;
+  if (M < 0 || !fgrid || (M > 0 && (!x || !tf))) return selm_fail(SELM_ERR_INVALID, "bad arrays");
+  if (M == 0) return SELM_OK;
+  if (precision == 64) return op_spread<double>(dims, lo, dx, fgrid, M, x, tf);
+  if (precision == 32) return op_spread<float>(dims, lo, dx, fgrid, M, x, tf);
+  return selm_fail(SELM_ERR_INVALID, "precision must be 64 or 32");
+}
+
+extern "C" int selm_op_fft3_r2c(int precision, const int dims[3], const double* in, double* out) {
+  int rc = check_dims(dims);
+  if (rc) return rc;
+  if (!in || !out) return selm_fail(SELM_ERR_INVALID, "NULL buffer");
+  if (precision == 64) return op_fft<double>(dims, in, out, true);
+  if (precision == 32) return op_fft<float>(dims, in, out, true);
+  return selm_fail(SELM_ERR_INVALID, "precision must be 64 or 32");
+}
+
+extern "C" int selm_op_fft3_c2r(int precision, const int dims[3], const double* in, double* out) {
+  int rc = check_dims(dims);
+  if (rc) return rc;
+  if (!in || !out) return selm_fail(SELM_ERR_INVALID, "NULL buffer");
+  if (precision == 64) return op_fft<double>(dims, in, out, false);
+  if (precision == 32) return op_fft<float>(dims, in, out, false);
+  return selm_fail(SELM_ERR_INVALID, "precision must be 64 or 32");
+}
+
+// ================================================================ case directories
+extern "C" int selm_create_from_files(const char* case_dir, selm_sim** out) {
+  return selm_case_create(case_dir, out);
+}

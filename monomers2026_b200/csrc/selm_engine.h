@@ -1,0 +1,72 @@
+// selm_engine.h - state of one SELM simulation (internal to libselm_b200.so).
+#pragma once
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/selm_b200.h"
+#include "selm_kernels.h"
+
+struct ProfEvent {
+  std::string name;
+  cudaEvent_t a = nullptr, b = nullptr;
+  bool closed = false;
+};
+
+struct FusedState;  // spectral-form buffers (fluid_fused.cu)
+
+struct selm_sim {
+  selm_params prm{};
+  int nx = 0, ny = 0, nz = 0;
+  long N = 0, N2 = 0;
+  double lo = 0, hi = 0, dx = 0;
+  cudaStream_t st = nullptr;
+  bool own_st = false;
+  std::vector<void*> allocs;
+  // monomers (Lagrangian::d_x/d_v/d_f/d_m, cuda/SELM_Lagrangian.cuh:22-25); x double-buffered
+  int M = 0;
+  double* x[2] = {nullptr, nullptr};
+  double *v = nullptr, *f = nullptr, *m = nullptr, *tf = nullptr;
+  int cx = 0;
+  // plain-form grid (Eulerian::d_u[2], d_f, d_p, cuda/SELM_Eulerian.cuh:12-20)
+  double* u64[2] = {nullptr, nullptr};
+  double *fg64 = nullptr, *p64 = nullptr, *work64 = nullptr, *partial = nullptr, *sum = nullptr;
+  int cu = 0;
+  uint32_t* err = nullptr;
+  selm::FftTables<double> tb64{};
+  selm::FftTables<float> tb32{};
+  selm::BinSpec tiles{}, fcells{};
+  selm::BinBuffers tbb{}, fbb{};
+  bool have_topo = false;
+  selm::ForceTopo topo{};
+  selm_force_fn cb = nullptr;
+  void* cb_user = nullptr;
+  std::vector<double> hx, hv, hf;
+  uint64_t step = 0;
+  bool initialized = false;
+  FusedState* fz = nullptr;
+  // profiling
+  bool prof = false;
+  std::vector<ProfEvent> pending;
+  std::map<std::string, std::pair<double, long>> prof_acc;
+};
+
+int selm_fail(int code, const std::string& msg);
+void prof_mark(selm_sim* s, const char* name, bool begin);
+int engine_allocate_grid(selm_sim* s);
+int engine_forces(selm_sim* s);
+
+// case directory input (Model.SELM + LAMMPS script/data subset), selm_input.cpp
+int selm_case_create(const char* case_dir, selm_sim** out);
+
+// spectral (fused) form, fluid_fused.cu
+int fused_allocate(selm_sim* s);
+int fused_initial(selm_sim* s);
+int fused_step(selm_sim* s);
+int fused_get_field(selm_sim* s, int which, double* out);
+int fused_set_field(selm_sim* s, int which, const double* in);
+int fused_stream_changed(selm_sim* s);
+void fused_release(selm_sim* s);

@@ -1,0 +1,94 @@
+// selm_kernels.h - host-side launchers of the SELM device kernels (internal).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace selm {
+
+constexpr int kSumParts = 296;  // fixed number of partial sums (2 per SM)
+
+// Twiddle tables of the three axes, forward (sign -1) and backward (+1).
+template <typename T> struct FftTables {
+  FftRadix rx, ry, rz;
+  const cpx<T>*wx_f, *wx_b, *wy_f, *wy_b, *wz_f, *wz_b;
+};
+
+// ---- fluid, reference structure (FP64)
+cudaError_t plain_fluid_run(const double* u_old, double* u_new, const double* f, double* p, double2* work,
+                            double* partial, double* sum, int nx, int ny, int nz, double dx, double dt, double mu,
+                            double rho, const FftTables<double>& tb, cudaStream_t st);
+cudaError_t plain_compute_f(double* f, double2* work, int nx, int ny, int nz, double dx, double kB, double T,
+                            double dt, double mu, bool stochastic, uint64_t seed, uint64_t step, int noise_mode,
+                            const FftTables<double>& tb, cudaStream_t st);
+template <typename T>
+cudaError_t fft3_r2c(const T* in, cpx<T>* out, int nx, int ny, int nz, int ncomp, const FftTables<T>& tb,
+                     cudaStream_t st);
+template <typename T>
+cudaError_t fft3_c2r(cpx<T>* in, T* out, int nx, int ny, int nz, int ncomp, T scale, const FftTables<T>& tb,
+                     cudaStream_t st);
+
+// ---- binning (counting sort of monomers into buckets, deterministic order)
+struct BinSpec {
+  int mode;      // 0: grid tiles (cell = floor((x-lo)/dx), bucket = cell / tile), 1: cells of size L/nc
+  int n[3];      // grid points (mode 0) or cells (mode 1) per axis
+  int tile[3];   // tile extent in grid cells (mode 0), 1 in mode 1
+  int nb[3];     // buckets per axis
+  double lo, dx, L;
+};
+struct BinBuffers {
+  int* counts;    // [nbuckets + 1]
+  int* offsets;   // [nbuckets + 1]
+  int* cursor;    // [nbuckets]
+  int* bucket_of; // [M]
+  int* unsorted;  // [M]
+  int* sorted;    // [M]
+  int* scan_tmp;  // [scan_tmp_size(nbuckets)]
+};
+long scan_tmp_size(long n);
+cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBuffers& bb, cudaStream_t st);
+
+// ---- coupling and monomer update
+struct CouplingArgs {
+  int nx, ny, nz;
+  double lo, hi, dx, dt, upsilon, coef;
+  int stochastic;
+  uint64_t seed, step;
+  int M;
+};
+template <typename T>
+cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double* v, double* f, const double* m,
+                          double* tf, const int* order, const CouplingArgs& a, uint32_t* err, cudaStream_t st);
+template <typename T>
+cudaError_t interp_only(const T* u, const double* x, int M, int nx, int ny, int nz, double lo, double dx, double* out,
+                        cudaStream_t st);
+template <typename T>
+cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const double* tf, const BinSpec& bs,
+                          const int* offsets, const int* sorted, const CouplingArgs& a, cudaStream_t st);
+
+// ---- conservative forces (FP64)
+struct ForceTopo {
+  int M, ntypes;
+  const int* type;        // [M] 1-based
+  int bond_style;         // 0 none 1 harmonic 2 fene
+  const int* bond_off;    // [M+1] CSR of incident bonds
+  const int* bond_nbr;    // partner atom
+  const int* bond_typ;    // bond type
+  const double* bond_coeff;  // [ntb+1][4]
+  int angle_style;        // 0 none 1 harmonic
+  const int* ang_off;     // [M+1] CSR of incident angles
+  const int* ang_atoms;   // [nentries][4] = type, i, j, k (0-based)
+  const double* angle_coeff;  // [nta+1][2]
+  int pair_style;         // 0 none 1 lj/cut
+  const double* pair_coeff;  // [(nt+1)^2][3] eps sigma rc
+  const int* sp_off;      // [M+1] CSR of special partners
+  const int* sp_nbr;
+  const double* sp_w;     // weight per entry
+  double body[3];
+  double lo, hi;
+};
+cudaError_t compute_forces(const double* x, double* f, const ForceTopo& t, const BinSpec& cells, const int* offsets,
+                           const int* sorted, uint32_t* err, cudaStream_t st);
+
+}  // namespace selm
