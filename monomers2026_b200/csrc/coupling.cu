@@ -231,7 +231,8 @@ __global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, 
   double t_f = -a.upsilon * (vg - (double)val) * a.dt;
   if (a.stochastic) {
     double z0, z1;
-    philox_normal2(a.seed, (uint32_t)p, 4u + (uint32_t)d, a.step, z0, z1);
+    const uint64_t step = a.step_ptr ? *a.step_ptr : a.step;
+    philox_normal2(a.seed, (uint32_t)p, 4u + (uint32_t)d, step, z0, z1);
     t_f += z0 * a.coef;
   }
   tf_out[g] = t_f;

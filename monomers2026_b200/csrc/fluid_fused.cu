@@ -1,10 +1,575 @@
-// fluid_fused.cu - spectral-state fused form (placeholder until built).
-#include "selm_engine.h"
+// fluid_fused.cu - the fused spectral form of the fluid step (FP64 or FP32).
+//
+// The reference advances the velocity in real space: u* = u + (mu dt L_h u +
+// f)/rho (cuda/SELM_Kernel.cu:155-195), divergence, D2Z, Poisson solve with
+// the 7-point symbol (:3-34), Z2D, gradient correction (:119-152), mean
+// removal (:197-207), and draws the next forcing through a Z2D of the noise
+// spectrum (:37-98).  Every one of those operators is diagonal per wavevector
+// on the periodic MAC grid, so this form keeps the velocity spectrum u_hat as
+// the state and does the whole update in one pass over the spectrum:
+//
+//   u*_hat = u_hat (1 + mu dt L(k)/rho) + (F_hat + scale N X(k))/rho
+//   u_hat' = u*_hat - G(k) (D(k) . u*_hat) / L(k),   u_hat'(0) = 0
+//
+// with D_d = (e^{i th_d} - 1)/dx (forward difference), G_d = (1 - e^{-i th_d})/dx
+// (backward difference), L = D.G = sum_d 2(cos th_d - 1)/dx^2, F_hat the FFT of
+// the spread monomer impulse and X the reference's noise draw (Philox, same
+// counters as the plain form; on the x = 0 and x = Nx/2 planes the Hermitian
+// average the reference's c2r applies is taken explicitly).
+//
+// Three kernels per step, each reading and writing its data once:
+//   k_xy_forward : per (component, z) plane: x r2c (two rows per complex FFT)
+//                  then y FFT, written as the half spectrum [c][z][y][x].
+//   k_z_update   : per (y, block of W x-modes) pencil group: z FFT, the
+//                  update above against u_hat, inverse z FFT.
+//   k_xy_inverse : per plane: inverse y FFT, then x c2r (two rows per FFT),
+//                  writing u in the layout the interpolation reads.
+// Positions stay FP64, the zero mode is set exactly, and the noise amplitude
+// sqrt(2 kB T dt mu / N) * N * sqrt(lambda_h) is formed in FP64 in both forms.
+#include <cmath>
 
-int fused_allocate(selm_sim*) { return selm_fail(SELM_ERR_INVALID, "fused forms are not available in this build"); }
-int fused_initial(selm_sim*) { return selm_fail(SELM_ERR_INVALID, "fused forms are not available"); }
-int fused_step(selm_sim*) { return selm_fail(SELM_ERR_INVALID, "fused forms are not available"); }
-int fused_get_field(selm_sim*, int, double*) { return selm_fail(SELM_ERR_INVALID, "fused forms are not available"); }
-int fused_set_field(selm_sim*, int, const double*) { return selm_fail(SELM_ERR_INVALID, "fused forms are not available"); }
-int fused_stream_changed(selm_sim*) { return SELM_OK; }
-void fused_release(selm_sim*) {}
+#include "common.cuh"
+#include "selm_engine.h"
+#include "selm_kernels.h"
+
+namespace selm {
+
+struct FusedGeom {
+  int nx, ny, nz, nxh;
+  double dx, mu, rho, dt;
+  int stochastic, noise_mode, integrator;
+  uint64_t seed;
+  double noise_amp;  // sqrt(2 kB T dt mu / N) * N
+  const uint64_t* step;  // device step counter (the step being taken)
+};
+
+// ---------------------------------------------------------------- plane kernels
+// Shared memory: plane P [ny][nxh] complex + two scratch buffers of `scr`
+// complex each (line FFT ping-pong).
+template <typename T>
+__global__ void __launch_bounds__(512) k_xy_forward(const T* __restrict__ in, cpx<T>* __restrict__ out, FusedGeom g,
+                                                    FftRadix Rx, FftRadix Ry, const cpx<T>* __restrict__ wx,
+                                                    const cpx<T>* __restrict__ wy, int rows_per_chunk,
+                                                    int cols_per_chunk, int scr) {
+  using C = cpx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nx = g.nx, ny = g.ny, nxh = g.nxh;
+  C* P = reinterpret_cast<C*>(smem_raw);
+  C* A = P + (long)ny * nxh;
+  C* B = A + scr;
+  C* W = B + scr;  // twiddles: nx then ny
+  const long plane = blockIdx.x;  // c*nz + z
+  const T* src = in + plane * (long)ny * nx;
+  C* dst = out + plane * (long)ny * nxh;
+  for (int t = threadIdx.x; t < nx; t += blockDim.x) W[t] = wx[t];
+  for (int t = threadIdx.x; t < ny; t += blockDim.x) W[nx + t] = wy[t];
+  // x: pairs of real rows as one complex line
+  const int R = rows_per_chunk;
+  for (int y0 = 0; y0 < ny; y0 += 2 * R) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < R * nx; idx += blockDim.x) {
+      const int l = idx / nx, t = idx % nx;
+      const int ya = y0 + 2 * l, yb = ya + 1;
+      A[idx] = cmk<C>(ya < ny ? src[(long)ya * nx + t] : T(0), yb < ny ? src[(long)yb * nx + t] : T(0));
+    }
+    __syncthreads();
+    C* res = line_fft(A, B, W, Rx, R, nx, 1, false, -1);
+    for (int idx = threadIdx.x; idx < R * nxh; idx += blockDim.x) {
+      const int l = idx / nxh, m = idx % nxh;
+      const int ya = y0 + 2 * l, yb = ya + 1;
+      if (ya >= ny) continue;
+      const C z = res[l * nx + m];
+      const C zr = res[l * nx + (nx - m) % nx];
+      const C zc = cmk<C>(zr.x, -zr.y);
+      const C s = cadd(z, zc), d = csub(z, zc);
+      P[(long)ya * nxh + m] = cmk<C>(s.x * T(0.5), s.y * T(0.5));
+      if (yb < ny) P[(long)yb * nxh + m] = cmk<C>(d.y * T(0.5), -d.x * T(0.5));
+    }
+  }
+  // y: columns of the half spectrum
+  const int Bc = cols_per_chunk;
+  for (int c0 = 0; c0 < nxh; c0 += Bc) {
+    const int nb = min(Bc, nxh - c0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < ny * Bc; idx += blockDim.x) {
+      const int t = idx / Bc, b = idx % Bc;
+      A[idx] = (b < nb) ? P[(long)t * nxh + c0 + b] : cmk<C>(T(0), T(0));
+    }
+    __syncthreads();
+    C* res = line_fft(A, B, W + nx, Ry, Bc, 1, Bc, true, -1);
+    for (int idx = threadIdx.x; idx < ny * Bc; idx += blockDim.x) {
+      const int t = idx / Bc, b = idx % Bc;
+      if (b < nb) dst[(long)t * nxh + c0 + b] = res[idx];
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(512) k_xy_inverse(const cpx<T>* __restrict__ in, T* __restrict__ out, FusedGeom g,
+                                                    FftRadix Rx, FftRadix Ry, const cpx<T>* __restrict__ wx,
+                                                    const cpx<T>* __restrict__ wy, int rows_per_chunk,
+                                                    int cols_per_chunk, int scr) {
+  using C = cpx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nx = g.nx, ny = g.ny, nxh = g.nxh;
+  C* P = reinterpret_cast<C*>(smem_raw);
+  C* A = P + (long)ny * nxh;
+  C* B = A + scr;
+  C* W = B + scr;
+  const long plane = blockIdx.x;
+  const C* src = in + plane * (long)ny * nxh;
+  T* dst = out + plane * (long)ny * nx;
+  for (int t = threadIdx.x; t < nx; t += blockDim.x) W[t] = wx[t];
+  for (int t = threadIdx.x; t < ny; t += blockDim.x) W[nx + t] = wy[t];
+  const int Bc = cols_per_chunk;
+  for (int c0 = 0; c0 < nxh; c0 += Bc) {
+    const int nb = min(Bc, nxh - c0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < ny * Bc; idx += blockDim.x) {
+      const int t = idx / Bc, b = idx % Bc;
+      A[idx] = (b < nb) ? src[(long)t * nxh + c0 + b] : cmk<C>(T(0), T(0));
+    }
+    __syncthreads();
+    C* res = line_fft(A, B, W + nx, Ry, Bc, 1, Bc, true, +1);
+    for (int idx = threadIdx.x; idx < ny * Bc; idx += blockDim.x) {
+      const int t = idx / Bc, b = idx % Bc;
+      if (b < nb) P[(long)t * nxh + c0 + b] = res[idx];
+    }
+  }
+  // x c2r, two rows per complex line; the imaginary parts of the m = 0 and
+  // m = nx/2 entries drop out as in FFTW's c2r
+  const int R = rows_per_chunk;
+  for (int y0 = 0; y0 < ny; y0 += 2 * R) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < R * nx; idx += blockDim.x) {
+      const int l = idx / nx, m = idx % nx;
+      const int ya = y0 + 2 * l, yb = ya + 1;
+      C a = cmk<C>(T(0), T(0)), b = cmk<C>(T(0), T(0));
+      const bool edge = (m == 0) || ((nx & 1) == 0 && m == nx / 2);
+      if (ya < ny) {
+        if (m < nxh) a = P[(long)ya * nxh + m];
+        else {
+          const C h = P[(long)ya * nxh + (nx - m)];
+          a = cmk<C>(h.x, -h.y);
+        }
+        if (edge) a.y = T(0);
+      }
+      if (yb < ny) {
+        if (m < nxh) b = P[(long)yb * nxh + m];
+        else {
+          const C h = P[(long)yb * nxh + (nx - m)];
+          b = cmk<C>(h.x, -h.y);
+        }
+        if (edge) b.y = T(0);
+      }
+      A[idx] = cmk<C>(a.x - b.y, a.y + b.x);  // a + i b
+    }
+    __syncthreads();
+    C* res = line_fft(A, B, W, Rx, R, nx, 1, false, +1);
+    for (int idx = threadIdx.x; idx < R * nx; idx += blockDim.x) {
+      const int l = idx / nx, t = idx % nx;
+      const int ya = y0 + 2 * l, yb = ya + 1;
+      if (ya < ny) dst[(long)ya * nx + t] = res[idx].x;
+      if (yb < ny) dst[(long)yb * nx + t] = res[idx].y;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- z pencils + update
+// reference noise draw of one half-spectrum mode (cuda/SELM_Kernel.cu:56-79)
+__device__ __forceinline__ void noise_draw(const FusedGeom& g, uint64_t step, int i, int j, int k, double2 out[3]) {
+  const double dxsq = g.dx * g.dx;
+  double coef = (2 * (1 - cos(2 * kPi * i / g.nx)) + 2 * (1 - cos(2 * kPi * j / g.ny)) +
+                 2 * (1 - cos(2 * kPi * k / g.nz))) / dxsq;
+  coef = sqrt(coef);
+  const int k1 = (g.nz - k) % g.nz, j1 = (g.ny - j) % g.ny, i1 = (g.nx - i) % g.nx;
+  const bool selfc = !(k1 != k || j1 != j || i1 != i);
+  double re, im;
+  if (!selfc) {
+    re = coef / sqrt(2.0);
+    im = re;
+  } else {
+    re = coef;
+    im = 0.0;
+  }
+  const uint32_t q = (uint32_t)(((long)k * g.ny + j) * g.nxh + i);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    double z0, z1;
+    philox_normal2(g.seed, q, (uint32_t)d, step, z0, z1);
+    out[d] = make_double2(z0 * re, z1 * im);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_z_update(cpx<T>* __restrict__ work, cpx<T>* __restrict__ uhat, FusedGeom g,
+                                                  FftRadix Rz, const cpx<T>* __restrict__ wzf,
+                                                  const cpx<T>* __restrict__ wzb, const double* __restrict__ symx,
+                                                  const double* __restrict__ symy, const double* __restrict__ symz,
+                                                  int Wb) {
+  using C = cpx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nxh = g.nxh;
+  const int nl = 3 * Wb;  // lines: (component, x-mode in block)
+  C* A = reinterpret_cast<C*>(smem_raw);
+  C* B = A + (long)nz * nl;
+  C* Wf = B + (long)nz * nl;
+  C* Wi = Wf + nz;
+  const int nblk = (nxh + Wb - 1) / Wb;
+  const int j = blockIdx.x / nblk;
+  const int i0 = (blockIdx.x % nblk) * Wb;
+  const int wn = min(Wb, nxh - i0);
+  const long plane = (long)ny * nxh;
+  for (int t = threadIdx.x; t < nz; t += blockDim.x) {
+    Wf[t] = wzf[t];
+    Wi[t] = wzb[t];
+  }
+  for (int idx = threadIdx.x; idx < nz * nl; idx += blockDim.x) {
+    const int t = idx / nl, r = idx % nl, c = r / Wb, w = r % Wb;
+    A[idx] = (w < wn) ? work[((long)c * nz + t) * plane + (long)j * nxh + i0 + w] : cmk<C>(T(0), T(0));
+  }
+  __syncthreads();
+  C* F = line_fft(A, B, Wf, Rz, nl, 1, nl, true, -1);
+  C* other = (F == A) ? B : A;
+  const uint64_t step = *g.step;
+  const double invN = 1.0 / ((double)nx * ny * nz);
+  for (int idx = threadIdx.x; idx < nz * Wb; idx += blockDim.x) {
+    const int k = idx / Wb, w = idx % Wb;
+    if (w >= wn) continue;
+    const int i = i0 + w;
+    const long gidx = (long)k * plane + (long)j * nxh + i;  // within one component
+    // symbols (FP64): cm1 = cos(theta) - 1, sn = sin(theta)
+    const double cx = symx[2 * i], sx = symx[2 * i + 1];
+    const double cy = symy[2 * j], sy = symy[2 * j + 1];
+    const double cz = symz[2 * k], sz = symz[2 * k + 1];
+    const double idx2 = 1.0 / (g.dx * g.dx);
+    const double Lk = 2.0 * (cx + cy + cz) * idx2;  // sum_d 2(cos - 1)/dx^2 (<= 0)
+    C Fk[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) Fk[c] = F[k * nl + c * Wb + w];
+    if (g.stochastic) {
+      double2 X[3];
+      noise_draw(g, step, i, j, k, X);
+      const bool plane_edge = (i == 0) || ((nx & 1) == 0 && i == nx / 2);
+      if (plane_edge) {
+        // the c2r of the reference averages (j,k) with the conjugate of (-j,-k)
+        const int jc = (ny - j) % ny, kc = (nz - k) % nz;
+        if (jc != j || kc != k) {
+          double2 Xc[3];
+          noise_draw(g, step, i, jc, kc, Xc);
+          const double s = (g.noise_mode == 1) ? 0.7071067811865476 : 0.5;
+#pragma unroll
+          for (int c = 0; c < 3; c++) X[c] = make_double2((X[c].x + Xc[c].x) * s, (X[c].y - Xc[c].y) * s);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; c++) X[c].y = 0.0;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        Fk[c].x += (T)(g.noise_amp * X[c].x);
+        Fk[c].y += (T)(g.noise_amp * X[c].y);
+      }
+    }
+    C un[3];
+    if (i == 0 && j == 0 && k == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) un[c] = cmk<C>(T(0), T(0));
+    } else {
+      const T visc = (T)(1.0 + g.mu * g.dt * Lk / g.rho);
+      const T irho = (T)(1.0 / g.rho);
+      C us[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const C uh = uhat[(long)c * nz * plane + gidx];
+        us[c] = cmk<C>(uh.x * visc + Fk[c].x * irho, uh.y * visc + Fk[c].y * irho);
+      }
+      // D_d = (cm1 + i sn)/dx, G_d = (-cm1 + i sn)/dx
+      const T idx1 = (T)(1.0 / g.dx);
+      const C D[3] = {cmk<C>((T)cx * idx1, (T)sx * idx1), cmk<C>((T)cy * idx1, (T)sy * idx1),
+                      cmk<C>((T)cz * idx1, (T)sz * idx1)};
+      C s = cmul(D[0], us[0]);
+      s = cadd(s, cmul(D[1], us[1]));
+      s = cadd(s, cmul(D[2], us[2]));
+      const T iL = (T)(1.0 / Lk);
+      s = cmk<C>(s.x * iL, s.y * iL);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const C G = cmk<C>(-D[c].x, D[c].y);
+        un[c] = csub(us[c], cmul(G, s));
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      uhat[(long)c * nz * plane + gidx] = un[c];
+      F[k * nl + c * Wb + w] = cmk<C>(un[c].x * (T)invN, un[c].y * (T)invN);
+    }
+  }
+  __syncthreads();
+  C* res = line_fft(F, other, Wi, Rz, nl, 1, nl, true, +1);
+  for (int idx = threadIdx.x; idx < nz * nl; idx += blockDim.x) {
+    const int t = idx / nl, r = idx % nl, c = r / Wb, w = r % Wb;
+    if (w < wn) work[((long)c * nz + t) * plane + (long)j * nxh + i0 + w] = res[idx];
+  }
+}
+
+__global__ void k_step_advance(uint64_t* step) { *step += 1; }
+
+// ---------------------------------------------------------------- host side
+struct FusedPlan {
+  int rows_per_chunk, cols_per_chunk, scr, Wb;
+  size_t smem_xy, smem_z;
+  int threads_xy;
+};
+
+template <typename T> static FusedPlan plan_for(int nx, int ny, int nz) {
+  using C = cpx<T>;
+  FusedPlan p{};
+  const int nxh = nx / 2 + 1;
+  p.cols_per_chunk = (sizeof(T) == 8) ? 8 : 16;
+  p.rows_per_chunk = (sizeof(T) == 8) ? 4 : 8;
+  p.scr = std::max(p.rows_per_chunk * nx, p.cols_per_chunk * ny);
+  p.smem_xy = sizeof(C) * ((size_t)ny * nxh + 2 * (size_t)p.scr + nx + ny);
+  while (p.smem_xy > 200 * 1024 && p.cols_per_chunk > 1) {
+    p.cols_per_chunk /= 2;
+    p.rows_per_chunk = std::max(1, p.rows_per_chunk / 2);
+    p.scr = std::max(p.rows_per_chunk * nx, p.cols_per_chunk * ny);
+    p.smem_xy = sizeof(C) * ((size_t)ny * nxh + 2 * (size_t)p.scr + nx + ny);
+  }
+  p.Wb = (sizeof(T) == 8) ? 8 : 16;
+  p.smem_z = sizeof(C) * (2 * (size_t)nz * 3 * p.Wb + 2 * nz);
+  while (p.smem_z > 200 * 1024 && p.Wb > 1) {
+    p.Wb /= 2;
+    p.smem_z = sizeof(C) * (2 * (size_t)nz * 3 * p.Wb + 2 * nz);
+  }
+  p.threads_xy = 512;
+  return p;
+}
+
+}  // namespace selm
+
+using namespace selm;
+
+struct FusedState {
+  bool fp32 = false;
+  void* u = nullptr;      // T [3][N]
+  void* fp = nullptr;     // T [3][N] spread impulse
+  void* work = nullptr;   // C [3][nz][ny][nxh]
+  void* uhat = nullptr;   // C [3][nz][ny][nxh]
+  double *symx = nullptr, *symy = nullptr, *symz = nullptr;
+  uint64_t* d_step = nullptr;
+  FusedPlan plan{};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_ok = false;
+};
+
+#define CUF(x)                                                                                  \
+  do {                                                                                          \
+    cudaError_t e_ = (x);                                                                       \
+    if (e_ != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
+  using C = cpx<T>;
+  const long N = s->N, N2 = s->N2;
+  auto al = [&](void** p, size_t bytes) -> int {
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return selm_fail(SELM_ERR_NOMEM, "cudaMalloc failed (fused form)");
+    }
+    s->allocs.push_back(*p);
+    return SELM_OK;
+  };
+  int rc;
+  if ((rc = al(&z->u, sizeof(T) * 3 * N))) return rc;
+  if ((rc = al(&z->fp, sizeof(T) * 3 * N))) return rc;
+  if ((rc = al(&z->work, sizeof(C) * 3 * N2))) return rc;
+  if ((rc = al(&z->uhat, sizeof(C) * 3 * N2))) return rc;
+  if ((rc = al((void**)&z->symx, sizeof(double) * 2 * s->nx))) return rc;
+  if ((rc = al((void**)&z->symy, sizeof(double) * 2 * s->ny))) return rc;
+  if ((rc = al((void**)&z->symz, sizeof(double) * 2 * s->nz))) return rc;
+  if ((rc = al((void**)&z->d_step, sizeof(uint64_t)))) return rc;
+  CUF(cudaMemset(z->u, 0, sizeof(T) * 3 * N));
+  CUF(cudaMemset(z->uhat, 0, sizeof(C) * 3 * N2));
+  CUF(cudaMemset(z->d_step, 0, sizeof(uint64_t)));
+  const int nn[3] = {s->nx, s->ny, s->nz};
+  double* tabs[3] = {z->symx, z->symy, z->symz};
+  for (int a = 0; a < 3; a++) {
+    std::vector<double> h(2 * nn[a]);
+    for (int t = 0; t < nn[a]; t++) {
+      const double sh = sin(M_PI * t / nn[a]);
+      h[2 * t] = -2.0 * sh * sh;                 // cos(theta) - 1
+      h[2 * t + 1] = sin(2.0 * M_PI * t / nn[a]);  // sin(theta)
+    }
+    CUF(cudaMemcpy(tabs[a], h.data(), sizeof(double) * 2 * nn[a], cudaMemcpyHostToDevice));
+  }
+  z->plan = plan_for<T>(s->nx, s->ny, s->nz);
+  CUF(cudaFuncSetAttribute((const void*)k_xy_forward<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)z->plan.smem_xy));
+  CUF(cudaFuncSetAttribute((const void*)k_xy_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)z->plan.smem_xy));
+  CUF(cudaFuncSetAttribute((const void*)k_z_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)z->plan.smem_z));
+  return SELM_OK;
+}
+
+int fused_allocate(selm_sim* s) {
+  FusedState* z = new FusedState();
+  s->fz = z;
+  z->fp32 = (s->prm.form == SELM_FORM_FUSED32);
+  return z->fp32 ? fused_alloc_t<float>(s, z) : fused_alloc_t<double>(s, z);
+}
+
+void fused_release(selm_sim* s) {
+  if (!s->fz) return;
+  if (s->fz->gexec) cudaGraphExecDestroy(s->fz->gexec);
+  if (s->fz->graph) cudaGraphDestroy(s->fz->graph);
+  delete s->fz;
+  s->fz = nullptr;
+}
+
+int fused_stream_changed(selm_sim* s) {
+  (void)s;
+  return SELM_OK;
+}
+
+static FusedGeom geom_of(selm_sim* s) {
+  FusedGeom g{};
+  g.nx = s->nx;
+  g.ny = s->ny;
+  g.nz = s->nz;
+  g.nxh = s->nx / 2 + 1;
+  g.dx = s->dx;
+  g.mu = s->prm.mu;
+  g.rho = s->prm.rho;
+  g.dt = s->prm.dt;
+  g.stochastic = s->prm.flag_stochastic;
+  g.noise_mode = s->prm.noise_mode;
+  g.integrator = s->prm.integrator;
+  g.seed = s->prm.seed;
+  const double N = (double)s->N;
+  g.noise_amp = sqrt(2 * s->prm.KB * s->prm.T * s->prm.dt * s->prm.mu / N) * N;  // cuda/SELM_Eulerian_Period.cu:141
+  g.step = s->fz->d_step;
+  return g;
+}
+
+template <typename T> static int fused_fluid_t(selm_sim* s) {
+  using C = cpx<T>;
+  FusedState* z = s->fz;
+  const FusedPlan& P = z->plan;
+  const FftTables<T>& tb = *reinterpret_cast<const FftTables<T>*>(z->fp32 ? (const void*)&s->tb32 : (const void*)&s->tb64);
+  const FusedGeom g = geom_of(s);
+  const unsigned planes = (unsigned)(3 * s->nz);
+  prof_mark(s, "xy_forward", true);
+  k_xy_forward<T><<<planes, P.threads_xy, P.smem_xy, s->st>>>((const T*)z->fp, (C*)z->work, g, tb.rx, tb.ry,
+                                                                tb.wx_f, tb.wy_f, P.rows_per_chunk,
+                                                                P.cols_per_chunk, P.scr);
+  prof_mark(s, "xy_forward", false);
+  prof_mark(s, "z_update", true);
+  const int nblk = (g.nxh + P.Wb - 1) / P.Wb;
+  k_z_update<T><<<(unsigned)(s->ny * nblk), 256, P.smem_z, s->st>>>((C*)z->work, (C*)z->uhat, g, tb.rz, tb.wz_f,
+                                                                     tb.wz_b, z->symx, z->symy, z->symz, P.Wb);
+  prof_mark(s, "z_update", false);
+  prof_mark(s, "xy_inverse", true);
+  k_xy_inverse<T><<<planes, P.threads_xy, P.smem_xy, s->st>>>((const C*)z->work, (T*)z->u, g, tb.rx, tb.ry,
+                                                                tb.wx_b, tb.wy_b, P.rows_per_chunk,
+                                                                P.cols_per_chunk, P.scr);
+  prof_mark(s, "xy_inverse", false);
+  CUF(cudaGetLastError());
+  return SELM_OK;
+}
+
+template <typename T> static int fused_step_t(selm_sim* s) {
+  FusedState* z = s->fz;
+  CouplingArgs a{};
+  a.nx = s->nx;
+  a.ny = s->ny;
+  a.nz = s->nz;
+  a.lo = s->lo;
+  a.hi = s->hi;
+  a.dx = s->dx;
+  a.dt = s->prm.dt;
+  a.upsilon = 6.0 * M_PI * 2 * s->dx * s->prm.mu;
+  a.coef = sqrt(2.0 * s->prm.KB * s->prm.T * a.upsilon * s->prm.dt);
+  a.stochastic = s->prm.flag_stochastic;
+  a.seed = s->prm.seed;
+  a.step = 0;
+  a.step_ptr = z->d_step;
+  a.M = s->M;
+  // the step being taken is (*d_step + 1): advance first
+  k_step_advance<<<1, 1, 0, s->st>>>(z->d_step);
+  double* xo = s->x[s->cx];
+  double* xn = s->x[s->cx ^ 1];
+  if (s->M > 0) {
+    prof_mark(s, "bin", true);
+    CUF(bin_particles(xo, s->M, s->tiles, s->tbb, s->st));
+    prof_mark(s, "bin", false);
+    prof_mark(s, "interp_update", true);
+    CUF(interp_update<T>((const T*)z->u, xo, xn, s->v, s->f, s->m, s->tf, s->tbb.sorted, a, s->err, s->st));
+    prof_mark(s, "interp_update", false);
+    prof_mark(s, "spread", true);
+    CUF(spread_gather<T>((T*)z->fp, false, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st));
+    prof_mark(s, "spread", false);
+  } else {
+    CUF(cudaMemsetAsync(z->fp, 0, sizeof(T) * 3 * s->N, s->st));
+  }
+  int rc = fused_fluid_t<T>(s);
+  if (rc) return rc;
+  return SELM_OK;
+}
+
+int fused_initial(selm_sim* s) {
+  FusedState* z = s->fz;
+  using std::size_t;
+  const size_t es = z->fp32 ? sizeof(float) : sizeof(double);
+  CUF(cudaMemsetAsync(z->u, 0, es * 3 * s->N, s->st));
+  CUF(cudaMemsetAsync(z->uhat, 0, 2 * es * 3 * s->N2, s->st));
+  CUF(cudaMemsetAsync(z->d_step, 0, sizeof(uint64_t), s->st));
+  return SELM_OK;
+}
+
+int fused_step(selm_sim* s) {
+  const bool f32 = s->fz->fp32;
+  // the step counter on the host mirrors the device one
+  int rc = f32 ? fused_step_t<float>(s) : fused_step_t<double>(s);
+  if (rc) return rc;
+  s->step += 1;
+  if (s->M > 0) s->cx ^= 1;
+  return engine_forces(s);
+}
+
+int fused_get_field(selm_sim* s, int which, double* out) {
+  if (which != SELM_FIELD_U)
+    return selm_fail(SELM_ERR_STATE, "the fused forms keep the forcing in the spectrum; only the velocity is readable");
+  FusedState* z = s->fz;
+  const long n = 3 * s->N;
+  if (z->fp32) {
+    std::vector<float> h(n);
+    CUF(cudaMemcpyAsync(h.data(), z->u, sizeof(float) * n, cudaMemcpyDeviceToHost, s->st));
+    CUF(cudaStreamSynchronize(s->st));
+    for (long i = 0; i < n; i++) out[i] = h[i];
+  } else {
+    CUF(cudaMemcpyAsync(out, z->u, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
+    CUF(cudaStreamSynchronize(s->st));
+  }
+  return SELM_OK;
+}
+
+int fused_set_field(selm_sim* s, int which, const double* in) {
+  if (which != SELM_FIELD_U)
+    return selm_fail(SELM_ERR_STATE, "the fused forms keep the forcing in the spectrum; only the velocity is settable");
+  FusedState* z = s->fz;
+  const long n = 3 * s->N;
+  if (z->fp32) {
+    std::vector<float> h(in, in + n);
+    CUF(cudaMemcpyAsync(z->u, h.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s->st));
+    CUF(fft3_r2c<float>((const float*)z->u, (float2*)z->uhat, s->nx, s->ny, s->nz, 3, s->tb32, s->st));
+    CUF(cudaStreamSynchronize(s->st));
+  } else {
+    CUF(cudaMemcpyAsync(z->u, in, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
+    CUF(fft3_r2c<double>((const double*)z->u, (double2*)z->uhat, s->nx, s->ny, s->nz, 3, s->tb64, s->st));
+    CUF(cudaStreamSynchronize(s->st));
+  }
+  return SELM_OK;
+}

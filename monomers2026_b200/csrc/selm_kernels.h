@@ -55,6 +55,7 @@ struct CouplingArgs {
   double lo, hi, dx, dt, upsilon, coef;
   int stochastic;
   uint64_t seed, step;
+  const uint64_t* step_ptr;  // if set, the step index is read on the device (graph replay)
   int M;
 };
 template <typename T>

@@ -106,6 +106,7 @@ class Workload:
     mass: np.ndarray
     topology: Topology
     nsteps: int
+    v: np.ndarray | None = None
 
 
 def config(idx: int, kT: float | None = None, form: str = "plain64", body: float = 0.0, nchains: int | None = None,

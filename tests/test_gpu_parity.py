@@ -81,14 +81,14 @@ def _oracle_sim(oracle, wl, stochastic=None, noise_mode=0):
     p = wl.params
     ff = oracle.ForceField(wl.topology.as_dict(), p.box_lo, p.box_hi)
     st = p.flagStochasticDriving if stochastic is None else stochastic
-    s = oracle.Sim(p.numMeshPtsPerDir, p.box_lo, p.box_hi, p.dt, p.mu, p.rho, p.KB, p.T, wl.x, wl.mass,
+    s = oracle.Sim(p.numMeshPtsPerDir, p.box_lo, p.box_hi, p.dt, p.mu, p.rho, p.KB, p.T, wl.x, wl.mass, v=wl.v,
                    stochastic=st, seed=p.SELM_Seed, noise_mode=noise_mode, ff=ff)
     s.initial()
     return s
 
 
 def _gpu_sim(wl):
-    s = Selm(wl.params, wl.x, wl.mass, topology=wl.topology)
+    s = Selm(wl.params, wl.x, wl.mass, v=wl.v, topology=wl.topology)
     s.initial()
     return s
 
@@ -109,14 +109,20 @@ def _compare_run(oracle, wl, nsteps, tol, every=1):
     return worst
 
 
+def _moving(wl, seed=3, scale=0.3):
+    # the random walk starts at the bond rest length; initial velocities make every field non-trivial
+    wl.v = np.random.default_rng(seed).normal(0.0, scale, wl.x.shape)
+    return wl
+
+
 def test_plain64_harmonic_chain_kT0(oracle):
-    wl = W.config(1, kT=0.0, grid=16)
+    wl = _moving(W.config(1, kT=0.0, grid=16))
     wl.params.flagStochasticDriving = 0
     _compare_run(oracle, wl, 40, 1e-12)
 
 
 def test_plain64_harmonic_chain_kT1_same_philox(oracle):
-    wl = W.config(1, kT=1.0, grid=16)
+    wl = _moving(W.config(1, kT=1.0, grid=16))
     wl.params.flagStochasticDriving = 1
     _compare_run(oracle, wl, 20, 1e-11)
 
@@ -182,3 +188,60 @@ def test_error_word_flags_large_displacement():
     g.initial()
     g.run(1)
     assert g.status() & 0x2
+
+
+# ---------------------------------------------------------------- fused spectral forms
+# FP64 fused: same tolerance as the plain form; FP32 fused: 1e-5 relative (velocity
+# error target of the FP32 form), positions in FP64.
+@pytest.mark.parametrize("form,tol", [("fused64", 1e-12), ("fused32", 1e-5)])
+@pytest.mark.parametrize("kT", [0.0, 1.0])
+def test_fused_harmonic_chain_vs_oracle(oracle, form, tol, kT):
+    wl = _moving(W.config(1, kT=kT, grid=16, form=form))
+    wl.params.flagStochasticDriving = int(kT > 0)
+    _compare_run(oracle, wl, 20, tol * (10 if kT > 0 else 1))
+
+
+@pytest.mark.parametrize("form,tol", [("fused64", 1e-12), ("fused32", 1e-5)])
+def test_fused_fene_wca_vs_oracle(oracle, form, tol):
+    wl = W.config(3, kT=0.0, nchains=4, length=25, grid=24, body=0.01, form=form)
+    wl.params.flagStochasticDriving = 0
+    _compare_run(oracle, wl, 20, tol)
+
+
+@pytest.mark.parametrize("grid", [30, 48])
+def test_fused64_nonpow2_grid_with_noise(oracle, grid):
+    wl = W.config(3, kT=1.0, nchains=3, length=20, grid=grid, form="fused64")
+    _compare_run(oracle, wl, 8, 1e-11)
+
+
+def test_fused64_exact_noise_mode(oracle):
+    wl = _moving(W.config(1, kT=1.0, grid=16, form="fused64"))
+    wl.params.noise_mode = "exact"
+    o = _oracle_sim(oracle, wl, noise_mode=1)
+    g = _gpu_sim(wl)
+    o.step(10)
+    g.run(10)
+    x, v, _ = g.particles()
+    assert rel(x, o.x) < 1e-11 and rel(v, o.v) < 1e-11 and rel(g.get_field(0), o.u) < 1e-11
+
+
+def test_fused_matches_plain64():
+    wl = W.config(3, kT=1.0, nchains=5, length=20, grid=32)
+    res = {}
+    for form in ("plain64", "fused64"):
+        wl.params.form = form
+        g = _gpu_sim(wl)
+        g.run(15)
+        res[form] = (g.particles()[1], g.get_field(0))
+    assert rel(res["fused64"][0], res["plain64"][0]) < 1e-11
+    assert rel(res["fused64"][1], res["plain64"][1]) < 1e-11
+
+
+def test_fused32_is_deterministic():
+    wl = W.config(3, kT=1.0, nchains=6, length=30, grid=32, form="fused32")
+    out = []
+    for _ in range(2):
+        g = _gpu_sim(wl)
+        g.run(10)
+        out.append((g.particles()[0], g.get_field(0)))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
