@@ -1,0 +1,427 @@
+#!/usr/bin/env python
+"""Benchmark of the SELM step: fluid-cell-steps/s at 128^3 with 1e5 monomers.
+
+Workload (the large single-instance configuration): 1000 FENE chains x 100
+monomers (K=30, R0=1.5, WCA sigma=eps=1) seeded as random walks in a periodic
+box L=128 on a 128^3 grid, kT=1, dt=0.005, mu=rho=1, synthetic (seeded)
+positions.  A "step" is one full SELM step: monomer binning, interpolation +
+monomer update, spreading, the fluid update (FFT, projection, viscous step,
+thermal noise), and the device conservative forces.
+
+``value`` is the FP32 fused form, whole job (all ranks), device-timed with
+CUDA events around each step (L2 flushed before every timed step, outside the
+events), max over ranks.  The plain FP64 form (reference structure) and the
+FP64 fused form are timed on the same workload beside it.  ``e2e`` is the
+same metric through the public API with host buffers: set the monomer state
+from pinned host memory, step, read the monomer state back, every step.
+
+``--impl reference`` times the reference's CPU step (the reference's own
+source built against single-rank shims when available, else the FP64 port in
+oracle/) on the host cores, one rank only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+# --------------------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [t.strip() for t in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- helpers
+def algorithmic_bytes(kernel: str, N: int, N2: int, M: int, s: int, U: int) -> float:
+    """Compulsory DRAM bytes of one launch (one job)."""
+    c = 2 * s
+    table = {
+        "xy_forward": 3 * N * s + 3 * N2 * c,
+        "z_update": 4 * 3 * N2 * c,
+        "xy_inverse": 3 * N2 * c + 3 * N * s,
+        "spread": 3 * N * s + M * (24 + 24 + 4),
+        "interp_update": 3 * U * s + M * (24 + 24 + 48 + 48 + 8 + 24 + 4),
+        "forces": M * (24 + 24),
+        "bin": M * (24 + 4 * 5),
+    }
+    return float(table.get(kernel, 0.0))
+
+
+def stencil_union(x: np.ndarray, n: int, lo: float, dx: float) -> int:
+    """Distinct grid points read by the interpolation (union of staggered 4^3 stencils)."""
+    g = (x - lo) / dx
+    pts = set()
+    keys = []
+    for d in range(3):
+        sh = np.where(np.arange(3) == d, 0.0, 0.5)
+        base = np.floor(g - sh).astype(np.int64) - 1
+        off = np.arange(4)
+        ix = (base[:, 0, None, None, None] + off[None, :, None, None]) % n
+        iy = (base[:, 1, None, None, None] + off[None, None, :, None]) % n
+        iz = (base[:, 2, None, None, None] + off[None, None, None, :]) % n
+        keys.append(((d * n + iz) * n + iy) * n + ix)
+    del pts
+    return int(np.unique(np.concatenate([k.ravel() for k in keys])).size)
+
+
+def traffic_from_profiles(kernel: str, form: str, N: int):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    e = d.get(form, {}).get(kernel)
+    if not e:
+        return None
+    return float(e["bytes_per_launch"]) * (N / float(e["cells"]))
+
+
+# --------------------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from monomers2026_b200 import _lib
+    from monomers2026_b200 import workloads as W
+    from monomers2026_b200.selm import Selm
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    wl = W.config(3, form=args.form, seed=1003 + rank)
+    p = wl.params
+    p.SELM_Seed = 1003 + rank
+    n = p.numMeshPtsPerDir[0]
+    N = n ** 3
+    N2 = (n // 2 + 1) * n * n
+    M = len(wl.mass)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def make(form):
+        wl.params.form = form
+        sim = Selm(wl.params, wl.x, wl.mass, topology=wl.topology)
+        sim.set_stream(stream.cuda_stream)
+        sim.initial()
+        return sim
+
+    def timed(sim, K, Wm):
+        for _ in range(Wm):
+            flush.zero_()
+            sim.run(1)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        l0 = lib.selm_kernel_launches()
+        for k in range(K):
+            flush.zero_()
+            ev[k][0].record(stream)
+            sim.run(1)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        launches = lib.selm_kernel_launches() - l0
+        if world > 1:
+            torch.distributed.barrier()
+        per = [a.elapsed_time(b) for a, b in ev]
+        return per, launches
+
+    def reduce_max(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- headline form, timed with clocks sampled
+    sim = make(args.form)
+    clk = Clocks(local_rank)
+    clk.start()
+    per, launches = timed(sim, args.steps, args.warmup)
+    clocks = clk.stop()
+    total_ms = reduce_max(sum(per))
+    value = world * N * args.steps / (total_ms / 1e3)
+    status = sim.status()
+
+    # ---- per-kernel times (a separate pass with CUDA events around every kernel)
+    sim.profile(True)
+    pk = max(5, min(args.steps, 20))
+    for _ in range(pk):
+        flush.zero_()
+        sim.run(1)
+    kern = {}
+    for name in ("bin", "interp_update", "spread", "xy_forward", "z_update", "xy_inverse", "forces"):
+        ms, cnt = sim.profile_read(name)
+        if cnt:
+            kern[name] = (ms / cnt, cnt // pk)
+    sim.profile(False)
+
+    # ---- end-to-end through the public API with host buffers
+    x, v, f = sim.particles()
+    xp = torch.empty((M, 3), dtype=torch.float64).pin_memory().numpy()
+    vp = torch.empty((M, 3), dtype=torch.float64).pin_memory().numpy()
+    fp = torch.empty((M, 3), dtype=torch.float64).pin_memory().numpy()
+    mp = torch.empty((M,), dtype=torch.float64).pin_memory().numpy()
+    xp[:] = x
+    vp[:] = v
+    mp[:] = wl.mass
+    import ctypes as C
+
+    dp = C.POINTER(C.c_double)
+    h = sim._h
+    ke = max(5, args.steps // 2)
+    for _ in range(2):
+        _lib.check(lib.selm_set_particles(h, M, xp.ctypes.data_as(dp), vp.ctypes.data_as(dp), mp.ctypes.data_as(dp)))
+        _lib.check(lib.selm_step(h, 1))
+        _lib.check(lib.selm_get_particles(h, xp.ctypes.data_as(dp), vp.ctypes.data_as(dp), fp.ctypes.data_as(dp)))
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        _lib.check(lib.selm_set_particles(h, M, xp.ctypes.data_as(dp), vp.ctypes.data_as(dp), mp.ctypes.data_as(dp)))
+        _lib.check(lib.selm_step(h, 1))
+        _lib.check(lib.selm_get_particles(h, xp.ctypes.data_as(dp), vp.ctypes.data_as(dp), fp.ctypes.data_as(dp)))
+    torch.cuda.synchronize()
+    e2e_s = reduce_max(time.perf_counter() - t0)
+    e2e = {"value": world * N * ke / e2e_s, "unit": "fluid-cell-steps/s", "h2d_bytes_per_step": M * (24 + 24 + 8),
+           "d2h_bytes_per_step": M * 72, "steps": ke}
+    U = stencil_union(xp, n, p.box_lo, (p.box_hi - p.box_lo) / n)
+    sim.final()
+    del sim
+
+    # ---- the other forms on the same workload
+    forms = {}
+    if not args.no_forms:
+        for form in ("plain64", "fused64"):
+            if form == args.form:
+                continue
+            s2 = make(form)
+            k2 = max(5, args.steps // 2)
+            per2, _ = timed(s2, k2, max(3, args.warmup // 2))
+            forms[form] = world * N * k2 / (reduce_max(sum(per2)) / 1e3)
+            s2.final()
+    forms[args.form] = value
+
+    # ---- roofline of the dominant kernel
+    s = 4 if args.form == "fused32" else 8
+    hbm, peak_kind = peaks()
+    dom = max(kern, key=lambda k: kern[k][0] * max(1, kern[k][1])) if kern else None
+    roof = None
+    if dom:
+        ab = algorithmic_bytes(dom, N, N2, M, s, U)
+        ach = ab / (kern[dom][0] / 1e3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "algorithmic_bytes": ab,
+                "traffic": traffic_from_profiles(dom, args.form, N)}
+
+    # ---- CPU baseline (rank 0 at N=1): the FP64 oracle port on a bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(wl, budget_s=args.cpu_seconds)
+
+    if rank == 0:
+        out = {
+            "metric": "fluid-cell-steps/s @128^3, 1e5 monomers (FP32 fused form; plain FP64 form beside it)",
+            "value": value,
+            "unit": "fluid-cell-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32" if args.form == "fused32" else "f64",
+            "data": "synthetic (seeded random-walk FENE chains)",
+            "config": {"workload": "large single instance: 1000 FENE chains x 100 monomers, L=128, 128^3 grid, "
+                                   "kT=1, dt=0.005", "grid": n, "monomers": M, "form": args.form,
+                       "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before every timed step"},
+            "latency_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
+            "forms": forms,
+            "fp32_vs_plain64": (forms[args.form] / forms["plain64"]) if "plain64" in forms else None,
+            "kernels_ms": {k: round(v[0], 5) for k, v in kern.items()},
+            "interp_union_points": U,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "status_word": status,
+        }
+        print(json.dumps(out))
+
+
+def cpu_baseline(wl, budget_s=20.0):
+    """FP64 oracle port (or the reference's own CPU code when built) on this host, single thread."""
+    from oracle import pyoracle as O
+    p = wl.params
+    ff = O.ForceField(wl.topology.as_dict(), p.box_lo, p.box_hi)
+    sim = O.Sim(p.numMeshPtsPerDir, p.box_lo, p.box_hi, p.dt, p.mu, p.rho, p.KB, p.T, wl.x, wl.mass,
+                stochastic=p.flagStochasticDriving, seed=p.SELM_Seed, ff=ff)
+    sim.initial()
+    sim.step(1)
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        sim.step(1)
+        k += 1
+        if time.perf_counter() - t0 > budget_s or k >= 50:
+            break
+    dt = time.perf_counter() - t0
+    N = int(np.prod(p.numMeshPtsPerDir))
+    return {"value": N * k / dt, "unit": "fluid-cell-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{k} full steps of the same workload (FP64 oracle port, single thread)"}
+
+
+# --------------------------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from monomers2026_b200 import workloads as W
+    wl = W.config(3)
+    p = wl.params
+    N = int(np.prod(p.numMeshPtsPerDir))
+    ref = None
+    try:
+        from oracle import refdriver  # the reference's own CPU source, built under oracle/_ref
+        ref = refdriver.available()
+    except Exception:
+        ref = None
+    if ref:
+        from oracle import refdriver
+        run = refdriver.ReferenceRun(wl)
+        kind = "reference"
+        sample = "full steps of the same workload through the reference's own CPU code (single rank)"
+    else:
+        from oracle import pyoracle as O
+        ff = O.ForceField(wl.topology.as_dict(), p.box_lo, p.box_hi)
+        run = O.Sim(p.numMeshPtsPerDir, p.box_lo, p.box_hi, p.dt, p.mu, p.rho, p.KB, p.T, wl.x, wl.mass,
+                    stochastic=p.flagStochasticDriving, seed=p.SELM_Seed, ff=ff)
+        run.initial()
+        kind = "port"
+        sample = "full steps of the same workload (FP64 oracle port, single thread)"
+    for _ in range(args.warmup):
+        run.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        run.step(1)
+    dt = time.perf_counter() - t0
+    value = N * args.steps / dt
+    out = {
+        "impl": "reference",
+        "metric": "fluid-cell-steps/s @128^3, 1e5 monomers (FP32 fused form; plain FP64 form beside it)",
+        "value": value, "unit": "fluid-cell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded random-walk FENE chains)",
+        "config": {"workload": "large single instance: 1000 FENE chains x 100 monomers, L=128, 128^3 grid, "
+                               "kT=1, dt=0.005", "grid": p.numMeshPtsPerDir[0], "monomers": len(wl.mass)},
+        "cpu_baseline": {"value": value, "unit": "fluid-cell-steps/s", "cores": 1, "kind": kind,
+                         "sample": f"{args.steps} " + sample},
+        "e2e": {"value": value, "unit": "fluid-cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="fused32", choices=["fused32", "fused64", "plain64"])
+    ap.add_argument("--no-forms", action="store_true", help="skip timing the other forms")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if args.steps > 10:
+            args.steps = 10
+        if args.warmup > 3:
+            args.warmup = 3
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -148,6 +148,9 @@ int selm_op_spread(int precision, const int dims[3], double lo, double dx, doubl
 int selm_op_fft3_r2c(int precision, const int dims[3], const double* in, double* out);
 int selm_op_fft3_c2r(int precision, const int dims[3], const double* in, double* out);
 
+/* kernels this library has launched since it was loaded (all simulations) */
+unsigned long long selm_kernel_launches(void);
+
 /* ---- errors ---- */
 const char* selm_last_error(void);
 const char* selm_version(void);

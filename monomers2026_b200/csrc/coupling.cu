@@ -139,13 +139,17 @@ static cudaError_t exclusive_scan(const int* in, int* out, long n, int* tmp, cud
   if (nb > kScanBlock) return cudaErrorInvalidValue;
   if (nb == 1) {
     k_scan_block<<<1, kScanThreads, 0, st>>>(in, out, n, nullptr);
+    count_launches(1);
     return cudaGetLastError();
   }
   int* bsum = tmp;
   int* boff = tmp + nb;
   k_scan_block<<<(unsigned)nb, kScanThreads, 0, st>>>(in, out, n, bsum);
+  count_launches(1);
   k_scan_block<<<1, kScanThreads, 0, st>>>(bsum, boff, nb, nullptr);
+  count_launches(1);
   k_scan_add<<<(unsigned)nb, 256, 0, st>>>(out, n, boff);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -153,13 +157,18 @@ cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBu
   const long nbk = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
   cudaError_t e = cudaMemsetAsync(bb.counts, 0, sizeof(int) * (nbk + 1), st);
   if (e != cudaSuccess) return e;
-  if (M > 0) k_bin_count<<<(M + 255) / 256, 256, 0, st>>>(x, M, bs, bb.bucket_of, bb.counts);
+  if (M > 0) {
+    k_bin_count<<<(M + 255) / 256, 256, 0, st>>>(x, M, bs, bb.bucket_of, bb.counts);
+    count_launches(1);
+  }
   if ((e = exclusive_scan(bb.counts, bb.offsets, nbk + 1, bb.scan_tmp, st)) != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(bb.cursor, bb.offsets, sizeof(int) * nbk, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return e;
   if (M > 0) {
     k_bin_scatter<<<(M + 255) / 256, 256, 0, st>>>(bb.bucket_of, M, bb.cursor, bb.unsorted);
+    count_launches(1);
     k_bucket_sort<<<(unsigned)((nbk * 32 + 255) / 256), 256, 0, st>>>(bb.offsets, (int)nbk, bb.unsorted, bb.sorted);
+    count_launches(1);
   }
   return cudaGetLastError();
 }
@@ -271,6 +280,7 @@ cudaError_t interp_only(const T* u, const double* x, int M, int nx, int ny, int 
                         cudaStream_t st) {
   if (M <= 0) return cudaSuccess;
   k_interp_only<T><<<(unsigned)((3L * M + 255) / 256), 256, 0, st>>>(u, x, M, nx, ny, nz, lo, dx, out);
+  count_launches(1);
   return cudaGetLastError();
 }
 template cudaError_t interp_only<double>(const double*, const double*, int, int, int, int, double, double, double*,
@@ -284,6 +294,7 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
   if (a.M <= 0) return cudaSuccess;
   const long nt = 3L * a.M;
   k_interp_update<T><<<(unsigned)((nt + 383) / 384), 384, 0, st>>>(u, x_old, x_new, v, f, m, tf, order, a, err);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -447,6 +458,7 @@ cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const 
   if (e != cudaSuccess) return e;
   k_spread_gather<T><<<ntiles, kSpreadThreads, sm, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets, sorted,
                                                         a);
+  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -465,16 +465,19 @@ template <typename T> static int fused_fluid_t(selm_sim* s) {
   k_xy_forward<T><<<planes, P.threads_xy, P.smem_xy, s->st>>>((const T*)z->fp, (C*)z->work, g, tb.rx, tb.ry,
                                                                 tb.wx_f, tb.wy_f, P.rows_per_chunk,
                                                                 P.cols_per_chunk, P.scr);
+  count_launches(1);
   prof_mark(s, "xy_forward", false);
   prof_mark(s, "z_update", true);
   const int nblk = (g.nxh + P.Wb - 1) / P.Wb;
   k_z_update<T><<<(unsigned)(s->ny * nblk), 256, P.smem_z, s->st>>>((C*)z->work, (C*)z->uhat, g, tb.rz, tb.wz_f,
                                                                      tb.wz_b, z->symx, z->symy, z->symz, P.Wb);
+  count_launches(1);
   prof_mark(s, "z_update", false);
   prof_mark(s, "xy_inverse", true);
   k_xy_inverse<T><<<planes, P.threads_xy, P.smem_xy, s->st>>>((const C*)z->work, (T*)z->u, g, tb.rx, tb.ry,
                                                                 tb.wx_b, tb.wy_b, P.rows_per_chunk,
                                                                 P.cols_per_chunk, P.scr);
+  count_launches(1);
   prof_mark(s, "xy_inverse", false);
   CUF(cudaGetLastError());
   return SELM_OK;
@@ -499,6 +502,7 @@ template <typename T> static int fused_step_t(selm_sim* s) {
   a.M = s->M;
   // the step being taken is (*d_step + 1): advance first
   k_step_advance<<<1, 1, 0, s->st>>>(z->d_step);
+  count_launches(1);
   double* xo = s->x[s->cx];
   double* xn = s->x[s->cx ^ 1];
   if (s->M > 0) {

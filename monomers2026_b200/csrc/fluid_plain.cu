@@ -284,6 +284,7 @@ cudaError_t fft3_r2c(const T* in, cpx<T>* out, int nx, int ny, int nz, int ncomp
     if ((e = set_smem<T>((const void*)k_fft_x_r2c<T>, sm)) != cudaSuccess) return e;
     const long rows = (long)ny * nz * ncomp;
     k_fft_x_r2c<T><<<(unsigned)((rows + B - 1) / B), 256, sm, st>>>(in, out, rows, tb.rx, tb.wx_f, B);
+    count_launches(1);
   }
   {  // y pass: lines (o=(c,k), i), element stride nxh
     const int B = fft_lines_per_block(ny, sizeof(C), cap);
@@ -291,6 +292,7 @@ cudaError_t fft3_r2c(const T* in, cpx<T>* out, int nx, int ny, int nz, int ncomp
     if ((e = set_smem<T>((const void*)k_fft_axis<T>, sm)) != cudaSuccess) return e;
     dim3 g((nxh + B - 1) / B, nz * ncomp);
     k_fft_axis<T><<<g, 256, sm, st>>>(out, nxh, (long)ny * nxh, nxh, tb.ry, tb.wy_f, -1, B);
+    count_launches(1);
   }
   {  // z pass: lines (o=c, i=(j,i)), element stride ny*nxh
     const int B = fft_lines_per_block(nz, sizeof(C), cap);
@@ -299,6 +301,7 @@ cudaError_t fft3_r2c(const T* in, cpx<T>* out, int nx, int ny, int nz, int ncomp
     const int ni = ny * nxh;
     dim3 g((ni + B - 1) / B, ncomp);
     k_fft_axis<T><<<g, 256, sm, st>>>(out, ni, (long)nz * ny * nxh, (long)ny * nxh, tb.rz, tb.wz_f, -1, B);
+    count_launches(1);
   }
   return cudaGetLastError();
 }
@@ -317,6 +320,7 @@ cudaError_t fft3_c2r(cpx<T>* in, T* out, int nx, int ny, int nz, int ncomp, T sc
     const int ni = ny * nxh;
     dim3 g((ni + B - 1) / B, ncomp);
     k_fft_axis<T><<<g, 256, sm, st>>>(in, ni, (long)nz * ny * nxh, (long)ny * nxh, tb.rz, tb.wz_b, +1, B);
+    count_launches(1);
   }
   {  // y pass (inverse)
     const int B = fft_lines_per_block(ny, sizeof(C), cap);
@@ -324,6 +328,7 @@ cudaError_t fft3_c2r(cpx<T>* in, T* out, int nx, int ny, int nz, int ncomp, T sc
     if ((e = set_smem<T>((const void*)k_fft_axis<T>, sm)) != cudaSuccess) return e;
     dim3 g((nxh + B - 1) / B, nz * ncomp);
     k_fft_axis<T><<<g, 256, sm, st>>>(in, nxh, (long)ny * nxh, nxh, tb.ry, tb.wy_b, +1, B);
+    count_launches(1);
   }
   {  // x pass c2r
     const int B = fft_lines_per_block(nx, sizeof(C), cap);
@@ -331,6 +336,7 @@ cudaError_t fft3_c2r(cpx<T>* in, T* out, int nx, int ny, int nz, int ncomp, T sc
     if ((e = set_smem<T>((const void*)k_fft_x_c2r<T>, sm)) != cudaSuccess) return e;
     const long rows = (long)ny * nz * ncomp;
     k_fft_x_c2r<T><<<(unsigned)((rows + B - 1) / B), 256, sm, st>>>(in, out, rows, tb.rx, tb.wx_b, B, scale);
+    count_launches(1);
   }
   return cudaGetLastError();
 }
@@ -354,17 +360,24 @@ cudaError_t plain_fluid_run(const double* u_old, double* u_new, const double* f,
   const int bs = 128;
   const unsigned g1 = (unsigned)((N + bs - 1) / bs), g2 = (unsigned)((N2 + bs - 1) / bs);
   k_u2uAsterisk<<<g1, bs, 0, st>>>(u_old, f, u_new, dx, dt, mu, rho, nx, ny, nz);
+  count_launches(1);
   k_div<<<g1, bs, 0, st>>>(u_new, p, nx, ny, nz, dx);
+  count_launches(1);
   cudaError_t e = fft3_r2c<double>(p, work, nx, ny, nz, 1, tb, st);
   if (e != cudaSuccess) return e;
   k_poisson<<<g2, bs, 0, st>>>(work, nx, ny, nz, dx);
+  count_launches(1);
   e = fft3_c2r<double>(work, p, nx, ny, nz, 1, 1.0, tb, st);
   if (e != cudaSuccess) return e;
   k_grad<<<g1, bs, 0, st>>>(p, u_new, nx, ny, nz, dx);
+  count_launches(1);
   const int nparts = kSumParts;
   k_sum_partial<<<dim3(nparts, 3), kSumThreads, 0, st>>>(u_new, N, partial);
+  count_launches(1);
   k_sum_final<<<3, kSumThreads, 0, st>>>(partial, nparts, sum);
+  count_launches(1);
   k_subtract_mean<<<g1, bs, 0, st>>>(u_new, sum, N);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -378,6 +391,7 @@ cudaError_t plain_compute_f(double* f, double2* work, int nx, int ny, int nz, do
   const long N2 = (long)(nx / 2 + 1) * ny * nz;
   const double scale = sqrt(2 * kB * T * dt * mu / N);
   k_noise_generate<<<(unsigned)((N2 + 127) / 128), 128, 0, st>>>(work, nx, ny, nz, dx, seed, step, noise_mode);
+  count_launches(1);
   return fft3_c2r<double>(work, f, nx, ny, nz, 3, scale, tb, st);
 }
 

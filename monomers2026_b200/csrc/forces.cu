@@ -134,6 +134,7 @@ cudaError_t compute_forces(const double* x, double* f, const ForceTopo& t, const
                            const int* sorted, uint32_t* err, cudaStream_t st) {
   if (t.M <= 0) return cudaSuccess;
   k_forces<<<(t.M + 127) / 128, 128, 0, st>>>(x, f, t, cells, offsets, sorted, err);
+  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -6,6 +6,7 @@
 // synchronisation inside a step, device forces instead of the LAMMPS round
 // trip.  Errors are returned as status codes (the reference prints and calls
 // exit(-1), cuda/check.cuh:6-10).
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -20,6 +21,14 @@
 using namespace selm;
 
 static thread_local std::string g_err;
+static std::atomic<unsigned long long> g_launches{0};
+
+namespace selm {
+void count_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long launches_total() { return g_launches.load(); }
+}  // namespace selm
+
+extern "C" unsigned long long selm_kernel_launches(void) { return g_launches.load(); }
 
 int selm_fail(int code, const std::string& msg) {
   g_err = msg;

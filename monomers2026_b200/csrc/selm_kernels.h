@@ -7,6 +7,10 @@
 
 namespace selm {
 
+// kernels launched by this library since load (process-wide, host side)
+void count_launches(unsigned n);
+unsigned long long launches_total();
+
 constexpr int kSumParts = 296;  // fixed number of partial sums (2 per SM)
 
 // Twiddle tables of the three axes, forward (sign -1) and backward (+1).
