@@ -240,8 +240,10 @@ extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const dou
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
   if (M < 0 || (M > 0 && (!x || !mass))) return selm_fail(SELM_ERR_INVALID, "bad particle arrays");
   if (s->M != 0 && M != s->M) return selm_fail(SELM_ERR_STATE, "monomer count is fixed once set");
+  const double L = s->hi - s->lo;
   for (long i = 0; i < 3L * M; i++)
-    if (!std::isfinite(x[i])) return selm_fail(SELM_ERR_INVALID, "non-finite position");
+    if (!std::isfinite(x[i]) || std::fabs(x[i] - s->lo) > 1e6 * L)
+      return selm_fail(SELM_ERR_INVALID, "non-finite or far out-of-box position");
   for (int i = 0; i < M; i++)
     if (!(mass[i] > 0)) return selm_fail(SELM_ERR_INVALID, "masses must be positive");
   int rc;
@@ -257,7 +259,24 @@ extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const dou
     CU(cudaMemsetAsync(s->f, 0, sizeof(double) * 3 * M, s->st));
   }
   if (M == 0) return SELM_OK;
-  CU(cudaMemcpyAsync(s->x[s->cx], x, sizeof(double) * 3 * M, cudaMemcpyHostToDevice, s->st));
+  // periodic remap as LAMMPS' Domain::pbc at setup (whole box lengths until x is in [lo, hi));
+  // positions already in the box are passed through untouched
+  const double* xs = x;
+  bool inside = true;
+  for (long i = 0; i < 3L * M && inside; i++) inside = (x[i] >= s->lo && x[i] < s->hi);
+  if (!inside) {
+    s->hx.assign(x, x + 3L * M);
+    for (double& q : s->hx) {
+      while (q < s->lo) q += L;
+      while (q >= s->hi) q -= L;
+      if (q < s->lo) q = s->lo;
+    }
+    xs = s->hx.data();
+    CU(cudaMemcpyAsync(s->x[s->cx], xs, sizeof(double) * 3 * M, cudaMemcpyHostToDevice, s->st));
+    CU(cudaStreamSynchronize(s->st));
+  } else {
+    CU(cudaMemcpyAsync(s->x[s->cx], xs, sizeof(double) * 3 * M, cudaMemcpyHostToDevice, s->st));
+  }
   if (v) CU(cudaMemcpyAsync(s->v, v, sizeof(double) * 3 * M, cudaMemcpyHostToDevice, s->st));
   else CU(cudaMemsetAsync(s->v, 0, sizeof(double) * 3 * M, s->st));
   CU(cudaMemcpyAsync(s->m, mass, sizeof(double) * M, cudaMemcpyHostToDevice, s->st));

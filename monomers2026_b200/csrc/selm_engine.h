@@ -46,6 +46,7 @@ struct selm_sim {
   void* cb_user = nullptr;
   std::vector<double> hx, hv, hf;
   uint64_t step = 0;
+  int case_nsteps = 0;  // nsteps of Model.SELM when created from a case directory
   bool initialized = false;
   FusedState* fz = nullptr;
   // profiling

@@ -1,0 +1,85 @@
+// selm_main.cpp - the selm_b200 executable: a drop-in for the reference's
+// selm_cuda (cuda/main.cu:5-12).  Run from a case directory holding
+// Model.SELM and Model.LAMMPS_script; runs nsteps and prints the timing.
+// Optional Model.SELM keys saveSkipSimulationData, writeParticalX/V/F append
+// the monomer state to particleX/V/F.dat every saveSkipSimulationData steps in
+// the reference's "%g %g %g" format (cuda/SELM_Lagrangian_LAMMPS.cu:147-175).
+// The elapsed time printed is the time of the loop (the reference prints the
+// absolute clock, cuda/SELM.cu:92).
+#include <chrono>
+#include <cstdio>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/selm_b200.h"
+
+static int key_int(const char* path, const char* key, int dflt) {
+  std::ifstream f(path);
+  std::string line;
+  int v = dflt;
+  while (std::getline(f, line)) {
+    const size_t c = line.find('#');
+    if (c != std::string::npos) line = line.substr(0, c);
+    std::istringstream is(line);
+    std::string k;
+    if ((is >> k) && k == key) is >> v;
+  }
+  return v;
+}
+
+static void append(const char* name, const std::vector<double>& a) {
+  FILE* f = fopen(name, "a");
+  if (!f) return;
+  for (size_t i = 0; i + 2 < a.size(); i += 3) fprintf(f, "%g %g %g\n", a[i], a[i + 1], a[i + 2]);
+  fclose(f);
+}
+
+int main(int argc, char** argv) {
+  const char* dir = argc > 1 ? argv[1] : ".";
+  selm_sim* s = nullptr;
+  if (selm_create_from_files(dir, &s) != SELM_OK) {
+    fprintf(stderr, "selm_b200: %s\n", selm_last_error());
+    return 1;
+  }
+  const std::string mp = std::string(dir) + "/Model.SELM";
+  const int nsteps = key_int(mp.c_str(), "nsteps", 0);
+  const int skip = key_int(mp.c_str(), "saveSkipSimulationData", 0);
+  const int wx = key_int(mp.c_str(), "writeParticalX", 0), wv = key_int(mp.c_str(), "writeParticalV", 0),
+            wf = key_int(mp.c_str(), "writeParticalF", 0);
+  int M = 0, dims[3];
+  unsigned long long st = 0;
+  selm_get_info(s, &M, dims, &st);
+  if (selm_initial(s) != SELM_OK) {
+    fprintf(stderr, "selm_b200: %s\n", selm_last_error());
+    return 1;
+  }
+  std::vector<double> x(3 * (size_t)M), v(3 * (size_t)M), f(3 * (size_t)M);
+  selm_synchronize(s);
+  const auto t0 = std::chrono::steady_clock::now();
+  int done = 0;
+  while (done < nsteps) {
+    int chunk = nsteps - done;
+    if (skip > 0) chunk = skip - (done % skip);
+    if (selm_step(s, chunk) != SELM_OK) {
+      fprintf(stderr, "selm_b200: %s\n", selm_last_error());
+      return 1;
+    }
+    done += chunk;
+    if (skip > 0 && done % skip == 0 && (wx || wv || wf)) {
+      selm_get_particles(s, x.data(), v.data(), f.data());
+      if (wf) append("particleF.dat", f);
+      if (wv) append("particleV.dat", v);
+      if (wx) append("particleX.dat", x);
+    }
+  }
+  selm_synchronize(s);
+  const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  unsigned int w = 0;
+  selm_status(s, &w);
+  printf("\nnGpu: 1\nsteps: %d\nTotal time: %fs\nTotal time average: %fs\nstatus: 0x%x\n", nsteps, el,
+         nsteps ? el / nsteps : 0.0, w);
+  selm_destroy(s);
+  return 0;
+}

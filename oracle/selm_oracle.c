@@ -729,9 +729,24 @@ static void sim_compute_f(orc_sim *s, uint64_t noise_step) {
   }
 }
 
+/* Periodic remap of the initial positions as LAMMPS' Domain::pbc does it at
+ * integrate->setup(1) (mpi/SELM_Lagrangian_LAMMPS.cpp:54): whole box lengths
+ * are added or subtracted until x is in [lo, hi). */
+static void remap_initial(orc_sim *s) {
+  const double L = s->hi - s->lo;
+  for (int i = 0; i < 3 * s->M; i++) {
+    double x = s->x[i];
+    while (x < s->lo) x += L;
+    while (x >= s->hi) x -= L;
+    if (x < s->lo) x = s->lo;
+    s->x[i] = x;
+  }
+}
+
 void orc_sim_initial(orc_sim *s) {
   const size_t N = (size_t)s->nx * s->ny * s->nz;
   s->step = 0;
+  remap_initial(s);
   memset(s->u, 0, sizeof(double) * 3 * N);
   if (s->ff) orc_forces(s->ff, s->x, s->f);
   sim_compute_f(s, 1);
