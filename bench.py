@@ -36,6 +36,11 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 HBM_FALLBACK_GBS = 6650.0
+_T0 = time.time()
+
+
+def log(msg: str) -> None:
+    print(f"[bench {time.time() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
 def peaks():
@@ -150,7 +155,9 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     lib = _lib.load()
+    log("generating the workload")
     wl = W.config(3, form=args.form, seed=1003 + rank)
+    log(f"workload ready: {len(wl.mass)} monomers")
     p = wl.params
     p.SELM_Seed = 1003 + rank
     n = p.numMeshPtsPerDir[0]
@@ -198,6 +205,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- headline form, timed with clocks sampled
     sim = make(args.form)
+    log("timed steps")
     clk = Clocks(local_rank)
     clk.start()
     per, launches = timed(sim, args.steps, args.warmup)
@@ -206,6 +214,7 @@ def run_ours(args, rank, world, local_rank):
     value = world * N * args.steps / (total_ms / 1e3)
     status = sim.status()
 
+    log(f"timed: {sum(per) / len(per):.3f} ms/step, status 0x{status:x}")
     # ---- per-kernel times (a separate pass with CUDA events around every kernel)
     sim.profile(True)
     pk = max(5, min(args.steps, 20))
@@ -219,6 +228,7 @@ def run_ours(args, rank, world, local_rank):
             kern[name] = (ms / cnt, cnt // pk)
     sim.profile(False)
 
+    log(f"kernel times: {kern}")
     # ---- end-to-end through the public API with host buffers
     x, v, f = sim.particles()
     xp = torch.empty((M, 3), dtype=torch.float64).pin_memory().numpy()
@@ -249,6 +259,7 @@ def run_ours(args, rank, world, local_rank):
     e2e_s = reduce_max(time.perf_counter() - t0)
     e2e = {"value": world * N * ke / e2e_s, "unit": "fluid-cell-steps/s", "h2d_bytes_per_step": M * (24 + 24 + 8),
            "d2h_bytes_per_step": M * 72, "steps": ke}
+    log(f"e2e: {e2e['value']:.3e} cell-steps/s")
     U = stencil_union(xp, n, p.box_lo, (p.box_hi - p.box_lo) / n)
     sim.final()
     del sim
@@ -263,6 +274,7 @@ def run_ours(args, rank, world, local_rank):
             k2 = max(5, args.steps // 2)
             per2, _ = timed(s2, k2, max(3, args.warmup // 2))
             forms[form] = world * N * k2 / (reduce_max(sum(per2)) / 1e3)
+            log(f"form {form}: {sum(per2) / k2:.3f} ms/step")
             s2.final()
     forms[args.form] = value
 
@@ -281,6 +293,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- CPU baseline (rank 0 at N=1): the FP64 oracle port on a bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        log("CPU baseline")
         cpu = cpu_baseline(wl, budget_s=args.cpu_seconds)
 
     if rank == 0:

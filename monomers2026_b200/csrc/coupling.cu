@@ -55,19 +55,54 @@ __global__ void k_bin_scatter(const int* __restrict__ bucket_of, int M, int* __r
   unsorted[pos] = p;
 }
 
-// One warp per bucket: rank of every member by monomer index.
+// One warp per bucket: rank of every member by monomer index.  Buckets with
+// more than kWarpSortMax members (dense clusters, or every monomer of a job
+// whose state went non-finite) are queued for k_bucket_sort_big instead.
+constexpr int kWarpSortMax = 256;
 __global__ void k_bucket_sort(const int* __restrict__ offsets, int nbuckets, const int* __restrict__ unsorted,
-                              int* __restrict__ sorted) {
+                              int* __restrict__ sorted, int* __restrict__ big_list, int* __restrict__ big_count) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= nbuckets) return;
   const int s = offsets[warp], e = offsets[warp + 1];
   const int n = e - s;
+  if (n > kWarpSortMax) {
+    if (lane == 0) big_list[atomicAdd(big_count, 1)] = warp;
+    return;
+  }
   for (int i = lane; i < n; i += 32) {
     const int id = unsorted[s + i];
     int rank = 0;
     for (int j = 0; j < n; j++) rank += (unsorted[s + j] < id);
     sorted[s + rank] = id;
+  }
+}
+
+// Large buckets: one block per bucket (grid-stride over the queued list),
+// members staged in shared memory when they fit.
+constexpr int kBigSortThreads = 1024, kBigSortSmem = 8192;
+__global__ void __launch_bounds__(kBigSortThreads) k_bucket_sort_big(const int* __restrict__ offsets,
+                                                                     const int* __restrict__ unsorted,
+                                                                     int* __restrict__ sorted,
+                                                                     const int* __restrict__ big_list,
+                                                                     const int* __restrict__ big_count) {
+  __shared__ int ids[kBigSortSmem];
+  const int nbig = *big_count;
+  for (int q = blockIdx.x; q < nbig; q += gridDim.x) {
+    const int b = big_list[q];
+    const int s = offsets[b], n = offsets[b + 1] - s;
+    const bool staged = n <= kBigSortSmem;
+    __syncthreads();
+    if (staged)
+      for (int i = threadIdx.x; i < n; i += blockDim.x) ids[i] = unsorted[s + i];
+    __syncthreads();
+    const int* src = staged ? ids : unsorted + s;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int id = src[i];
+      int rank = 0;
+      for (int j = 0; j < n; j++) rank += (src[j] < id);
+      sorted[s + rank] = id;
+    }
   }
 }
 
@@ -167,7 +202,11 @@ cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBu
   if (M > 0) {
     k_bin_scatter<<<(M + 255) / 256, 256, 0, st>>>(bb.bucket_of, M, bb.cursor, bb.unsorted);
     count_launches(1);
-    k_bucket_sort<<<(unsigned)((nbk * 32 + 255) / 256), 256, 0, st>>>(bb.offsets, (int)nbk, bb.unsorted, bb.sorted);
+    if ((e = cudaMemsetAsync(bb.big_count, 0, sizeof(int), st)) != cudaSuccess) return e;
+    k_bucket_sort<<<(unsigned)((nbk * 32 + 255) / 256), 256, 0, st>>>(bb.offsets, (int)nbk, bb.unsorted, bb.sorted,
+                                                                      bb.big_list, bb.big_count);
+    count_launches(1);
+    k_bucket_sort_big<<<148, kBigSortThreads, 0, st>>>(bb.offsets, bb.unsorted, bb.sorted, bb.big_list, bb.big_count);
     count_launches(1);
   }
   return cudaGetLastError();

@@ -233,6 +233,8 @@ static int alloc_bins(selm_sim* s, const BinSpec& bs, BinBuffers& bb, int M) {
   if ((rc = dalloc(s, &bb.unsorted, M))) return rc;
   if ((rc = dalloc(s, &bb.sorted, M))) return rc;
   if ((rc = dalloc(s, &bb.scan_tmp, scan_tmp_size(nbk + 1)))) return rc;
+  if ((rc = dalloc(s, &bb.big_list, nbk))) return rc;
+  if ((rc = dalloc(s, &bb.big_count, 1))) return rc;
   return SELM_OK;
 }
 
@@ -756,6 +758,8 @@ template <typename T> int op_spread(const int dims[3], double lo, double dx, dou
   bb.unsorted = o.alloc<int>(M);
   bb.sorted = o.alloc<int>(M);
   bb.scan_tmp = o.alloc<int>(scan_tmp_size(nbk + 1));
+  bb.big_list = o.alloc<int>(nbk);
+  bb.big_count = o.alloc<int>(1);
   std::vector<T> hg(3 * N);
   for (long i = 0; i < 3 * N; i++) hg[i] = (T)fgrid[i];
   T* dg = o.alloc<T>(3 * N);

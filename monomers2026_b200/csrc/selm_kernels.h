@@ -49,6 +49,8 @@ struct BinBuffers {
   int* unsorted;  // [M]
   int* sorted;    // [M]
   int* scan_tmp;  // [scan_tmp_size(nbuckets)]
+  int* big_list;  // [nbuckets] buckets too large for one warp
+  int* big_count; // [1]
 };
 long scan_tmp_size(long n);
 cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBuffers& bb, cudaStream_t st);

@@ -52,23 +52,41 @@ def random_walk_chains(nchains: int, length: int, L: float, lo: float, rng: np.r
 
     i = 0
     for c in range(nchains):
-        while True:
-            p0 = lo + rng.random(3) * L
-            if ok(p0):
-                break
-        add(i, p0)
-        prev = x[i].copy()
-        i += 1
-        for _ in range(1, length):
-            for t in range(max_tries):
-                d = rng.standard_normal(3)
-                d *= step / np.linalg.norm(d)
-                p = prev + d
-                if ok(lo + np.mod(p - lo, L)) or t == max_tries - 1:
+        for attempt in range(200):
+            # grow the chain; if a bead cannot be placed, drop the chain and regrow it from a new origin
+            start = i
+            placed = []
+            while True:
+                p0 = lo + rng.random(3) * L
+                if ok(p0):
                     break
-            add(i, p)
-            prev = p  # unwrapped continuation keeps bond vectors exact
+            add(i, p0)
+            placed.append(i)
+            prev = x[i].copy()
             i += 1
+            stuck = False
+            for _ in range(1, length):
+                for t in range(max_tries):
+                    d = rng.standard_normal(3)
+                    d *= step / np.linalg.norm(d)
+                    p = prev + d
+                    if ok(lo + np.mod(p - lo, L)):
+                        break
+                else:
+                    stuck = True
+                    break
+                add(i, p)
+                placed.append(i)
+                prev = p  # unwrapped continuation keeps bond vectors exact
+                i += 1
+            if not stuck:
+                break
+            for q in placed:
+                if min_sep > 0:
+                    grid[key(x[q])].remove(q)
+            i = start
+        else:
+            raise RuntimeError("random_walk_chains: could not place a self-avoiding chain")
     return x
 
 

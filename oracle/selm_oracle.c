@@ -661,7 +661,8 @@ int orc_forces(const orc_ff *ff, const double *x, double *f) {
     for (int i = 0; i < M; i++) {
       int c3[3];
       for (int d = 0; d < 3; d++) {
-        int c = (int)floor((x[3 * i + d] - ff->lo) / L * nc);
+        const double q = floor((x[3 * i + d] - ff->lo) / L * nc);
+        int c = isfinite(q) && fabs(q) < 1e9 ? (int)q : 0; /* non-finite state: any cell, no overrun */
         c %= nc; if (c < 0) c += nc;
         c3[d] = c;
       }
