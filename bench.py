@@ -164,7 +164,10 @@ def run_ours(args, rank, world, local_rank):
     N = n ** 3
     N2 = (n // 2 + 1) * n * n
     M = len(wl.mass)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library runs on it and the CUDA events are recorded on it
+    # (the handle of torch's default stream is 0, which the library reads as "own stream")
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
     def make(form):
