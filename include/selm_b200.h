@@ -143,6 +143,18 @@ int selm_op_interp(int precision, const int dims[3], double lo, double dx, const
 /* lambda(): cuda/SELM_Kernel.cu:424-470; fgrid -= Lambda(tf) */
 int selm_op_spread(int precision, const int dims[3], double lo, double dx, double* fgrid, int natoms,
                    const double* x, const double* tf);
+/* The spreading operator for callers that cannot let a library allocate device
+ * memory (a host that owns the whole HBM budget through its own pool, or one
+ * that cannot afford the device synchronisation cudaMalloc/cudaFree bring).
+ * No counterpart in the reference.  Inputs and output are DEVICE pointers
+ * (fgrid is double* for precision 64, float* for 32; x and tf are [M][3]
+ * doubles); the call is ordered on `stream` (NULL = the legacy default stream).
+ * Scratch is a fixed file-scope device array: at most 65536 monomers and grids
+ * up to 128^3 (4096 tiles of 8^3); larger sizes are rejected.  Calls that
+ * overlap on the GPU share that array and race.  The first call on a device
+ * looks up the array's address; make it before any stream capture. */
+int selm_op_spread_noalloc(int precision, const int dims[3], double lo, double dx, void* fgrid, int natoms,
+                           const double* x, const double* tf, void* stream);
 /* cufftExecD2Z / cufftExecZ2D (cuda/SELM_Eulerian_Period.cu:113,117), unnormalised;
  * precision 64 or 32; half spectrum as interleaved complex doubles */
 int selm_op_fft3_r2c(int precision, const int dims[3], const double* in, double* out);

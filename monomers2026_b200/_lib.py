@@ -17,7 +17,7 @@ EXPORTED = [
     "selm_set_force_callback", "selm_initial", "selm_step", "selm_destroy", "selm_get_particles",
     "selm_get_field", "selm_set_field", "selm_get_info", "selm_status", "selm_set_stream",
     "selm_get_stream", "selm_synchronize", "selm_profile_enable", "selm_profile_read",
-    "selm_op_interp", "selm_op_spread", "selm_op_fft3_r2c", "selm_op_fft3_c2r", "selm_kernel_launches",
+    "selm_op_interp", "selm_op_spread", "selm_op_spread_noalloc", "selm_op_fft3_r2c", "selm_op_fft3_c2r", "selm_kernel_launches",
     "selm_last_error", "selm_version",
 ]
 
@@ -83,6 +83,7 @@ def load():
     L.selm_profile_read.argtypes = [vp, C.c_char_p, dp, C.POINTER(C.c_long)]
     L.selm_op_interp.argtypes = [C.c_int, ip, C.c_double, C.c_double, dp, C.c_int, dp, dp]
     L.selm_op_spread.argtypes = [C.c_int, ip, C.c_double, C.c_double, dp, C.c_int, dp, dp]
+    L.selm_op_spread_noalloc.argtypes = [C.c_int, ip, C.c_double, C.c_double, vp, C.c_int, vp, vp, vp]
     L.selm_op_fft3_r2c.argtypes = [C.c_int, ip, dp, dp]
     L.selm_op_fft3_c2r.argtypes = [C.c_int, ip, dp, dp]
     L.selm_kernel_launches.argtypes = []
