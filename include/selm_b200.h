@@ -149,8 +149,8 @@ int selm_op_spread(int precision, const int dims[3], double lo, double dx, doubl
  * No counterpart in the reference.  Inputs and output are DEVICE pointers
  * (fgrid is double* for precision 64, float* for 32; x and tf are [M][3]
  * doubles); the call is ordered on `stream` (NULL = the legacy default stream).
- * Scratch is a fixed file-scope device array: at most 65536 monomers and grids
- * up to 128^3 (4096 tiles of 8^3); larger sizes are rejected.  Calls that
+ * Scratch is a fixed file-scope device array (about 4.5 MB): at most 65536
+ * monomers and grids up to 128^3; larger sizes are rejected.  Calls that
  * overlap on the GPU share that array and race.  The first call on a device
  * looks up the array's address; make it before any stream capture. */
 int selm_op_spread_noalloc(int precision, const int dims[3], double lo, double dx, void* fgrid, int natoms,

@@ -15,6 +15,8 @@
 //                     value is summed by one thread in a fixed order.  No
 //                     floating-point atomics; results do not depend on
 //                     scheduling.
+#include <algorithm>
+
 #include "common.cuh"
 #include "selm_kernels.h"
 
@@ -45,6 +47,47 @@ __global__ void k_bin_count(const double* __restrict__ x, int M, BinSpec bs, int
   const int b = (b3[2] * bs.nb[1] + b3[1]) * bs.nb[0] + b3[0];
   bucket_of[p] = b;
   atomicAdd(&counts[b], 1);
+}
+
+// Mode 2: file a monomer under every spread tile its union stencil reaches.
+__device__ __forceinline__ int axis_tiles(double x, int a, const BinSpec& bs, int out[5]) {
+  double g = (x - bs.lo) / bs.dx;
+  if (!isfinite(g)) g = 0.0;
+  const int c0 = (int)floor(g - 0.5) - 1;
+  int cnt = 0;
+  for (int i = 0; i < 5; i++) {
+    const int t = wrapi(c0 + i, bs.n[a]) / bs.tile[a];
+    bool dup = false;
+    for (int j = 0; j < cnt; j++) dup |= (out[j] == t);
+    if (!dup) out[cnt++] = t;
+  }
+  return cnt;
+}
+
+__global__ void k_bin_count_multi(const double* __restrict__ x, int M, BinSpec bs, int* __restrict__ counts) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= M) return;
+  int tx[5], ty[5], tz[5];
+  const int nxt = axis_tiles(x[3 * p], 0, bs, tx), nyt = axis_tiles(x[3 * p + 1], 1, bs, ty),
+            nzt = axis_tiles(x[3 * p + 2], 2, bs, tz);
+  for (int k = 0; k < nzt; k++)
+    for (int j = 0; j < nyt; j++)
+      for (int i = 0; i < nxt; i++) atomicAdd(&counts[(tz[k] * bs.nb[1] + ty[j]) * bs.nb[0] + tx[i]], 1);
+}
+
+__global__ void k_bin_scatter_multi(const double* __restrict__ x, int M, BinSpec bs, int* __restrict__ cursor,
+                                    int* __restrict__ unsorted) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= M) return;
+  int tx[5], ty[5], tz[5];
+  const int nxt = axis_tiles(x[3 * p], 0, bs, tx), nyt = axis_tiles(x[3 * p + 1], 1, bs, ty),
+            nzt = axis_tiles(x[3 * p + 2], 2, bs, tz);
+  for (int k = 0; k < nzt; k++)
+    for (int j = 0; j < nyt; j++)
+      for (int i = 0; i < nxt; i++) {
+        const int pos = atomicAdd(&cursor[(tz[k] * bs.nb[1] + ty[j]) * bs.nb[0] + tx[i]], 1);
+        unsorted[pos] = p;
+      }
 }
 
 __global__ void k_bin_scatter(const int* __restrict__ bucket_of, int M, int* __restrict__ cursor,
@@ -193,14 +236,16 @@ cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBu
   cudaError_t e = cudaMemsetAsync(bb.counts, 0, sizeof(int) * (nbk + 1), st);
   if (e != cudaSuccess) return e;
   if (M > 0) {
-    k_bin_count<<<(M + 255) / 256, 256, 0, st>>>(x, M, bs, bb.bucket_of, bb.counts);
+    if (bs.mode == 2) k_bin_count_multi<<<(M + 255) / 256, 256, 0, st>>>(x, M, bs, bb.counts);
+    else k_bin_count<<<(M + 255) / 256, 256, 0, st>>>(x, M, bs, bb.bucket_of, bb.counts);
     count_launches(1);
   }
   if ((e = exclusive_scan(bb.counts, bb.offsets, nbk + 1, bb.scan_tmp, st)) != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(bb.cursor, bb.offsets, sizeof(int) * nbk, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return e;
   if (M > 0) {
-    k_bin_scatter<<<(M + 255) / 256, 256, 0, st>>>(bb.bucket_of, M, bb.cursor, bb.unsorted);
+    if (bs.mode == 2) k_bin_scatter_multi<<<(M + 255) / 256, 256, 0, st>>>(x, M, bs, bb.cursor, bb.unsorted);
+    else k_bin_scatter<<<(M + 255) / 256, 256, 0, st>>>(bb.bucket_of, M, bb.cursor, bb.unsorted);
     count_launches(1);
     if ((e = cudaMemsetAsync(bb.big_count, 0, sizeof(int), st)) != cudaSuccess) return e;
     k_bucket_sort<<<(unsigned)((nbk * 32 + 255) / 256), 256, 0, st>>>(bb.offsets, (int)nbk, bb.unsorted, bb.sorted,
@@ -338,150 +383,148 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
 }
 
 // ================================================================ spread (gather)
-constexpr int kTile = 8;
-constexpr int kSpreadThreads = 3 * kTile * kTile;  // one thread per (component, y row, z row)
-constexpr int kSpreadCap = 256;                    // staged candidates per accumulation round
+// Tiles of kTX x kTY x kTZ cells.  bin_particles (mode 2) files every monomer
+// under each tile its union stencil reaches (5 cells per axis,
+// floor(g - 1/2) - 1 .. floor(g) + 2), so a tile's bucket is exactly its list
+// of candidates, ordered by monomer index.  A block per tile stages the
+// candidates' weights in shared memory; one thread per (component, y row,
+// z row) owns a row of kTX cells and subtracts the contributions of the
+// candidates that reach it, in candidate order.
+constexpr int kTX = 16, kTY = 8, kTZ = 8;
+constexpr int kSpreadThreads = 3 * kTY * kTZ;
+constexpr int kRowPad = kTX + 1;  // odd row stride of the shared accumulators
 
 template <typename T> struct SpreadCand {
-  int rb[3][2];     // base of the 4-point stencil relative to the tile, wrapped: [axis][unshifted, shifted]
-  T w[3][2][4];     // weight factors [axis][unshifted, shifted][point]
-  T tf[3];          // impulse per component
+  int rb[3][2];                       // stencil base relative to the tile, in [0, n): [axis][unshifted, shifted]
+  T w[3][2][4];                       // weight factors [axis][unshifted, shifted][point]
+  T tf[3];                            // impulse per component
+  unsigned char ymask[2], zmask[2];   // tile rows the stencil reaches: [unshifted, shifted]
 };
 
 template <typename T>
-__device__ __forceinline__ void spread_accumulate(const SpreadCand<T>* __restrict__ cand, int ncand, int d, int ry,
-                                                  int rz, int nx, int ny, int nz, T (&acc)[kTile]) {
+__device__ __forceinline__ void spread_rows(const SpreadCand<T>* __restrict__ cand, int ncand, int d, int ry, int rz,
+                                            int nx, int ny, int nz, int extx, T* __restrict__ acc) {
   const int sx = (d == 0) ? 0 : 1, sy = (d == 1) ? 0 : 1, sz = (d == 2) ? 0 : 1;
   for (int c = 0; c < ncand; c++) {
     const SpreadCand<T>& C = cand[c];
-    int kz0 = rz - C.rb[2][sz];
-    if (kz0 < 0) kz0 += nz;
-    if (kz0 >= 4) continue;
-    int jy0 = ry - C.rb[1][sy];
-    if (jy0 < 0) jy0 += ny;
-    if (jy0 >= 4) continue;
+    if (!(((C.ymask[sy] >> ry) & (C.zmask[sz] >> rz)) & 1)) continue;
+    int jy = ry - C.rb[1][sy];
+    if (jy < 0) jy += ny;
+    int kz = rz - C.rb[2][sz];
+    if (kz < 0) kz += nz;
+    const T dj = (T(1) * C.w[2][sz][kz]) * C.w[1][sy][jy];
     const T tfd = C.tf[d];
     const int rbx = C.rb[0][sx];
-    for (int kz = kz0; kz < 4; kz += nz) {
-      const T dk = T(1) * C.w[2][sz][kz];
-      for (int jy = jy0; jy < 4; jy += ny) {
-        const T dj = dk * C.w[1][sy][jy];
 #pragma unroll
-        for (int cx = 0; cx < kTile; cx++) {
-          int ix = cx - rbx;
-          if (ix < 0) ix += nx;
-          for (; ix < 4; ix += nx) acc[cx] -= tfd * (dj * C.w[0][sx][ix]);
-        }
-      }
+    for (int ix = 0; ix < 4; ix++) {
+      int cx = rbx + ix;
+      if (cx >= nx) cx -= nx;
+      if (cx < extx) acc[cx] -= tfd * (dj * C.w[0][sx][ix]);
     }
   }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSpreadThreads) k_spread_gather(T* __restrict__ fgrid, int accumulate,
-                                                                  const double* __restrict__ x_old,
-                                                                  const double* __restrict__ tf, BinSpec bs,
-                                                                  const int* __restrict__ offsets,
-                                                                  const int* __restrict__ sorted, CouplingArgs a) {
+__global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__ fgrid, int accumulate,
+                                                                 const double* __restrict__ x_old,
+                                                                 const double* __restrict__ tf, BinSpec bs,
+                                                                 const int* __restrict__ offsets,
+                                                                 const int* __restrict__ sorted, CouplingArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SpreadCand<T>* cand = reinterpret_cast<SpreadCand<T>*>(smem_raw);
-  __shared__ int wtot[kSpreadThreads / 32];
-  __shared__ int s_ncand;
+  T* accs = reinterpret_cast<T*>(smem_raw + sizeof(SpreadCand<T>) * kSpreadThreads);
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int tb = blockIdx.x;
   const int tbx = tb % bs.nb[0], tby = (tb / bs.nb[0]) % bs.nb[1], tbz = tb / (bs.nb[0] * bs.nb[1]);
-  const int t0[3] = {tbx * kTile, tby * kTile, tbz * kTile};
-  const int ext[3] = {min(kTile, nx - t0[0]), min(kTile, ny - t0[1]), min(kTile, nz - t0[2])};
+  const int t0[3] = {tbx * kTX, tby * kTY, tbz * kTZ};
+  const int ext[3] = {min(kTX, nx - t0[0]), min(kTY, ny - t0[1]), min(kTZ, nz - t0[2])};
   const int nn[3] = {nx, ny, nz};
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  const int d = tid / (kTile * kTile), r = tid % (kTile * kTile), ry = r % kTile, rz = r / kTile;
+  const int tid = threadIdx.x;
+  const int d = tid / (kTY * kTZ), r = tid % (kTY * kTZ), ry = r % kTY, rz = r / kTY;
   const long N = (long)nx * ny * nz;
   const bool row_ok = (ry < ext[1]) && (rz < ext[2]);
   T* row = fgrid + d * N + ((long)(t0[2] + rz) * ny + (t0[1] + ry)) * nx + t0[0];
-  T acc[kTile];
+  T* acc = accs + tid * kRowPad;
+  for (int cx = 0; cx < kTX; cx++) acc[cx] = (accumulate && row_ok && cx < ext[0]) ? row[cx] : T(0);
+  const int s = offsets[tb], e = offsets[tb + 1];
+  for (int base = s; base < e; base += kSpreadThreads) {
+    const int q = base + tid;
+    if (q < e) {
+      const int p = sorted[q];
+      SpreadCand<T> c;
 #pragma unroll
-  for (int cx = 0; cx < kTile; cx++) acc[cx] = (accumulate && row_ok && cx < ext[0]) ? row[cx] : T(0);
-  if (tid == 0) s_ncand = 0;
-  __syncthreads();
-  // distinct neighbouring buckets along each axis (fewer than 3 on tiny grids)
-  int noff[3], offs[3][3];
+      for (int ax = 0; ax < 3; ax++) {
+        const double g = (x_old[3L * p + ax] - a.lo) / a.dx;
+        const double gs = g - 0.5;
+        const int b0 = (int)floor(g) - 1, b1 = (int)floor(gs) - 1;
+        c.rb[ax][0] = wrapi(b0 - t0[ax], nn[ax]);
+        c.rb[ax][1] = wrapi(b1 - t0[ax], nn[ax]);
 #pragma unroll
-  for (int ax = 0; ax < 3; ax++) {
-    const int nb = bs.nb[ax];
-    const int tcur = (ax == 0) ? tbx : (ax == 1) ? tby : tbz;
-    if (nb >= 3) {
-      noff[ax] = 3;
-      offs[ax][0] = wrapi(tcur - 1, nb); offs[ax][1] = tcur; offs[ax][2] = wrapi(tcur + 1, nb);
-    } else if (nb == 2) {
-      noff[ax] = 2;
-      offs[ax][0] = 0; offs[ax][1] = 1;
-    } else {
-      noff[ax] = 1;
-      offs[ax][0] = 0;
-    }
-  }
-  for (int oz = 0; oz < noff[2]; oz++)
-    for (int oy = 0; oy < noff[1]; oy++)
-      for (int ox = 0; ox < noff[0]; ox++) {
-        const int b = (offs[2][oz] * bs.nb[1] + offs[1][oy]) * bs.nb[0] + offs[0][ox];
-        const int s = offsets[b], e = offsets[b + 1];
-        for (int base = s; base < e; base += kSpreadThreads) {
-          const int q = base + tid;
-          bool take = false;
-          SpreadCand<T> mine;
-          if (q < e) {
-            const int p = sorted[q];
-            double g[3];
-#pragma unroll
-            for (int ax = 0; ax < 3; ax++) g[ax] = (x_old[3L * p + ax] - a.lo) / a.dx;
-            take = true;
-#pragma unroll
-            for (int ax = 0; ax < 3; ax++) {
-              const double gs = g[ax] - 0.5;
-              const int b0 = (int)floor(g[ax]) - 1, b1 = (int)floor(gs) - 1;
-              const int r0 = wrapi(b0 - t0[ax], nn[ax]), r1 = wrapi(b1 - t0[ax], nn[ax]);
-              mine.rb[ax][0] = r0;
-              mine.rb[ax][1] = r1;
-              bool hit = false;
-              for (int c = 0; c < 5; c++) hit |= (((r1 + c) % nn[ax]) < ext[ax]);
-              take = take && hit;
-#pragma unroll
-              for (int i = 0; i < 4; i++) {
-                mine.w[ax][0][i] = ref_weight<T>(fabs(g[ax] - (double)(b0 + i)));
-                mine.w[ax][1][i] = ref_weight<T>(fabs(gs - (double)(b1 + i)));
-              }
-            }
-#pragma unroll
-            for (int dd = 0; dd < 3; dd++) mine.tf[dd] = (T)tf[3L * p + dd];
-          }
-          const unsigned bal = __ballot_sync(0xffffffffu, take);
-          if (lane == 0) wtot[wid] = __popc(bal);
-          __syncthreads();
-          int wbase = 0, tot = 0;
-#pragma unroll
-          for (int w = 0; w < kSpreadThreads / 32; w++) {
-            if (w < wid) wbase += wtot[w];
-            tot += wtot[w];
-          }
-          const int n0 = s_ncand;
-          if (take) cand[n0 + wbase + __popc(bal & ((1u << lane) - 1u))] = mine;
-          __syncthreads();
-          if (tid == 0) s_ncand = n0 + tot;
-          __syncthreads();
-          if (s_ncand >= kSpreadCap) {
-            if (row_ok) spread_accumulate(cand, s_ncand, d, ry, rz, nx, ny, nz, acc);
-            __syncthreads();
-            if (tid == 0) s_ncand = 0;
-            __syncthreads();
-          }
+        for (int i = 0; i < 4; i++) {
+          c.w[ax][0][i] = ref_weight<T>(fabs(g - (double)(b0 + i)));
+          c.w[ax][1][i] = ref_weight<T>(fabs(gs - (double)(b1 + i)));
         }
       }
-  if (row_ok) spread_accumulate(cand, s_ncand, d, ry, rz, nx, ny, nz, acc);
-  if (row_ok) {
 #pragma unroll
-    for (int cx = 0; cx < kTile; cx++)
-      if (cx < ext[0]) row[cx] = acc[cx];
+      for (int sh = 0; sh < 2; sh++) {
+        unsigned ym = 0, zm = 0;
+        for (int rr = 0; rr < 8; rr++) {
+          int jy = rr - c.rb[1][sh];
+          if (jy < 0) jy += ny;
+          int kz = rr - c.rb[2][sh];
+          if (kz < 0) kz += nz;
+          ym |= (unsigned)(jy < 4 && rr < ext[1]) << rr;
+          zm |= (unsigned)(kz < 4 && rr < ext[2]) << rr;
+        }
+        c.ymask[sh] = (unsigned char)ym;
+        c.zmask[sh] = (unsigned char)zm;
+      }
+#pragma unroll
+      for (int dd = 0; dd < 3; dd++) c.tf[dd] = (T)tf[3L * p + dd];
+      cand[tid] = c;
+    }
+    __syncthreads();
+    if (row_ok) spread_rows(cand, min(kSpreadThreads, e - base), d, ry, rz, nx, ny, nz, ext[0], acc);
+    __syncthreads();
   }
+  if (row_ok)
+    for (int cx = 0; cx < ext[0]; cx++) row[cx] = acc[cx];
+}
+
+BinSpec spread_bin_spec(const int dims[3], double lo, double dx) {
+  BinSpec bs{};
+  bs.mode = 2;
+  bs.lo = lo;
+  bs.dx = dx;
+  bs.L = dx * dims[0];
+  const int t[3] = {kTX, kTY, kTZ};
+  for (int a = 0; a < 3; a++) {
+    bs.n[a] = dims[a];
+    bs.tile[a] = t[a];
+    bs.nb[a] = (dims[a] + t[a] - 1) / t[a];
+  }
+  return bs;
+}
+
+// most tiles one monomer can be filed under (product over axes of the most
+// distinct tiles 5 consecutive cells can touch)
+long spread_entries_per_monomer(const BinSpec& bs) {
+  long prod = 1;
+  for (int a = 0; a < 3; a++) {
+    int best = 1;
+    for (int c0 = 0; c0 < bs.n[a]; c0++) {
+      int tl[5], cnt = 0;
+      for (int i = 0; i < 5; i++) {
+        const int t = ((c0 + i) % bs.n[a]) / bs.tile[a];
+        bool dup = false;
+        for (int j = 0; j < cnt; j++) dup |= (tl[j] == t);
+        if (!dup) tl[cnt++] = t;
+      }
+      best = std::max(best, cnt);
+    }
+    prod *= best;
+  }
+  return prod;
 }
 
 template <typename T>
@@ -491,12 +534,12 @@ cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const 
   if (!accumulate && a.M == 0) {
     return cudaMemsetAsync(fgrid, 0, sizeof(T) * 3L * a.nx * a.ny * a.nz, st);
   }
-  const size_t sm = sizeof(SpreadCand<T>) * (kSpreadCap + kSpreadThreads);
-  cudaError_t e = cudaFuncSetAttribute((const void*)k_spread_gather<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (bs.mode != 2 || bs.tile[0] != kTX || bs.tile[1] != kTY || bs.tile[2] != kTZ) return cudaErrorInvalidValue;
+  const size_t sm = sizeof(SpreadCand<T>) * kSpreadThreads + sizeof(T) * kSpreadThreads * kRowPad;
+  cudaError_t e = cudaFuncSetAttribute((const void*)k_spread_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sm);
   if (e != cudaSuccess) return e;
-  k_spread_gather<T><<<ntiles, kSpreadThreads, sm, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets, sorted,
-                                                        a);
+  k_spread_tiles<T><<<ntiles, kSpreadThreads, sm, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets, sorted, a);
   count_launches(1);
   return cudaGetLastError();
 }

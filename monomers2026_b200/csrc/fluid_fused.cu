@@ -510,7 +510,7 @@ template <typename T> static int fused_step_t(selm_sim* s) {
     CUF(bin_particles(xo, s->M, s->tiles, s->tbb, s->st));
     prof_mark(s, "bin", false);
     prof_mark(s, "interp_update", true);
-    CUF(interp_update<T>((const T*)z->u, xo, xn, s->v, s->f, s->m, s->tf, s->tbb.sorted, a, s->err, s->st));
+    CUF(interp_update<T>((const T*)z->u, xo, xn, s->v, s->f, s->m, s->tf, nullptr, a, s->err, s->st));
     prof_mark(s, "interp_update", false);
     prof_mark(s, "spread", true);
     CUF(spread_gather<T>((T*)z->fp, false, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st));

@@ -7,13 +7,15 @@
 // cudaFree synchronise the device, which a caller stepping in a tight loop
 // cannot afford.  selm_op_spread_noalloc serves them: the caller passes
 // device buffers for the inputs and the output, and the scratch the spread
-// needs (the counting sort of monomers into 8^3-cell tiles) lives in one
+// needs (the counting sort of monomers into 16x8x8-cell spread tiles) lives in one
 // file-scope __device__ array of fixed size that every GPU loading this
 // library holds until the process exits.
 //
-// Limits: at most kNoAllocMaxAtoms monomers and kNoAllocMaxTiles tiles
-// (grids up to 128^3).  All calls share the one array, so calls whose work
-// overlaps on the GPU (different streams, no ordering between them) race on
+// Limits: at most kNoAllocMaxAtoms monomers, kNoAllocMaxTiles spread tiles
+// (grids up to 128^3) and kNoAllocEntries tile entries per monomer (a monomer
+// is filed under every tile its stencil reaches: at most 8 on grids whose
+// tiles span at least 5 cells per axis), about 4.5 MB in all.  All calls
+// share the one array, so calls whose work overlaps on the GPU (different streams, no ordering between them) race on
 // it; order them on one stream or with events.  The array keeps the last
 // call's contents; the parts that must start at zero (bucket counts, the
 // large-bucket counter) are cleared on the caller's stream by every call.
@@ -33,9 +35,12 @@ namespace {
 
 constexpr int kNoAllocMaxAtoms = 65536;
 constexpr int kNoAllocMaxTiles = 4096;
+constexpr int kNoAllocEntries = 8;
 constexpr long kScanTmp = 2 * ((kNoAllocMaxTiles + 1 + 4095) / 4096) + 2;
-// counts, offsets (nbk+1 each), cursor, big_list (nbk each), big_count, scan temp; bucket_of, unsorted, sorted (M each)
-constexpr long kScratchInts = 2L * (kNoAllocMaxTiles + 1) + 2L * kNoAllocMaxTiles + 1 + kScanTmp + 3L * kNoAllocMaxAtoms;
+// counts, offsets (nbk+1 each), cursor, big_list (nbk each), big_count, scan temp, bucket_of (M),
+// unsorted and sorted (kNoAllocEntries * M each)
+constexpr long kScratchInts = 2L * (kNoAllocMaxTiles + 1) + 2L * kNoAllocMaxTiles + 1 + kScanTmp +
+                              (1L + 2L * kNoAllocEntries) * kNoAllocMaxAtoms;
 
 static __device__ __align__(256) int g_spread_scratch[kScratchInts];
 
@@ -71,20 +76,13 @@ extern "C" int selm_op_spread_noalloc(int precision, const int dims[3], double l
   if (natoms < 0 || !fgrid || (natoms > 0 && (!x || !tf))) return selm_fail(SELM_ERR_INVALID, "bad buffers");
   if (natoms > kNoAllocMaxAtoms)
     return selm_fail(SELM_ERR_INVALID, "selm_op_spread_noalloc: more than 65536 monomers (the fixed scratch size)");
-  BinSpec bs{};
-  bs.mode = 0;
-  bs.lo = lo;
-  bs.dx = dx;
-  bs.L = dx * dims[0];
-  long nbk = 1;
-  for (int a = 0; a < 3; a++) {
-    bs.n[a] = dims[a];
-    bs.tile[a] = 8;
-    bs.nb[a] = (dims[a] + 7) / 8;
-    nbk *= bs.nb[a];
-  }
+  const BinSpec bs = spread_bin_spec(dims, lo, dx);
+  const long nbk = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
   if (nbk > kNoAllocMaxTiles)
-    return selm_fail(SELM_ERR_INVALID, "selm_op_spread_noalloc: grid needs more than 4096 tiles of 8^3 (max 128^3)");
+    return selm_fail(SELM_ERR_INVALID, "selm_op_spread_noalloc: grid needs more than 4096 spread tiles (max 128^3)");
+  const long per = spread_entries_per_monomer(bs);
+  if (per > kNoAllocEntries)
+    return selm_fail(SELM_ERR_INVALID, "selm_op_spread_noalloc: grid tiles too small for the fixed scratch");
   if (natoms == 0) return SELM_OK;
   int* base = nullptr;
   int rc = scratch_for_current_device(&base);
@@ -98,7 +96,7 @@ extern "C" int selm_op_spread_noalloc(int precision, const int dims[3], double l
   bb.big_count = q; q += 1;
   bb.scan_tmp = q; q += kScanTmp;
   bb.bucket_of = q; q += natoms;
-  bb.unsorted = q; q += natoms;
+  bb.unsorted = q; q += per * natoms;
   bb.sorted = q;
   CouplingArgs a{};
   a.nx = dims[0];

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <map>
 #include <string>
 #include <vector>
@@ -208,30 +209,22 @@ int engine_allocate_grid(selm_sim* s) {
     rc = fused_allocate(s);
     if (rc) return rc;
   }
-  // coupling tiles (8^3 cells)
-  BinSpec& t = s->tiles;
-  t.mode = 0;
-  t.lo = s->lo;
-  t.dx = s->dx;
-  t.L = s->hi - s->lo;
+  // spread tiles (monomers filed under every tile their stencils reach)
   const int nn[3] = {s->nx, s->ny, s->nz};
-  for (int a = 0; a < 3; a++) {
-    t.n[a] = nn[a];
-    t.tile[a] = 8;
-    t.nb[a] = (nn[a] + 7) / 8;
-  }
+  s->tiles = spread_bin_spec(nn, s->lo, s->dx);
   return SELM_OK;
 }
 
 static int alloc_bins(selm_sim* s, const BinSpec& bs, BinBuffers& bb, int M) {
   const long nbk = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
+  const long entries = (bs.mode == 2) ? (long)M * spread_entries_per_monomer(bs) : (long)M;
   int rc;
   if ((rc = dalloc(s, &bb.counts, nbk + 1))) return rc;
   if ((rc = dalloc(s, &bb.offsets, nbk + 1))) return rc;
   if ((rc = dalloc(s, &bb.cursor, nbk))) return rc;
   if ((rc = dalloc(s, &bb.bucket_of, M))) return rc;
-  if ((rc = dalloc(s, &bb.unsorted, M))) return rc;
-  if ((rc = dalloc(s, &bb.sorted, M))) return rc;
+  if ((rc = dalloc(s, &bb.unsorted, entries))) return rc;
+  if ((rc = dalloc(s, &bb.sorted, entries))) return rc;
   if ((rc = dalloc(s, &bb.scan_tmp, scan_tmp_size(nbk + 1)))) return rc;
   if ((rc = dalloc(s, &bb.big_list, nbk))) return rc;
   if ((rc = dalloc(s, &bb.big_count, 1))) return rc;
@@ -429,6 +422,9 @@ extern "C" int selm_set_topology(selm_sim* s, const selm_topology* tp) {
     for (size_t q = 0; q < (size_t)(nt + 1) * (nt + 1); q++) rcmax = std::max(rcmax, tp->pair_coeff[3 * q + 2]);
   const double L = s->hi - s->lo;
   int nc = rcmax > 0 ? (int)std::floor(L / rcmax) : 1;
+  // no more cells than about two per monomer: cells stay >= the cutoff, the
+  // bucket arrays stay proportional to the monomers
+  nc = std::min(nc, std::max(3, (int)std::cbrt(2.0 * M)));
   if (nc < 3) nc = 1;
   if (nc > 1024) nc = 1024;
   BinSpec& fc = s->fcells;
@@ -528,7 +524,7 @@ static int plain_step(selm_sim* s) {
     CU(bin_particles(xo, s->M, s->tiles, s->tbb, s->st));
     prof_mark(s, "bin", false);
     prof_mark(s, "interp_update", true);
-    CU(interp_update<double>(s->u64[s->cu], xo, xn, s->v, s->f, s->m, s->tf, s->tbb.sorted, a, s->err, s->st));
+    CU(interp_update<double>(s->u64[s->cu], xo, xn, s->v, s->f, s->m, s->tf, nullptr, a, s->err, s->st));
     prof_mark(s, "interp_update", false);
     prof_mark(s, "spread", true);
     CU(spread_gather<double>(s->fg64, true, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st));
@@ -739,24 +735,16 @@ template <typename T> int op_spread(const int dims[3], double lo, double dx, dou
   OpScope o;
   CU(cudaStreamCreate(&o.st));
   const long N = (long)dims[0] * dims[1] * dims[2];
-  BinSpec bs{};
-  bs.mode = 0;
-  bs.lo = lo;
-  bs.dx = dx;
-  bs.L = dx * dims[0];
-  for (int a = 0; a < 3; a++) {
-    bs.n[a] = dims[a];
-    bs.tile[a] = 8;
-    bs.nb[a] = (dims[a] + 7) / 8;
-  }
+  const BinSpec bs = spread_bin_spec(dims, lo, dx);
   const long nbk = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
+  const long entries = (long)M * spread_entries_per_monomer(bs);
   BinBuffers bb{};
   bb.counts = o.alloc<int>(nbk + 1);
   bb.offsets = o.alloc<int>(nbk + 1);
   bb.cursor = o.alloc<int>(nbk);
   bb.bucket_of = o.alloc<int>(M);
-  bb.unsorted = o.alloc<int>(M);
-  bb.sorted = o.alloc<int>(M);
+  bb.unsorted = o.alloc<int>(entries);
+  bb.sorted = o.alloc<int>(entries);
   bb.scan_tmp = o.alloc<int>(scan_tmp_size(nbk + 1));
   bb.big_list = o.alloc<int>(nbk);
   bb.big_count = o.alloc<int>(1);

@@ -35,7 +35,8 @@ cudaError_t fft3_c2r(cpx<T>* in, T* out, int nx, int ny, int nz, int ncomp, T sc
 
 // ---- binning (counting sort of monomers into buckets, deterministic order)
 struct BinSpec {
-  int mode;      // 0: grid tiles (cell = floor((x-lo)/dx), bucket = cell / tile), 1: cells of size L/nc
+  int mode;      // 0: grid tiles (cell = floor((x-lo)/dx), bucket = cell / tile), 1: cells of size L/nc,
+                 // 2: spread tiles (a monomer in every tile its union stencil reaches)
   int n[3];      // grid points (mode 0) or cells (mode 1) per axis
   int tile[3];   // tile extent in grid cells (mode 0), 1 in mode 1
   int nb[3];     // buckets per axis
@@ -53,6 +54,9 @@ struct BinBuffers {
   int* big_count; // [1]
 };
 long scan_tmp_size(long n);
+// spread tiles (mode 2): every monomer filed under each tile its stencil reaches
+BinSpec spread_bin_spec(const int dims[3], double lo, double dx);
+long spread_entries_per_monomer(const BinSpec& bs);
 cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBuffers& bb, cudaStream_t st);
 
 // ---- coupling and monomer update
