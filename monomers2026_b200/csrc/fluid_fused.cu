@@ -29,6 +29,7 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "fluid_fused_fast.cuh"
 #include "selm_engine.h"
 #include "selm_kernels.h"
 
@@ -346,6 +347,98 @@ template <typename T> static FusedPlan plan_for(int nx, int ny, int nz) {
   return p;
 }
 
+// ---------------------------------------------------------------- fast-path dispatch
+template <typename T, int N> constexpr int rows_per_chunk_fast() {
+  constexpr size_t c = sizeof(cpx<T>);
+  constexpr size_t full = c * ((size_t)N * (N / 2 + 2) + (size_t)N * (N / 2 + 1) + N);
+  return (full <= 200 * 1024 || (N % 4) != 0) ? N / 2 : N / 4;
+}
+template <typename T, int N> constexpr size_t smem_xy_fast() {
+  constexpr int RP = rows_per_chunk_fast<T, N>();
+  return sizeof(cpx<T>) * ((size_t)N * (N / 2 + 2) + (size_t)N * (RP + 1) + N);
+}
+template <typename T> constexpr int wb_fast() { return sizeof(T) == 8 ? 8 : 16; }
+template <typename T, int N> constexpr size_t smem_z_fast() {
+  return sizeof(cpx<T>) * ((size_t)N * 3 * wb_fast<T>() + N);
+}
+
+template <typename T, int N> static cudaError_t fast_attrs() {
+  cudaError_t e;
+  constexpr int RP = rows_per_chunk_fast<T, N>();
+  if ((e = cudaFuncSetAttribute((const void*)k_xy_forward_fast<T, N, RP>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xy_fast<T, N>())))
+    return e;
+  if ((e = cudaFuncSetAttribute((const void*)k_xy_inverse_fast<T, N, RP>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xy_fast<T, N>())))
+    return e;
+  return cudaFuncSetAttribute((const void*)k_z_update_fast<T, N, wb_fast<T>()>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z_fast<T, N>());
+}
+
+template <typename T, int N>
+static void fast_launch(const T* fp, cpx<T>* work, cpx<T>* uhat, T* u, const ZGeom& zg, const FftTables<T>& tb,
+                        const double* symx, const double* symy, const double* symz, int ny, int nz, cudaStream_t st,
+                        selm_sim* s) {
+  constexpr int RP = rows_per_chunk_fast<T, N>();
+  constexpr int WB = wb_fast<T>();
+  const unsigned planes = (unsigned)(3 * nz);
+  prof_mark(s, "xy_forward", true);
+  k_xy_forward_fast<T, N, RP><<<planes, 512, smem_xy_fast<T, N>(), st>>>(fp, work, tb.wx_f);
+  count_launches(1);
+  prof_mark(s, "xy_forward", false);
+  prof_mark(s, "z_update", true);
+  const int nblk = (zg.nxh + WB - 1) / WB;
+  k_z_update_fast<T, N, WB><<<(unsigned)(ny * nblk), 256, smem_z_fast<T, N>(), st>>>(work, uhat, zg, tb.wz_f, symx,
+                                                                                      symy, symz);
+  count_launches(1);
+  prof_mark(s, "z_update", false);
+  prof_mark(s, "xy_inverse", true);
+  k_xy_inverse_fast<T, N, RP><<<planes, 512, smem_xy_fast<T, N>(), st>>>(work, u, tb.wx_f);
+  count_launches(1);
+  prof_mark(s, "xy_inverse", false);
+}
+
+#define SELM_FAST_SIZES(X) X(16) X(24) X(30) X(32) X(48) X(64) X(96) X(128)
+
+static bool fast_size(int n) {
+  switch (n) {
+#define SELM_CASE(N) case N:
+    SELM_FAST_SIZES(SELM_CASE)
+#undef SELM_CASE
+    return true;
+    default:
+      return false;
+  }
+}
+
+template <typename T> static cudaError_t fast_attrs_for(int n) {
+  switch (n) {
+#define SELM_CASE(N) \
+  case N:            \
+    return fast_attrs<T, N>();
+    SELM_FAST_SIZES(SELM_CASE)
+#undef SELM_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T>
+static void fast_dispatch(int n, const T* fp, cpx<T>* work, cpx<T>* uhat, T* u, const ZGeom& zg,
+                          const FftTables<T>& tb, const double* symx, const double* symy, const double* symz, int ny,
+                          int nz, cudaStream_t st, selm_sim* s) {
+  switch (n) {
+#define SELM_CASE(N)                                                                    \
+  case N:                                                                               \
+    fast_launch<T, N>(fp, work, uhat, u, zg, tb, symx, symy, symz, ny, nz, st, s);      \
+    break;
+    SELM_FAST_SIZES(SELM_CASE)
+#undef SELM_CASE
+    default:
+      break;
+  }
+}
+
 }  // namespace selm
 
 using namespace selm;
@@ -362,6 +455,7 @@ struct FusedState {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   bool graph_ok = false;
+  bool fast = false;  // compile-time four-step kernels for this grid size
 };
 
 #define CUF(x)                                                                                  \
@@ -405,6 +499,8 @@ template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
     CUF(cudaMemcpy(tabs[a], h.data(), sizeof(double) * 2 * nn[a], cudaMemcpyHostToDevice));
   }
   z->plan = plan_for<T>(s->nx, s->ny, s->nz);
+  z->fast = fast_size(s->nx) && s->nx == s->ny && s->nx == s->nz;
+  if (z->fast) CUF(fast_attrs_for<T>(s->nx));
   CUF(cudaFuncSetAttribute((const void*)k_xy_forward<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)z->plan.smem_xy));
   CUF(cudaFuncSetAttribute((const void*)k_xy_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -461,6 +557,25 @@ template <typename T> static int fused_fluid_t(selm_sim* s) {
   const FftTables<T>& tb = *reinterpret_cast<const FftTables<T>*>(z->fp32 ? (const void*)&s->tb32 : (const void*)&s->tb64);
   const FusedGeom g = geom_of(s);
   const unsigned planes = (unsigned)(3 * s->nz);
+  if (z->fast) {
+    ZGeom zg{};
+    zg.ny = s->ny;
+    zg.nx = s->nx;
+    zg.nxh = s->nx / 2 + 1;
+    zg.dx = g.dx;
+    zg.mu = g.mu;
+    zg.rho = g.rho;
+    zg.dt = g.dt;
+    zg.noise_amp = g.noise_amp;
+    zg.stochastic = g.stochastic;
+    zg.noise_mode = g.noise_mode;
+    zg.seed = g.seed;
+    zg.step = g.step;
+    fast_dispatch<T>(s->nx, (const T*)z->fp, (C*)z->work, (C*)z->uhat, (T*)z->u, zg, tb, z->symx, z->symy, z->symz,
+                     s->ny, s->nz, s->st, s);
+    CUF(cudaGetLastError());
+    return SELM_OK;
+  }
   prof_mark(s, "xy_forward", true);
   k_xy_forward<T><<<planes, P.threads_xy, P.smem_xy, s->st>>>((const T*)z->fp, (C*)z->work, g, tb.rx, tb.ry,
                                                                 tb.wx_f, tb.wy_f, P.rows_per_chunk,

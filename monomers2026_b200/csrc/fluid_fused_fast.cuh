@@ -1,0 +1,336 @@
+// fluid_fused_fast.cuh - the fused spectral kernels for compile-time grid
+// sizes N = N1*N2 (N1, N2 <= 16), built on the four-step FFT of fft_fast.cuh.
+// Same arithmetic contract as the generic kernels of fluid_fused.cu:
+//   k_xy_forward_fast : per (component, z) plane, x r2c (two rows per complex
+//                       line) and y FFT -> half spectrum [c][z][y][x];
+//   k_z_update_fast   : per (y, block of Wb x modes): z FFT, the spectral
+//                       update (viscous factor, projection, Philox noise, zero
+//                       mode), inverse z FFT with the 1/N normalisation;
+//   k_xy_inverse_fast : inverse y FFT and x c2r, writing u.
+// Shared-memory lines are stored line-fastest (element t of line l at
+// t*stride + l), so threads of consecutive lines touch consecutive words.
+#pragma once
+#include "common.cuh"
+#include "fft_fast.cuh"
+
+namespace selm {
+
+// ---------------------------------------------------------------- helpers
+template <int N1, int N2, typename C>
+__device__ __forceinline__ void pass_a(C* s, int stride, int l, int n2, const C* tw, bool inverse_twiddle) {
+  // in place: reads x[N2 n1 + n2], writes Y at N2 k1 + n2
+  C v[N1];
+#pragma unroll
+  for (int n1 = 0; n1 < N1; n1++) v[n1] = s[(N2 * n1 + n2) * stride + l];
+  if (!inverse_twiddle) fftk::dft<N1, -1>(v);
+  else fftk::dft<N1, +1>(v);
+#pragma unroll
+  for (int k1 = 1; k1 < N1; k1++) {
+    C w = tw[n2 * k1];
+    if (inverse_twiddle) w.y = -w.y;
+    v[k1] = cmul(v[k1], w);
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < N1; k1++) s[(N2 * k1 + n2) * stride + l] = v[k1];
+}
+
+// position of natural index k after pass A + pass B (in place): N2 (k mod N1) + k / N1
+template <int N1, int N2> __device__ __forceinline__ int dpos(int k) { return N2 * (k % N1) + k / N1; }
+
+// ---------------------------------------------------------------- x/y plane kernels
+template <typename T, int N, int RP>
+__global__ void __launch_bounds__(512) k_xy_forward_fast(const T* __restrict__ in, cpx<T>* __restrict__ out,
+                                                         const cpx<T>* __restrict__ twx) {
+  using C = cpx<T>;
+  constexpr int N1 = fftk::Split<N>::N1, N2 = fftk::Split<N>::N2;
+  constexpr int NH = N / 2 + 1, NLP = NH + 1, RPP = RP + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* P = reinterpret_cast<C*>(smem_raw);  // [N rows y][NLP] : element y of line m at y*NLP + m
+  C* Ax = P + N * NLP;                    // [N][RPP]        : element x of row pair lr at x*RPP + lr
+  C* tw = Ax + N * RPP;                   // W_N^t
+  const long plane = blockIdx.x;
+  const T* src = in + plane * (long)N * N;
+  C* dst = out + plane * (long)N * NH;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twx[t];
+  for (int y0 = 0; y0 < N; y0 += 2 * RP) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < RP * N; idx += blockDim.x) {
+      const int lr = idx / N, x = idx % N;
+      const int ya = y0 + 2 * lr;
+      Ax[x * RPP + lr] = fftk::mk<C>(src[(long)ya * N + x], src[(long)(ya + 1) * N + x]);
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < RP * N2; u += blockDim.x) pass_a<N1, N2>(Ax, RPP, u % RP, u / RP, tw, false);
+    __syncthreads();
+    for (int u = threadIdx.x; u < RP * N1; u += blockDim.x) {
+      const int lr = u % RP, k1 = u / RP;
+      C v[N2];
+#pragma unroll
+      for (int n2 = 0; n2 < N2; n2++) v[n2] = Ax[(N2 * k1 + n2) * RPP + lr];
+      fftk::dft<N2, -1>(v);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; k2++) Ax[(N2 * k1 + k2) * RPP + lr] = v[k2];
+    }
+    __syncthreads();
+    // unpack two real rows: A = (Z[m] + conj Z[-m])/2, B = (Z[m] - conj Z[-m])/(2i)
+    for (int u = threadIdx.x; u < RP * NH; u += blockDim.x) {
+      const int lr = u % RP, m = u / RP;
+      const C z = Ax[dpos<N1, N2>(m) * RPP + lr];
+      const C zr = Ax[dpos<N1, N2>((N - m) % N) * RPP + lr];
+      const T sx = z.x + zr.x, sy = z.y - zr.y, dx_ = z.x - zr.x, dy = z.y + zr.y;
+      const int ya = y0 + 2 * lr;
+      P[ya * NLP + m] = fftk::mk<C>(sx * T(0.5), sy * T(0.5));
+      P[(ya + 1) * NLP + m] = fftk::mk<C>(dy * T(0.5), -dx_ * T(0.5));
+    }
+  }
+  __syncthreads();
+  for (int u = threadIdx.x; u < NH * N2; u += blockDim.x) pass_a<N1, N2>(P, NLP, u % NH, u / NH, tw, false);
+  __syncthreads();
+  for (int u = threadIdx.x; u < NH * N1; u += blockDim.x) {
+    const int m = u % NH, k1 = u / NH;
+    C v[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; n2++) v[n2] = P[(N2 * k1 + n2) * NLP + m];
+    fftk::dft<N2, -1>(v);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) dst[(long)(k1 + N1 * k2) * NH + m] = v[k2];
+  }
+}
+
+template <typename T, int N, int RP>
+__global__ void __launch_bounds__(512) k_xy_inverse_fast(const cpx<T>* __restrict__ in, T* __restrict__ out,
+                                                         const cpx<T>* __restrict__ twx) {
+  using C = cpx<T>;
+  constexpr int N1 = fftk::Split<N>::N1, N2 = fftk::Split<N>::N2;
+  constexpr int NH = N / 2 + 1, NLP = NH + 1, RPP = RP + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* P = reinterpret_cast<C*>(smem_raw);
+  C* Ax = P + N * NLP;
+  C* tw = Ax + N * RPP;
+  const long plane = blockIdx.x;
+  const C* src = in + plane * (long)N * NH;
+  T* dst = out + plane * (long)N * N;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twx[t];
+  for (int idx = threadIdx.x; idx < N * NH; idx += blockDim.x) {
+    const int ky = idx / NH, m = idx % NH;
+    P[ky * NLP + m] = src[idx];
+  }
+  __syncthreads();
+  // inverse y FFT, in place: row y ends at position dpos(y)
+  for (int u = threadIdx.x; u < NH * N2; u += blockDim.x) pass_a<N1, N2>(P, NLP, u % NH, u / NH, tw, true);
+  __syncthreads();
+  for (int u = threadIdx.x; u < NH * N1; u += blockDim.x) {
+    const int m = u % NH, k1 = u / NH;
+    C v[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; n2++) v[n2] = P[(N2 * k1 + n2) * NLP + m];
+    fftk::dft<N2, +1>(v);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) P[(N2 * k1 + k2) * NLP + m] = v[k2];
+  }
+  // x c2r, two rows per complex line; imaginary parts of m = 0 and m = N/2 drop out
+  for (int y0 = 0; y0 < N; y0 += 2 * RP) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < RP * N; idx += blockDim.x) {
+      const int lr = idx % RP, m = idx / RP;
+      const int pa = dpos<N1, N2>(y0 + 2 * lr), pb = dpos<N1, N2>(y0 + 2 * lr + 1);
+      C a, b;
+      if (m < NH) {
+        a = P[pa * NLP + m];
+        b = P[pb * NLP + m];
+      } else {
+        const C ha = P[pa * NLP + (N - m)], hb = P[pb * NLP + (N - m)];
+        a = fftk::mk<C>(ha.x, -ha.y);
+        b = fftk::mk<C>(hb.x, -hb.y);
+      }
+      if (m == 0 || ((N & 1) == 0 && m == N / 2)) {
+        a.y = T(0);
+        b.y = T(0);
+      }
+      Ax[m * RPP + lr] = fftk::mk<C>(a.x - b.y, a.y + b.x);
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < RP * N2; u += blockDim.x) pass_a<N1, N2>(Ax, RPP, u % RP, u / RP, tw, true);
+    __syncthreads();
+    for (int u = threadIdx.x; u < RP * N1; u += blockDim.x) {
+      const int k1 = u % N1, lr = u / N1;
+      C v[N2];
+#pragma unroll
+      for (int n2 = 0; n2 < N2; n2++) v[n2] = Ax[(N2 * k1 + n2) * RPP + lr];
+      fftk::dft<N2, +1>(v);
+      const int ya = y0 + 2 * lr;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; k2++) {
+        const int xx = k1 + N1 * k2;
+        dst[(long)ya * N + xx] = v[k2].x;
+        dst[(long)(ya + 1) * N + xx] = v[k2].y;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- z pencils + update
+struct ZGeom {
+  int ny, nxh, nx;
+  double dx, mu, rho, dt, noise_amp;
+  int stochastic, noise_mode;
+  uint64_t seed;
+  const uint64_t* step;
+};
+
+// reference noise draw of a half-spectrum mode (cuda/SELM_Kernel.cu:56-79); the
+// amplitude sqrt(lambda_h) comes from the symbol tables (cm = cos - 1)
+template <int N>
+__device__ __forceinline__ void noise_draw_fast(const ZGeom& g, uint64_t step, int i, int j, int k, double cmx,
+                                                double cmy, double cmz, double2 out[3]) {
+  const double lam = -2.0 * (cmx + cmy + cmz) / (g.dx * g.dx);
+  const double coef = sqrt(fmax(lam, 0.0));
+  const int k1 = (N - k) % N, j1 = (g.ny - j) % g.ny, i1 = (g.nx - i) % g.nx;
+  const bool selfc = (k1 == k && j1 == j && i1 == i);
+  const double re = selfc ? coef : coef * 0.7071067811865476;
+  const double im = selfc ? 0.0 : re;
+  const uint32_t q = (uint32_t)(((long)k * g.ny + j) * g.nxh + i);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    double z0, z1;
+    philox_normal2(g.seed, q, (uint32_t)d, step, z0, z1);
+    out[d] = make_double2(z0 * re, z1 * im);
+  }
+}
+
+template <typename T, int N, int WB>
+__global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work, cpx<T>* __restrict__ uhat, ZGeom g,
+                                                       const cpx<T>* __restrict__ twz,
+                                                       const double* __restrict__ symx,
+                                                       const double* __restrict__ symy,
+                                                       const double* __restrict__ symz) {
+  using C = cpx<T>;
+  constexpr int N1 = fftk::Split<N>::N1, N2 = fftk::Split<N>::N2;
+  constexpr int NL = 3 * WB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* A = reinterpret_cast<C*>(smem_raw);  // element t of line (c, w) at t*NL + c*WB + w
+  C* tw = A + N * NL;
+  const int nxh = g.nxh, ny = g.ny;
+  const int nblk = (nxh + WB - 1) / WB;
+  const int j = blockIdx.x / nblk;
+  const int i0 = (blockIdx.x % nblk) * WB;
+  const int wn = min(WB, nxh - i0);
+  const long plane = (long)ny * nxh;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twz[t];
+  __syncthreads();
+  // pass A forward, loading straight from global: thread (line, n2)
+  for (int u = threadIdx.x; u < NL * N2; u += blockDim.x) {
+    const int l = u % NL, n2 = u / NL;
+    const int c = l / WB, w = l % WB;
+    C v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; n1++)
+      v[n1] = (w < wn) ? work[((long)c * N + (N2 * n1 + n2)) * plane + (long)j * nxh + i0 + w] : fftk::mk<C>(T(0), T(0));
+    fftk::dft<N1, -1>(v);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) A[(N2 * k1 + n2) * NL + l] = (k1 == 0) ? v[0] : cmul(v[k1], tw[n2 * k1]);
+  }
+  __syncthreads();
+  // pass B forward, update, pass B inverse: thread (w, k1) for all three components
+  const uint64_t step = *g.step;
+  const T invN = (T)(1.0 / ((double)g.nx * ny * N));
+  for (int u = threadIdx.x; u < WB * N1; u += blockDim.x) {
+    const int w = u % WB, k1 = u / WB;
+    if (w >= wn) continue;
+    const int i = i0 + w;
+    C X[3][N2];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+#pragma unroll
+      for (int n2 = 0; n2 < N2; n2++) X[c][n2] = A[(N2 * k1 + n2) * NL + c * WB + w];
+      fftk::dft<N2, -1>(X[c]);
+    }
+    const double cx = symx[2 * i], sx = symx[2 * i + 1];
+    const double cy = symy[2 * j], sy = symy[2 * j + 1];
+    const double idx2 = 1.0 / (g.dx * g.dx);
+    const T idx1 = (T)(1.0 / g.dx);
+    const T irho = (T)(1.0 / g.rho);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) {
+      const int k = k1 + N1 * k2;
+      const long gidx = (long)k * plane + (long)j * nxh + i;
+      const double cz = symz[2 * k], sz = symz[2 * k + 1];
+      if (g.stochastic) {
+        double2 Xn[3];
+        noise_draw_fast<N>(g, step, i, j, k, cx, cy, cz, Xn);
+        if (i == 0 || ((g.nx & 1) == 0 && i == g.nx / 2)) {
+          const int jc = (ny - j) % ny, kc = (N - k) % N;
+          if (jc != j || kc != k) {
+            double2 Xc[3];
+            noise_draw_fast<N>(g, step, i, jc, kc, cx, symy[2 * jc], symz[2 * kc], Xc);
+            const double s = (g.noise_mode == 1) ? 0.7071067811865476 : 0.5;
+#pragma unroll
+            for (int c = 0; c < 3; c++) Xn[c] = make_double2((Xn[c].x + Xc[c].x) * s, (Xn[c].y - Xc[c].y) * s);
+          } else {
+#pragma unroll
+            for (int c = 0; c < 3; c++) Xn[c].y = 0.0;
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          X[c][k2].x += (T)(g.noise_amp * Xn[c].x);
+          X[c][k2].y += (T)(g.noise_amp * Xn[c].y);
+        }
+      }
+      C un[3];
+      if (i == 0 && j == 0 && k == 0) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) un[c] = fftk::mk<C>(T(0), T(0));
+      } else {
+        const double Lk = 2.0 * (cx + cy + cz) * idx2;
+        const T visc = (T)(1.0 + g.mu * g.dt * Lk / g.rho);
+        C us[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const C uh = uhat[(long)c * N * plane + gidx];
+          us[c] = fftk::mk<C>(uh.x * visc + X[c][k2].x * irho, uh.y * visc + X[c][k2].y * irho);
+        }
+        const C D[3] = {fftk::mk<C>((T)cx * idx1, (T)sx * idx1), fftk::mk<C>((T)cy * idx1, (T)sy * idx1),
+                        fftk::mk<C>((T)cz * idx1, (T)sz * idx1)};
+        C s = cmul(D[0], us[0]);
+        s = cadd(s, cmul(D[1], us[1]));
+        s = cadd(s, cmul(D[2], us[2]));
+        const T iL = (T)(1.0 / Lk);
+        s = fftk::mk<C>(s.x * iL, s.y * iL);
+#pragma unroll
+        for (int c = 0; c < 3; c++) un[c] = csub(us[c], cmul(fftk::mk<C>(-D[c].x, D[c].y), s));
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        uhat[(long)c * N * plane + gidx] = un[c];
+        X[c][k2] = fftk::mk<C>(un[c].x * invN, un[c].y * invN);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      fftk::dft<N2, +1>(X[c]);
+#pragma unroll
+      for (int n2 = 0; n2 < N2; n2++) {
+        C w2 = tw[n2 * k1];
+        w2.y = -w2.y;
+        A[(N2 * k1 + n2) * NL + c * WB + w] = (n2 == 0 || k1 == 0) ? X[c][n2] : cmul(X[c][n2], w2);
+      }
+    }
+  }
+  __syncthreads();
+  // pass A inverse, storing straight to global: thread (line, n2)
+  for (int u = threadIdx.x; u < NL * N2; u += blockDim.x) {
+    const int l = u % NL, n2 = u / NL;
+    const int c = l / WB, w = l % WB;
+    C v[N1];
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) v[k1] = A[(N2 * k1 + n2) * NL + l];
+    fftk::dft<N1, +1>(v);
+    if (w < wn) {
+#pragma unroll
+      for (int n1 = 0; n1 < N1; n1++) work[((long)c * N + (N2 * n1 + n2)) * plane + (long)j * nxh + i0 + w] = v[n1];
+    }
+  }
+}
+
+}  // namespace selm
