@@ -79,6 +79,21 @@ __device__ __forceinline__ void philox_normal2(uint64_t seed, uint32_t c0, uint3
   z1 = r * s;
 }
 
+// FP32 Box-Muller pair from the same Philox block (24-bit open-interval
+// uniforms); used by the FP32 form, whose noise needs no more than FP32
+__device__ __forceinline__ void philox_normal2_f32(uint64_t seed, uint32_t c0, uint32_t c1, uint64_t step, float& z0,
+                                                   float& z1) {
+  uint32_t o[4];
+  philox4x32_10(c0, c1, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)seed, (uint32_t)(seed >> 32), o);
+  const float u1 = ((float)(o[0] >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  const float u2 = ((float)(o[2] >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  const float r = sqrtf(-2.0f * logf(u1));
+  float sn, cs;
+  sincospif(2.0f * u2, &sn, &cs);
+  z0 = r * cs;
+  z1 = r * sn;
+}
+
 // ---------------------------------------------------------------- Peskin
 // phi(r) of cuda/SELM_Kernel.cu:391-395 for r = |distance| (grid units)
 template <typename T> __device__ __forceinline__ T peskin4(T r) {

@@ -64,24 +64,52 @@ __device__ __forceinline__ int axis_tiles(double x, int a, const BinSpec& bs, in
   return cnt;
 }
 
-__global__ void k_bin_count_multi(const double* __restrict__ x, int M, BinSpec bs, int* __restrict__ counts) {
+// the same from a stored stencil: c0 = wrapped shifted base of the axis
+__device__ __forceinline__ int axis_tiles_from_base(int c0, int a, const BinSpec& bs, int out[5]) {
+  int cnt = 0;
+  for (int i = 0; i < 5; i++) {
+    int c = c0 + i;
+    if (c >= bs.n[a]) c -= bs.n[a];
+    const int t = c / bs.tile[a];
+    bool dup = false;
+    for (int j = 0; j < cnt; j++) dup |= (out[j] == t);
+    if (!dup) out[cnt++] = t;
+  }
+  return cnt;
+}
+
+__device__ __forceinline__ void monomer_tiles(const double* __restrict__ x, const int* __restrict__ rec_b,
+                                              int rec_stride, int p, const BinSpec& bs, int (&tx)[5], int (&ty)[5],
+                                              int (&tz)[5], int& nxt, int& nyt, int& nzt) {
+  if (rec_b) {
+    const int* b = rec_b + (long)p * rec_stride;  // b[axis][shift]
+    nxt = axis_tiles_from_base(b[1], 0, bs, tx);
+    nyt = axis_tiles_from_base(b[3], 1, bs, ty);
+    nzt = axis_tiles_from_base(b[5], 2, bs, tz);
+  } else {
+    nxt = axis_tiles(x[3 * p], 0, bs, tx);
+    nyt = axis_tiles(x[3 * p + 1], 1, bs, ty);
+    nzt = axis_tiles(x[3 * p + 2], 2, bs, tz);
+  }
+}
+
+__global__ void k_bin_count_multi(const double* __restrict__ x, const int* __restrict__ rec_b, int rec_stride, int M,
+                                  BinSpec bs, int* __restrict__ counts) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= M) return;
-  int tx[5], ty[5], tz[5];
-  const int nxt = axis_tiles(x[3 * p], 0, bs, tx), nyt = axis_tiles(x[3 * p + 1], 1, bs, ty),
-            nzt = axis_tiles(x[3 * p + 2], 2, bs, tz);
+  int tx[5], ty[5], tz[5], nxt, nyt, nzt;
+  monomer_tiles(x, rec_b, rec_stride, p, bs, tx, ty, tz, nxt, nyt, nzt);
   for (int k = 0; k < nzt; k++)
     for (int j = 0; j < nyt; j++)
       for (int i = 0; i < nxt; i++) atomicAdd(&counts[(tz[k] * bs.nb[1] + ty[j]) * bs.nb[0] + tx[i]], 1);
 }
 
-__global__ void k_bin_scatter_multi(const double* __restrict__ x, int M, BinSpec bs, int* __restrict__ cursor,
-                                    int* __restrict__ unsorted) {
+__global__ void k_bin_scatter_multi(const double* __restrict__ x, const int* __restrict__ rec_b, int rec_stride,
+                                    int M, BinSpec bs, int* __restrict__ cursor, int* __restrict__ unsorted) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= M) return;
-  int tx[5], ty[5], tz[5];
-  const int nxt = axis_tiles(x[3 * p], 0, bs, tx), nyt = axis_tiles(x[3 * p + 1], 1, bs, ty),
-            nzt = axis_tiles(x[3 * p + 2], 2, bs, tz);
+  int tx[5], ty[5], tz[5], nxt, nyt, nzt;
+  monomer_tiles(x, rec_b, rec_stride, p, bs, tx, ty, tz, nxt, nyt, nzt);
   for (int k = 0; k < nzt; k++)
     for (int j = 0; j < nyt; j++)
       for (int i = 0; i < nxt; i++) {
@@ -231,12 +259,14 @@ static cudaError_t exclusive_scan(const int* in, int* out, long n, int* tmp, cud
   return cudaGetLastError();
 }
 
-cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBuffers& bb, cudaStream_t st) {
+cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBuffers& bb, cudaStream_t st,
+                          const int* rec_b, int rec_stride) {
   const long nbk = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
   cudaError_t e = cudaMemsetAsync(bb.counts, 0, sizeof(int) * (nbk + 1), st);
   if (e != cudaSuccess) return e;
   if (M > 0) {
-    if (bs.mode == 2) k_bin_count_multi<<<(M + 255) / 256, 256, 0, st>>>(x, M, bs, bb.counts);
+    if (bs.mode == 2)
+      k_bin_count_multi<<<(M + 255) / 256, 256, 0, st>>>(x, rec_b, rec_stride, M, bs, bb.counts);
     else k_bin_count<<<(M + 255) / 256, 256, 0, st>>>(x, M, bs, bb.bucket_of, bb.counts);
     count_launches(1);
   }
@@ -244,7 +274,8 @@ cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBu
   if ((e = cudaMemcpyAsync(bb.cursor, bb.offsets, sizeof(int) * nbk, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return e;
   if (M > 0) {
-    if (bs.mode == 2) k_bin_scatter_multi<<<(M + 255) / 256, 256, 0, st>>>(x, M, bs, bb.cursor, bb.unsorted);
+    if (bs.mode == 2)
+      k_bin_scatter_multi<<<(M + 255) / 256, 256, 0, st>>>(x, rec_b, rec_stride, M, bs, bb.cursor, bb.unsorted);
     else k_bin_scatter<<<(M + 255) / 256, 256, 0, st>>>(bb.bucket_of, M, bb.cursor, bb.unsorted);
     count_launches(1);
     if ((e = cudaMemsetAsync(bb.big_count, 0, sizeof(int), st)) != cudaSuccess) return e;
@@ -301,13 +332,17 @@ __device__ __forceinline__ T interp_one(double rx, double ry, double rz, int Nx,
 }
 
 // lagrangian_update() of cuda/SELM_Kernel.cu:302-373, one thread per
-// (monomer, component); the spread part lives in k_spread_gather.
+// (monomer, component); the spread part lives in k_spread_tiles.  The thread
+// of component d also stores, for the spread of the same step, the stencil
+// bases and weights of axis d (unshifted) and axis d+1 (shifted) in the
+// monomer's record, so the three threads together fill it.
 template <typename T>
 __global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, const double* __restrict__ x_old,
                                                        double* __restrict__ x_new, double* __restrict__ v,
                                                        double* __restrict__ f, const double* __restrict__ m,
                                                        double* __restrict__ tf_out, const int* __restrict__ order,
-                                                       CouplingArgs a, uint32_t* __restrict__ err) {
+                                                       WRec<T>* __restrict__ rec, CouplingArgs a,
+                                                       uint32_t* __restrict__ err) {
   const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= 3L * a.M) return;
   const int s = (int)(gid / 3), d = (int)(gid % 3);
@@ -316,10 +351,44 @@ __global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, 
   const long N = (long)a.nx * a.ny * a.nz;
   const double gx = (x_old[3L * p] - a.lo) / a.dx, gy = (x_old[3L * p + 1] - a.lo) / a.dx,
                gz = (x_old[3L * p + 2] - a.lo) / a.dx;
-  T val;
-  if (d == 0) val = interp_one<T>(gx, gy - 0.5, gz - 0.5, a.nx, a.ny, a.nz, u);
-  else if (d == 1) val = interp_one<T>(gx - 0.5, gy, gz - 0.5, a.nx, a.ny, a.nz, u + N);
-  else val = interp_one<T>(gx - 0.5, gy - 0.5, gz, a.nx, a.ny, a.nz, u + 2 * N);
+  const double r[3] = {d == 0 ? gx : gx - 0.5, d == 1 ? gy : gy - 0.5, d == 2 ? gz : gz - 0.5};
+  const int nn[3] = {a.nx, a.ny, a.nz};
+  int base[3];
+  T w[3][4];
+#pragma unroll
+  for (int ax = 0; ax < 3; ax++) {
+    base[ax] = (int)floor(r[ax]) - 1;
+#pragma unroll
+    for (int i = 0; i < 4; i++) w[ax][i] = ref_weight<T>(fabs(r[ax] - (double)(base[ax] + i)));
+  }
+  const T* ud = u + d * N;
+  int ix[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) ix[i] = wrapi(base[0] + i, a.nx);
+  T val = T(0);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const T dk = T(1) * w[2][k];
+    const long zoff = (long)wrapi(base[2] + k, a.nz) * a.ny;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const T dj = dk * w[1][j];
+      const T* row = ud + (zoff + wrapi(base[1] + j, a.ny)) * a.nx;
+#pragma unroll
+      for (int i = 0; i < 4; i++) val += __ldg(row + ix[i]) * (dj * w[0][i]);
+    }
+  }
+  if (rec) {
+    const int a1 = (d + 1) % 3;
+    WRec<T>& R = rec[p];
+    R.b[d][0] = wrapi(base[d], nn[d]);
+    R.b[a1][1] = wrapi(base[a1], nn[a1]);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      R.w[d][0][i] = w[d][i];
+      R.w[a1][1][i] = w[a1][i];
+    }
+  }
   const double vg = v[g];
   double t_f = -a.upsilon * (vg - (double)val) * a.dt;
   if (a.stochastic) {
@@ -374,10 +443,12 @@ template cudaError_t interp_only<float>(const float*, const double*, int, int, i
 
 template <typename T>
 cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double* v, double* f, const double* m,
-                          double* tf, const int* order, const CouplingArgs& a, uint32_t* err, cudaStream_t st) {
+                          double* tf, const int* order, WRec<T>* rec, const CouplingArgs& a, uint32_t* err,
+                          cudaStream_t st) {
   if (a.M <= 0) return cudaSuccess;
   const long nt = 3L * a.M;
-  k_interp_update<T><<<(unsigned)((nt + 383) / 384), 384, 0, st>>>(u, x_old, x_new, v, f, m, tf, order, a, err);
+  k_interp_update<T><<<(unsigned)((nt + 383) / 384), 384, 0, st>>>(u, x_old, x_new, v, f, m, tf, order, rec, a,
+                                                                    err);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -429,7 +500,8 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
                                                                  const double* __restrict__ x_old,
                                                                  const double* __restrict__ tf, BinSpec bs,
                                                                  const int* __restrict__ offsets,
-                                                                 const int* __restrict__ sorted, CouplingArgs a) {
+                                                                 const int* __restrict__ sorted,
+                                                                 const WRec<T>* __restrict__ rec, CouplingArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SpreadCand<T>* cand = reinterpret_cast<SpreadCand<T>*>(smem_raw);
   T* accs = reinterpret_cast<T*>(smem_raw + sizeof(SpreadCand<T>) * kSpreadThreads);
@@ -452,6 +524,19 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
     if (q < e) {
       const int p = sorted[q];
       SpreadCand<T> c;
+      if (rec) {
+        const WRec<T>& R = rec[p];
+#pragma unroll
+        for (int ax = 0; ax < 3; ax++)
+#pragma unroll
+          for (int sh = 0; sh < 2; sh++) {
+            int rb = R.b[ax][sh] - t0[ax];
+            if (rb < 0) rb += nn[ax];
+            c.rb[ax][sh] = rb;
+#pragma unroll
+            for (int i = 0; i < 4; i++) c.w[ax][sh][i] = R.w[ax][sh][i];
+          }
+      } else
 #pragma unroll
       for (int ax = 0; ax < 3; ax++) {
         const double g = (x_old[3L * p + ax] - a.lo) / a.dx;
@@ -529,7 +614,8 @@ long spread_entries_per_monomer(const BinSpec& bs) {
 
 template <typename T>
 cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const double* tf, const BinSpec& bs,
-                          const int* offsets, const int* sorted, const CouplingArgs& a, cudaStream_t st) {
+                          const int* offsets, const int* sorted, const CouplingArgs& a, cudaStream_t st,
+                          const WRec<T>* rec) {
   const int ntiles = bs.nb[0] * bs.nb[1] * bs.nb[2];
   if (!accumulate && a.M == 0) {
     return cudaMemsetAsync(fgrid, 0, sizeof(T) * 3L * a.nx * a.ny * a.nz, st);
@@ -539,18 +625,21 @@ cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const 
   cudaError_t e = cudaFuncSetAttribute((const void*)k_spread_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sm);
   if (e != cudaSuccess) return e;
-  k_spread_tiles<T><<<ntiles, kSpreadThreads, sm, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets, sorted, a);
+  k_spread_tiles<T><<<ntiles, kSpreadThreads, sm, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets, sorted,
+                                                         rec, a);
   count_launches(1);
   return cudaGetLastError();
 }
 
 template cudaError_t interp_update<double>(const double*, const double*, double*, double*, double*, const double*,
-                                           double*, const int*, const CouplingArgs&, uint32_t*, cudaStream_t);
+                                           double*, const int*, WRec<double>*, const CouplingArgs&, uint32_t*,
+                                           cudaStream_t);
 template cudaError_t interp_update<float>(const float*, const double*, double*, double*, double*, const double*,
-                                          double*, const int*, const CouplingArgs&, uint32_t*, cudaStream_t);
+                                          double*, const int*, WRec<float>*, const CouplingArgs&, uint32_t*,
+                                          cudaStream_t);
 template cudaError_t spread_gather<double>(double*, bool, const double*, const double*, const BinSpec&, const int*,
-                                           const int*, const CouplingArgs&, cudaStream_t);
+                                           const int*, const CouplingArgs&, cudaStream_t, const WRec<double>*);
 template cudaError_t spread_gather<float>(float*, bool, const double*, const double*, const BinSpec&, const int*,
-                                          const int*, const CouplingArgs&, cudaStream_t);
+                                          const int*, const CouplingArgs&, cudaStream_t, const WRec<float>*);
 
 }  // namespace selm

@@ -359,7 +359,7 @@ template <typename T, int N> constexpr size_t smem_xy_fast() {
 }
 template <typename T> constexpr int wb_fast() { return sizeof(T) == 8 ? 8 : 16; }
 template <typename T, int N> constexpr size_t smem_z_fast() {
-  return sizeof(cpx<T>) * ((size_t)N * 3 * wb_fast<T>() + N);
+  return sizeof(cpx<T>) * (2 * (size_t)N * 3 * wb_fast<T>() + N);
 }
 
 template <typename T, int N> static cudaError_t fast_attrs() {
@@ -621,14 +621,16 @@ template <typename T> static int fused_step_t(selm_sim* s) {
   double* xo = s->x[s->cx];
   double* xn = s->x[s->cx ^ 1];
   if (s->M > 0) {
-    prof_mark(s, "bin", true);
-    CUF(bin_particles(xo, s->M, s->tiles, s->tbb, s->st));
-    prof_mark(s, "bin", false);
+    WRec<T>* rec = static_cast<WRec<T>*>(s->wrec);
     prof_mark(s, "interp_update", true);
-    CUF(interp_update<T>((const T*)z->u, xo, xn, s->v, s->f, s->m, s->tf, nullptr, a, s->err, s->st));
+    CUF(interp_update<T>((const T*)z->u, xo, xn, s->v, s->f, s->m, s->tf, nullptr, rec, a, s->err, s->st));
     prof_mark(s, "interp_update", false);
+    prof_mark(s, "bin", true);
+    CUF(bin_particles(xo, s->M, s->tiles, s->tbb, s->st, reinterpret_cast<const int*>(rec),
+                      (int)(sizeof(WRec<T>) / sizeof(int))));
+    prof_mark(s, "bin", false);
     prof_mark(s, "spread", true);
-    CUF(spread_gather<T>((T*)z->fp, false, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st));
+    CUF(spread_gather<T>((T*)z->fp, false, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st, rec));
     prof_mark(s, "spread", false);
   } else {
     CUF(cudaMemsetAsync(z->fp, 0, sizeof(T) * 3 * s->N, s->st));

@@ -179,8 +179,10 @@ struct ZGeom {
 };
 
 // reference noise draw of a half-spectrum mode (cuda/SELM_Kernel.cu:56-79); the
-// amplitude sqrt(lambda_h) comes from the symbol tables (cm = cos - 1)
-template <int N>
+// amplitude sqrt(lambda_h) comes from the symbol tables (cm = cos - 1).  The
+// FP64 forms draw FP64 normals (same stream as the plain form); the FP32 form
+// draws FP32 normals from the same Philox counters.
+template <typename T, int N>
 __device__ __forceinline__ void noise_draw_fast(const ZGeom& g, uint64_t step, int i, int j, int k, double cmx,
                                                 double cmy, double cmz, double2 out[3]) {
   const double lam = -2.0 * (cmx + cmy + cmz) / (g.dx * g.dx);
@@ -192,9 +194,15 @@ __device__ __forceinline__ void noise_draw_fast(const ZGeom& g, uint64_t step, i
   const uint32_t q = (uint32_t)(((long)k * g.ny + j) * g.nxh + i);
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    double z0, z1;
-    philox_normal2(g.seed, q, (uint32_t)d, step, z0, z1);
-    out[d] = make_double2(z0 * re, z1 * im);
+    if constexpr (sizeof(T) == 8) {
+      double z0, z1;
+      philox_normal2(g.seed, q, (uint32_t)d, step, z0, z1);
+      out[d] = make_double2(z0 * re, z1 * im);
+    } else {
+      float z0, z1;
+      philox_normal2_f32(g.seed, q, (uint32_t)d, step, z0, z1);
+      out[d] = make_double2((double)z0 * re, (double)z1 * im);
+    }
   }
 }
 
@@ -209,7 +217,8 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
   constexpr int NL = 3 * WB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* A = reinterpret_cast<C*>(smem_raw);  // element t of line (c, w) at t*NL + c*WB + w
-  C* tw = A + N * NL;
+  C* U = A + N * NL;                      // u_hat block, mode k of line (c, w) at k*NL + c*WB + w
+  C* tw = U + N * NL;
   const int nxh = g.nxh, ny = g.ny;
   const int nblk = (nxh + WB - 1) / WB;
   const int j = blockIdx.x / nblk;
@@ -224,8 +233,12 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
     const int c = l / WB, w = l % WB;
     C v[N1];
 #pragma unroll
-    for (int n1 = 0; n1 < N1; n1++)
-      v[n1] = (w < wn) ? work[((long)c * N + (N2 * n1 + n2)) * plane + (long)j * nxh + i0 + w] : fftk::mk<C>(T(0), T(0));
+    for (int n1 = 0; n1 < N1; n1++) {
+      const long gi = ((long)c * N + (N2 * n1 + n2)) * plane + (long)j * nxh + i0 + w;
+      const bool ok = w < wn;
+      v[n1] = ok ? work[gi] : fftk::mk<C>(T(0), T(0));
+      U[(N2 * n1 + n2) * NL + l] = ok ? uhat[gi] : fftk::mk<C>(T(0), T(0));
+    }
     fftk::dft<N1, -1>(v);
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) A[(N2 * k1 + n2) * NL + l] = (k1 == 0) ? v[0] : cmul(v[k1], tw[n2 * k1]);
@@ -253,16 +266,15 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
 #pragma unroll
     for (int k2 = 0; k2 < N2; k2++) {
       const int k = k1 + N1 * k2;
-      const long gidx = (long)k * plane + (long)j * nxh + i;
       const double cz = symz[2 * k], sz = symz[2 * k + 1];
       if (g.stochastic) {
         double2 Xn[3];
-        noise_draw_fast<N>(g, step, i, j, k, cx, cy, cz, Xn);
+        noise_draw_fast<T, N>(g, step, i, j, k, cx, cy, cz, Xn);
         if (i == 0 || ((g.nx & 1) == 0 && i == g.nx / 2)) {
           const int jc = (ny - j) % ny, kc = (N - k) % N;
           if (jc != j || kc != k) {
             double2 Xc[3];
-            noise_draw_fast<N>(g, step, i, jc, kc, cx, symy[2 * jc], symz[2 * kc], Xc);
+            noise_draw_fast<T, N>(g, step, i, jc, kc, cx, symy[2 * jc], symz[2 * kc], Xc);
             const double s = (g.noise_mode == 1) ? 0.7071067811865476 : 0.5;
 #pragma unroll
             for (int c = 0; c < 3; c++) Xn[c] = make_double2((Xn[c].x + Xc[c].x) * s, (Xn[c].y - Xc[c].y) * s);
@@ -287,7 +299,7 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
         C us[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          const C uh = uhat[(long)c * N * plane + gidx];
+          const C uh = U[k * NL + c * WB + w];
           us[c] = fftk::mk<C>(uh.x * visc + X[c][k2].x * irho, uh.y * visc + X[c][k2].y * irho);
         }
         const C D[3] = {fftk::mk<C>((T)cx * idx1, (T)sx * idx1), fftk::mk<C>((T)cy * idx1, (T)sy * idx1),
@@ -302,7 +314,7 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
       }
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        uhat[(long)c * N * plane + gidx] = un[c];
+        U[k * NL + c * WB + w] = un[c];
         X[c][k2] = fftk::mk<C>(un[c].x * invN, un[c].y * invN);
       }
     }
@@ -328,7 +340,11 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
     fftk::dft<N1, +1>(v);
     if (w < wn) {
 #pragma unroll
-      for (int n1 = 0; n1 < N1; n1++) work[((long)c * N + (N2 * n1 + n2)) * plane + (long)j * nxh + i0 + w] = v[n1];
+      for (int n1 = 0; n1 < N1; n1++) {
+        const long gi = ((long)c * N + (N2 * n1 + n2)) * plane + (long)j * nxh + i0 + w;
+        work[gi] = v[n1];
+        uhat[gi] = U[(N2 * n1 + n2) * NL + l];
+      }
     }
   }
 }

@@ -15,10 +15,22 @@ namespace selm {
 
 __device__ __forceinline__ double min_img(double d, double L) { return d - L * rint(d / L); }
 
+// monomers in cell order: xs[q] = (x, y, z, type) of sorted[q]
+__global__ void k_gather_cells(const double* __restrict__ x, const int* __restrict__ type, const int* __restrict__ sorted,
+                               int M, double4* __restrict__ xs) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= M) return;
+  const int p = sorted[q];
+  xs[q] = make_double4(x[3 * p], x[3 * p + 1], x[3 * p + 2], (double)type[p]);
+}
+
 __global__ void k_forces(const double* __restrict__ x, double* __restrict__ f, ForceTopo t, BinSpec cells,
-                         const int* __restrict__ offsets, const int* __restrict__ sorted, uint32_t* err) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= t.M) return;
+                         const int* __restrict__ offsets, const int* __restrict__ sorted,
+                         const double4* __restrict__ xcell, uint32_t* err) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= t.M) return;
+  // threads follow the cell order when a pair list exists, so a warp's monomers are neighbours
+  const int i = (t.pair_style && t.M > 1) ? sorted[slot] : slot;
   const double L = t.hi - t.lo;
   const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
   double fx = 0.0, fy = 0.0, fz = 0.0;
@@ -95,9 +107,14 @@ __global__ void k_forces(const double* __restrict__ x, double* __restrict__ f, F
       for (int oy = -span; oy <= span; oy++)
         for (int ox = -span; ox <= span; ox++) {
           const int cc = (wrapi(c3[2] + oz, nc) * nc + wrapi(c3[1] + oy, nc)) * nc + wrapi(c3[0] + ox, nc);
-          for (int q = offsets[cc]; q < offsets[cc + 1]; q++) {
+          const int qe = offsets[cc + 1];
+          for (int q = offsets[cc]; q < qe; q++) {
+            if (q == slot) continue;
+            const double4 xj = xcell[q];
+            const double dx = min_img(xi - xj.x, L), dy = min_img(yi - xj.y, L), dz = min_img(zi - xj.z, L);
+            const double rsq = dx * dx + dy * dy + dz * dz;
+            if (rsq >= t.rc2max) continue;
             const int j = sorted[q];
-            if (j == i) continue;
             double w = 1.0;
             for (int s = t.sp_off[i]; s < t.sp_off[i + 1]; s++)
               if (t.sp_nbr[s] == j) {
@@ -105,10 +122,7 @@ __global__ void k_forces(const double* __restrict__ x, double* __restrict__ f, F
                 break;
               }
             if (w == 0.0) continue;
-            const double* pc = t.pair_coeff + 3 * (ti * nt1 + t.type[j]);
-            const double dx = min_img(xi - x[3 * j], L), dy = min_img(yi - x[3 * j + 1], L),
-                         dz = min_img(zi - x[3 * j + 2], L);
-            const double rsq = dx * dx + dy * dy + dz * dz;
+            const double* pc = t.pair_coeff + 3 * (ti * nt1 + (int)xj.w);
             if (rsq >= pc[2] * pc[2] || rsq <= 0.0) continue;
             const double r2i = 1.0 / rsq, s2 = pc[1] * pc[1] * r2i, s6 = s2 * s2 * s2;
             const double fp = w * 24.0 * pc[0] * s6 * (2.0 * s6 - 1.0) * r2i;
@@ -131,9 +145,13 @@ __global__ void k_forces(const double* __restrict__ x, double* __restrict__ f, F
 }
 
 cudaError_t compute_forces(const double* x, double* f, const ForceTopo& t, const BinSpec& cells, const int* offsets,
-                           const int* sorted, uint32_t* err, cudaStream_t st) {
+                           const int* sorted, double4* xs, uint32_t* err, cudaStream_t st) {
   if (t.M <= 0) return cudaSuccess;
-  k_forces<<<(t.M + 127) / 128, 128, 0, st>>>(x, f, t, cells, offsets, sorted, err);
+  if (t.pair_style && t.M > 1) {
+    k_gather_cells<<<(t.M + 255) / 256, 256, 0, st>>>(x, t.type, sorted, t.M, xs);
+    count_launches(1);
+  }
+  k_forces<<<(t.M + 127) / 128, 128, 0, st>>>(x, f, t, cells, offsets, sorted, xs, err);
   count_launches(1);
   return cudaGetLastError();
 }

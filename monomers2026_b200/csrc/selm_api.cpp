@@ -250,6 +250,12 @@ extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const dou
     if ((rc = dalloc(s, &s->f, 3L * M))) return rc;
     if ((rc = dalloc(s, &s->m, M))) return rc;
     if ((rc = dalloc(s, &s->tf, 3L * M))) return rc;
+    {
+      const size_t rb = (s->prm.form == SELM_FORM_FUSED32) ? sizeof(WRec<float>) : sizeof(WRec<double>);
+      unsigned char* w = nullptr;
+      if ((rc = dalloc(s, &w, rb * (size_t)M))) return rc;
+      s->wrec = w;
+    }
     if ((rc = alloc_bins(s, s->tiles, s->tbb, M))) return rc;
     CU(cudaMemsetAsync(s->f, 0, sizeof(double) * 3 * M, s->st));
   }
@@ -437,8 +443,10 @@ extern "C" int selm_set_topology(selm_sim* s, const selm_topology* tp) {
     fc.tile[a] = 1;
     fc.nb[a] = nc;
   }
+  T.rc2max = rcmax * rcmax;
   if (tp->pair_style && M > 1) {
     if ((rc = alloc_bins(s, s->fcells, s->fbb, M))) return rc;
+    if ((rc = dalloc(s, &s->fxs, M))) return rc;
   }
   s->have_topo = true;
   s->cb = nullptr;
@@ -461,9 +469,9 @@ int engine_forces(selm_sim* s) {
     prof_mark(s, "forces", true);
     if (s->topo.pair_style && s->M > 1) {
       CU(bin_particles(x, s->M, s->fcells, s->fbb, s->st));
-      CU(compute_forces(x, s->f, s->topo, s->fcells, s->fbb.offsets, s->fbb.sorted, s->err, s->st));
+      CU(compute_forces(x, s->f, s->topo, s->fcells, s->fbb.offsets, s->fbb.sorted, s->fxs, s->err, s->st));
     } else {
-      CU(compute_forces(x, s->f, s->topo, s->fcells, nullptr, nullptr, s->err, s->st));
+      CU(compute_forces(x, s->f, s->topo, s->fcells, nullptr, nullptr, nullptr, s->err, s->st));
     }
     prof_mark(s, "forces", false);
     return SELM_OK;
@@ -520,14 +528,16 @@ static int plain_step(selm_sim* s) {
   double* xo = s->x[s->cx];
   double* xn = s->x[s->cx ^ 1];
   if (s->M > 0) {
-    prof_mark(s, "bin", true);
-    CU(bin_particles(xo, s->M, s->tiles, s->tbb, s->st));
-    prof_mark(s, "bin", false);
+    WRec<double>* rec = static_cast<WRec<double>*>(s->wrec);
     prof_mark(s, "interp_update", true);
-    CU(interp_update<double>(s->u64[s->cu], xo, xn, s->v, s->f, s->m, s->tf, nullptr, a, s->err, s->st));
+    CU(interp_update<double>(s->u64[s->cu], xo, xn, s->v, s->f, s->m, s->tf, nullptr, rec, a, s->err, s->st));
     prof_mark(s, "interp_update", false);
+    prof_mark(s, "bin", true);
+    CU(bin_particles(xo, s->M, s->tiles, s->tbb, s->st, reinterpret_cast<const int*>(rec),
+                     (int)(sizeof(WRec<double>) / sizeof(int))));
+    prof_mark(s, "bin", false);
     prof_mark(s, "spread", true);
-    CU(spread_gather<double>(s->fg64, true, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st));
+    CU(spread_gather<double>(s->fg64, true, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st, rec));
     prof_mark(s, "spread", false);
     s->cx ^= 1;
   }

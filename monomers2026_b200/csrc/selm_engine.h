@@ -30,6 +30,7 @@ struct selm_sim {
   int M = 0;
   double* x[2] = {nullptr, nullptr};
   double *v = nullptr, *f = nullptr, *m = nullptr, *tf = nullptr;
+  void* wrec = nullptr;  // per-monomer stencil records (WRec<T> of the grid precision)
   int cx = 0;
   // plain-form grid (Eulerian::d_u[2], d_f, d_p, cuda/SELM_Eulerian.cuh:12-20)
   double* u64[2] = {nullptr, nullptr};
@@ -40,6 +41,7 @@ struct selm_sim {
   selm::FftTables<float> tb32{};
   selm::BinSpec tiles{}, fcells{};
   selm::BinBuffers tbb{}, fbb{};
+  double4* fxs = nullptr;  // monomers in force-cell order
   bool have_topo = false;
   selm::ForceTopo topo{};
   selm_force_fn cb = nullptr;

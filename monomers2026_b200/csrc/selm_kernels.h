@@ -57,9 +57,18 @@ long scan_tmp_size(long n);
 // spread tiles (mode 2): every monomer filed under each tile its stencil reaches
 BinSpec spread_bin_spec(const int dims[3], double lo, double dx);
 long spread_entries_per_monomer(const BinSpec& bs);
-cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBuffers& bb, cudaStream_t st);
+// rec_b (optional, mode 2): stencil bases of a per-monomer record (ints b[axis][shift]
+// at the record's start), rec_stride ints apart; without it the bases come from x
+cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBuffers& bb, cudaStream_t st,
+                          const int* rec_b = nullptr, int rec_stride = 0);
 
 // ---- coupling and monomer update
+// Per-monomer stencil of one step: wrapped base cell of the 4-point stencil and
+// its weight factors, per axis, unshifted and shifted by half a cell.
+template <typename T> struct WRec {
+  int b[3][2];
+  T w[3][2][4];
+};
 struct CouplingArgs {
   int nx, ny, nz;
   double lo, hi, dx, dt, upsilon, coef;
@@ -70,13 +79,15 @@ struct CouplingArgs {
 };
 template <typename T>
 cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double* v, double* f, const double* m,
-                          double* tf, const int* order, const CouplingArgs& a, uint32_t* err, cudaStream_t st);
+                          double* tf, const int* order, WRec<T>* rec, const CouplingArgs& a, uint32_t* err,
+                          cudaStream_t st);
 template <typename T>
 cudaError_t interp_only(const T* u, const double* x, int M, int nx, int ny, int nz, double lo, double dx, double* out,
                         cudaStream_t st);
 template <typename T>
 cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const double* tf, const BinSpec& bs,
-                          const int* offsets, const int* sorted, const CouplingArgs& a, cudaStream_t st);
+                          const int* offsets, const int* sorted, const CouplingArgs& a, cudaStream_t st,
+                          const WRec<T>* rec = nullptr);
 
 // ---- conservative forces (FP64)
 struct ForceTopo {
@@ -98,8 +109,9 @@ struct ForceTopo {
   const double* sp_w;     // weight per entry
   double body[3];
   double lo, hi;
+  double rc2max;          // largest pair cutoff squared (quick reject)
 };
 cudaError_t compute_forces(const double* x, double* f, const ForceTopo& t, const BinSpec& cells, const int* offsets,
-                           const int* sorted, uint32_t* err, cudaStream_t st);
+                           const int* sorted, double4* xs, uint32_t* err, cudaStream_t st);
 
 }  // namespace selm
