@@ -131,12 +131,17 @@ __global__ void k_bin_scatter(const int* __restrict__ bucket_of, int M, int* __r
 // whose state went non-finite) are queued for k_bucket_sort_big instead.
 constexpr int kWarpSortMax = 256;
 __global__ void k_bucket_sort(const int* __restrict__ offsets, int nbuckets, const int* __restrict__ unsorted,
-                              int* __restrict__ sorted, int* __restrict__ big_list, int* __restrict__ big_count) {
+                              int* __restrict__ sorted, int* __restrict__ big_list, int* __restrict__ big_count,
+                              int presorted_max) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= nbuckets) return;
   const int s = offsets[warp], e = offsets[warp + 1];
   const int n = e - s;
+  if (n <= presorted_max) {  // the consumer orders these itself
+    for (int i = lane; i < n; i += 32) sorted[s + i] = unsorted[s + i];
+    return;
+  }
   if (n > kWarpSortMax) {
     if (lane == 0) big_list[atomicAdd(big_count, 1)] = warp;
     return;
@@ -176,6 +181,8 @@ __global__ void __launch_bounds__(kBigSortThreads) k_bucket_sort_big(const int* 
     }
   }
 }
+
+constexpr int kSpreadChunk = 192;  // candidates per accumulation round of k_spread_tiles
 
 // ---- exclusive scan over n ints (two levels of 4096-element blocks)
 constexpr int kScanThreads = 1024, kScanIpt = 4, kScanBlock = kScanThreads * kScanIpt;
@@ -279,8 +286,10 @@ cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBu
     else k_bin_scatter<<<(M + 255) / 256, 256, 0, st>>>(bb.bucket_of, M, bb.cursor, bb.unsorted);
     count_launches(1);
     if ((e = cudaMemsetAsync(bb.big_count, 0, sizeof(int), st)) != cudaSuccess) return e;
+    // spread tiles sort buckets of up to one candidate chunk themselves
+    const int presorted_max = (bs.mode == 2) ? kSpreadChunk : 0;
     k_bucket_sort<<<(unsigned)((nbk * 32 + 255) / 256), 256, 0, st>>>(bb.offsets, (int)nbk, bb.unsorted, bb.sorted,
-                                                                      bb.big_list, bb.big_count);
+                                                                      bb.big_list, bb.big_count, presorted_max);
     count_launches(1);
     k_bucket_sort_big<<<148, kBigSortThreads, 0, st>>>(bb.offsets, bb.unsorted, bb.sorted, bb.big_list, bb.big_count);
     count_launches(1);
@@ -463,6 +472,7 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
 // candidates that reach it, in candidate order.
 constexpr int kTX = 16, kTY = 8, kTZ = 8;
 constexpr int kSpreadThreads = 3 * kTY * kTZ;
+static_assert(kTY == kTZ && kSpreadThreads == kSpreadChunk, "spread tile rows and chunk size");
 constexpr int kRowPad = kTX + 1;  // odd row stride of the shared accumulators
 
 template <typename T> struct SpreadCand {
@@ -472,25 +482,33 @@ template <typename T> struct SpreadCand {
   unsigned char ymask[2], zmask[2];   // tile rows the stencil reaches: [unshifted, shifted]
 };
 
+// Row (d, ry, rz) of the tile: the candidates that reach it are the set bits
+// of my & mz (candidate masks of this chunk); they are taken in increasing
+// candidate order, so every cell sums its contributions in a fixed order.
 template <typename T>
-__device__ __forceinline__ void spread_rows(const SpreadCand<T>* __restrict__ cand, int ncand, int d, int ry, int rz,
+__device__ __forceinline__ void spread_rows(const SpreadCand<T>* __restrict__ cand, const unsigned* __restrict__ my,
+                                            const unsigned* __restrict__ mz, int nwords, int d, int ry, int rz,
                                             int nx, int ny, int nz, int extx, T* __restrict__ acc) {
   const int sx = (d == 0) ? 0 : 1, sy = (d == 1) ? 0 : 1, sz = (d == 2) ? 0 : 1;
-  for (int c = 0; c < ncand; c++) {
-    const SpreadCand<T>& C = cand[c];
-    if (!(((C.ymask[sy] >> ry) & (C.zmask[sz] >> rz)) & 1)) continue;
-    int jy = ry - C.rb[1][sy];
-    if (jy < 0) jy += ny;
-    int kz = rz - C.rb[2][sz];
-    if (kz < 0) kz += nz;
-    const T dj = (T(1) * C.w[2][sz][kz]) * C.w[1][sy][jy];
-    const T tfd = C.tf[d];
-    const int rbx = C.rb[0][sx];
+  for (int wi = 0; wi < nwords; wi++) {
+    unsigned m = my[wi] & mz[wi];
+    while (m) {
+      const int c = wi * 32 + __ffs(m) - 1;
+      m &= m - 1;
+      const SpreadCand<T>& C = cand[c];
+      int jy = ry - C.rb[1][sy];
+      if (jy < 0) jy += ny;
+      int kz = rz - C.rb[2][sz];
+      if (kz < 0) kz += nz;
+      const T dj = (T(1) * C.w[2][sz][kz]) * C.w[1][sy][jy];
+      const T tfd = C.tf[d];
+      const int rbx = C.rb[0][sx];
 #pragma unroll
-    for (int ix = 0; ix < 4; ix++) {
-      int cx = rbx + ix;
-      if (cx >= nx) cx -= nx;
-      if (cx < extx) acc[cx] -= tfd * (dj * C.w[0][sx][ix]);
+      for (int ix = 0; ix < 4; ix++) {
+        int cx = rbx + ix;
+        if (cx >= nx) cx -= nx;
+        if (cx < extx) acc[cx] -= tfd * (dj * C.w[0][sx][ix]);
+      }
     }
   }
 }
@@ -518,11 +536,31 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
   T* row = fgrid + d * N + ((long)(t0[2] + rz) * ny + (t0[1] + ry)) * nx + t0[0];
   T* acc = accs + tid * kRowPad;
   for (int cx = 0; cx < kTX; cx++) acc[cx] = (accumulate && row_ok && cx < ext[0]) ? row[cx] : T(0);
+  // candidate masks of the current chunk: [d][row][word], for y rows and z rows
+  __shared__ unsigned masky[3][kTY][kSpreadThreads / 32];
+  __shared__ unsigned maskz[3][kTZ][kSpreadThreads / 32];
+  __shared__ int ids[kSpreadThreads];
+  const int lane = tid & 31, wid = tid >> 5;
   const int s = offsets[tb], e = offsets[tb + 1];
+  const bool self_sort = (e - s) <= kSpreadThreads;  // larger buckets arrive ordered by monomer index
   for (int base = s; base < e; base += kSpreadThreads) {
     const int q = base + tid;
+    unsigned cym[2] = {0u, 0u}, czm[2] = {0u, 0u};
+    int slot = tid;
+    int p = -1;
+    if (self_sort) {
+      if (q < e) ids[tid] = sorted[q];
+      __syncthreads();
+      if (q < e) {
+        p = ids[tid];
+        int r = 0;
+        for (int j = 0; j < e - s; j++) r += (ids[j] < p);
+        slot = r;
+      }
+    } else if (q < e) {
+      p = sorted[q];
+    }
     if (q < e) {
-      const int p = sorted[q];
       SpreadCand<T> c;
       if (rec) {
         const WRec<T>& R = rec[p];
@@ -563,13 +601,39 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
         }
         c.ymask[sh] = (unsigned char)ym;
         c.zmask[sh] = (unsigned char)zm;
+        cym[sh] = ym;
+        czm[sh] = zm;
       }
 #pragma unroll
       for (int dd = 0; dd < 3; dd++) c.tf[dd] = (T)tf[3L * p + dd];
-      cand[tid] = c;
+      cand[slot] = c;
+    }
+    if (self_sort) {
+      __syncthreads();
+      if (q < e)
+#pragma unroll
+        for (int sh = 0; sh < 2; sh++) {
+          cym[sh] = cand[tid].ymask[sh];
+          czm[sh] = cand[tid].zmask[sh];
+        }
+    }
+    // warp ballots: which of this warp's 32 candidates (slots) reach each row
+#pragma unroll
+    for (int dd = 0; dd < 3; dd++) {
+      const int shy = (dd == 1) ? 0 : 1, shz = (dd == 2) ? 0 : 1;
+#pragma unroll
+      for (int rr = 0; rr < kTY; rr++) {
+        const unsigned by = __ballot_sync(0xffffffffu, (cym[shy] >> rr) & 1u);
+        const unsigned bz = __ballot_sync(0xffffffffu, (czm[shz] >> rr) & 1u);
+        if (lane == 0) {
+          masky[dd][rr][wid] = by;
+          maskz[dd][rr][wid] = bz;
+        }
+      }
     }
     __syncthreads();
-    if (row_ok) spread_rows(cand, min(kSpreadThreads, e - base), d, ry, rz, nx, ny, nz, ext[0], acc);
+    const int nwords = (min(kSpreadThreads, e - base) + 31) / 32;
+    if (row_ok) spread_rows(cand, masky[d][ry], maskz[d][rz], nwords, d, ry, rz, nx, ny, nz, ext[0], acc);
     __syncthreads();
   }
   if (row_ok)
@@ -622,9 +686,13 @@ cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const 
   }
   if (bs.mode != 2 || bs.tile[0] != kTX || bs.tile[1] != kTY || bs.tile[2] != kTZ) return cudaErrorInvalidValue;
   const size_t sm = sizeof(SpreadCand<T>) * kSpreadThreads + sizeof(T) * kSpreadThreads * kRowPad;
-  cudaError_t e = cudaFuncSetAttribute((const void*)k_spread_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sm);
-  if (e != cudaSuccess) return e;
+  static bool attr_set = false;  // set once per precision, outside any stream capture after the first call
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute((const void*)k_spread_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sm);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
   k_spread_tiles<T><<<ntiles, kSpreadThreads, sm, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets, sorted,
                                                          rec, a);
   count_launches(1);
@@ -637,6 +705,17 @@ template cudaError_t interp_update<double>(const double*, const double*, double*
 template cudaError_t interp_update<float>(const float*, const double*, double*, double*, double*, const double*,
                                           double*, const int*, WRec<float>*, const CouplingArgs&, uint32_t*,
                                           cudaStream_t);
+// sets the shared-memory attribute of the spread kernels ahead of any stream capture
+cudaError_t spread_prepare_attributes() {
+  const size_t s64 = sizeof(SpreadCand<double>) * kSpreadThreads + sizeof(double) * kSpreadThreads * kRowPad;
+  const size_t s32 = sizeof(SpreadCand<float>) * kSpreadThreads + sizeof(float) * kSpreadThreads * kRowPad;
+  cudaError_t e = cudaFuncSetAttribute((const void*)k_spread_tiles<double>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s64);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute((const void*)k_spread_tiles<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)s32);
+}
+
 template cudaError_t spread_gather<double>(double*, bool, const double*, const double*, const BinSpec&, const int*,
                                            const int*, const CouplingArgs&, cudaStream_t, const WRec<double>*);
 template cudaError_t spread_gather<float>(float*, bool, const double*, const double*, const BinSpec&, const int*,

@@ -452,9 +452,9 @@ struct FusedState {
   double *symx = nullptr, *symy = nullptr, *symz = nullptr;
   uint64_t* d_step = nullptr;
   FusedPlan plan{};
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  bool graph_ok = false;
+  // one captured step per parity of the double-buffered positions
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  unsigned long long graph_kernels[2] = {0, 0};
   bool fast = false;  // compile-time four-step kernels for this grid size
 };
 
@@ -519,8 +519,8 @@ int fused_allocate(selm_sim* s) {
 
 void fused_release(selm_sim* s) {
   if (!s->fz) return;
-  if (s->fz->gexec) cudaGraphExecDestroy(s->fz->gexec);
-  if (s->fz->graph) cudaGraphDestroy(s->fz->graph);
+  for (int q = 0; q < 2; q++)
+    if (s->fz->gexec[q]) cudaGraphExecDestroy(s->fz->gexec[q]);
   delete s->fz;
   s->fz = nullptr;
 }
@@ -650,14 +650,58 @@ int fused_initial(selm_sim* s) {
   return SELM_OK;
 }
 
-int fused_step(selm_sim* s) {
+// The launches of one step: coupling and fluid on positions x[parity] ->
+// x[parity ^ 1], then the conservative forces at the new positions.
+static int fused_body(selm_sim* s) {
   const bool f32 = s->fz->fp32;
-  // the step counter on the host mirrors the device one
   int rc = f32 ? fused_step_t<float>(s) : fused_step_t<double>(s);
   if (rc) return rc;
+  if (s->M > 0) s->cx ^= 1;
+  rc = engine_forces(s);
+  if (s->M > 0) s->cx ^= 1;
+  return rc;
+}
+
+void fused_invalidate_graphs(selm_sim* s) {
+  if (!s->fz) return;
+  for (int q = 0; q < 2; q++) {
+    if (s->fz->gexec[q]) cudaGraphExecDestroy(s->fz->gexec[q]);
+    s->fz->gexec[q] = nullptr;
+  }
+}
+
+int fused_step(selm_sim* s) {
+  FusedState* z = s->fz;
+  // a host force provider or per-kernel timing needs the launches issued one by one
+  const bool graph = !s->cb && !s->prof;
+  const int par = (s->M > 0) ? s->cx : 0;
+  if (graph) {
+    if (!z->gexec[par]) {
+      const unsigned long long l0 = launches_total();
+      CUF(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+      const int rc = fused_body(s);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(s->st, &g);
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (ec != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+      const cudaError_t ei = cudaGraphInstantiate(&z->gexec[par], g, 0);
+      cudaGraphDestroy(g);
+      if (ei != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+      z->graph_kernels[par] = launches_total() - l0;
+    } else {
+      count_launches((unsigned)z->graph_kernels[par]);
+    }
+    CUF(cudaGraphLaunch(z->gexec[par], s->st));
+  } else {
+    const int rc = fused_body(s);
+    if (rc) return rc;
+  }
   s->step += 1;
   if (s->M > 0) s->cx ^= 1;
-  return engine_forces(s);
+  return SELM_OK;
 }
 
 int fused_get_field(selm_sim* s, int which, double* out) {

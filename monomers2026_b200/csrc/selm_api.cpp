@@ -192,6 +192,7 @@ int engine_allocate_grid(selm_sim* s) {
   const long N = s->N, N2 = s->N2;
   if ((rc = dalloc(s, &s->err, 1))) return rc;
   CU(cudaMemset(s->err, 0, sizeof(uint32_t)));
+  CU(spread_prepare_attributes());
   if ((rc = make_tables<double>(s->allocs, s->prm.num_mesh_pts, s->tb64))) return selm_fail(rc, "FFT tables");
   if ((rc = make_tables<float>(s->allocs, s->prm.num_mesh_pts, s->tb32))) return selm_fail(rc, "FFT tables");
   if (s->prm.form == SELM_FORM_PLAIN64) {
@@ -258,6 +259,7 @@ extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const dou
     }
     if ((rc = alloc_bins(s, s->tiles, s->tbb, M))) return rc;
     CU(cudaMemsetAsync(s->f, 0, sizeof(double) * 3 * M, s->st));
+    fused_invalidate_graphs(s);
   }
   if (M == 0) return SELM_OK;
   // periodic remap as LAMMPS' Domain::pbc at setup (whole box lengths until x is in [lo, hi));
@@ -450,6 +452,7 @@ extern "C" int selm_set_topology(selm_sim* s, const selm_topology* tp) {
   }
   s->have_topo = true;
   s->cb = nullptr;
+  fused_invalidate_graphs(s);
   return SELM_OK;
 }
 
@@ -458,6 +461,7 @@ extern "C" int selm_set_force_callback(selm_sim* s, selm_force_fn fn, void* user
   s->cb = fn;
   s->cb_user = user;
   if (fn) s->have_topo = false;
+  fused_invalidate_graphs(s);
   return SELM_OK;
 }
 

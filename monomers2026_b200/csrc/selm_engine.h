@@ -72,4 +72,5 @@ int fused_step(selm_sim* s);
 int fused_get_field(selm_sim* s, int which, double* out);
 int fused_set_field(selm_sim* s, int which, const double* in);
 int fused_stream_changed(selm_sim* s);
+void fused_invalidate_graphs(selm_sim* s);
 void fused_release(selm_sim* s);

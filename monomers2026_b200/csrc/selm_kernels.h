@@ -84,6 +84,7 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
 template <typename T>
 cudaError_t interp_only(const T* u, const double* x, int M, int nx, int ny, int nz, double lo, double dx, double* out,
                         cudaStream_t st);
+cudaError_t spread_prepare_attributes();
 template <typename T>
 cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const double* tf, const BinSpec& bs,
                           const int* offsets, const int* sorted, const CouplingArgs& a, cudaStream_t st,
