@@ -25,9 +25,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -53,51 +51,74 @@ def peaks():
 
 # --------------------------------------------------------------------------- clocks
 class Clocks:
-    """nvidia-smi sampler for the timed region."""
+    """SM clock and clock-event-reason sampler for the timed region.
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
-        self.path = None
+    Polls NVML from a background thread every few milliseconds, so that a
+    timed region of a few tens of milliseconds still gets samples; reports no
+    samples (and why) when NVML cannot be used."""
+
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
+
+    def __init__(self, device_index: int, period_s: float = 0.002):
+        self.device_index = device_index
+        self.period = period_s
+        self.samples = []
+        self.smax = None
+        self.stop_flag = None
+        self.thread = None
+        self.error = None
+
+    def _handle(self, nv):
+        import torch
+        try:
+            pr = torch.cuda.get_device_properties(self.device_index)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.device_index)
 
     def start(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except FileNotFoundError:
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        except Exception as e:  # no NVML: no samples
+            self.error = f"nvml unavailable: {type(e).__name__}"
+            return
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            getattr(nv, "nvmlDeviceGetCurrentClocksThrottleReasons")
+        self.stop_flag = threading.Event()
+
+        def run():
+            while True:
+                try:
+                    self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(get_reasons(h))))
+                except Exception as e:
+                    self.error = f"nvml query failed: {type(e).__name__}"
+                    return
+                if self.stop_flag.wait(self.period):
+                    return
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+        while not self.samples and self.thread.is_alive():  # at least one sample before the region starts
+            time.sleep(self.period)
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            f = [t.strip() for t in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "note": self.error}
+        self.stop_flag.set()
+        self.thread.join(timeout=5)
+        sm = [c for c, _ in self.samples]
+        reasons = sorted({n for _, r in self.samples for n, b in self.REASONS.items() if r & b})
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax, "reasons": reasons,
+               "samples": len(sm), "source": "nvml"}
+        if self.error:
+            out["note"] = self.error
+        return out
 
 
 # --------------------------------------------------------------------------- helpers

@@ -51,6 +51,7 @@ extern "C" {
 #define SELM_STATUS_DISPLACEMENT 0x2u /* |v dt| > L/2: the reference only prints (cuda/SELM_Kernel.cu:363) */
 #define SELM_STATUS_FENE_STRETCH 0x4u
 #define SELM_STATUS_FENE_BROKEN 0x8u
+#define SELM_STATUS_NLIST_OVERFLOW 0x20u /* a monomer had more pair partners in reach than its neighbour list holds */
 
 /* Model.SELM keys (cuda/SELM.cu:17-48) plus the box and dt that the
  * reference takes from LAMMPS (domain->boxlo/hi, update->dt). */

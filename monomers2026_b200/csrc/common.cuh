@@ -23,6 +23,7 @@ enum : uint32_t {
   ERR_FENE_STRETCH = 1u << 2,     // FENE bond past 0.9 R0^2, clamped
   ERR_FENE_BROKEN = 1u << 3,      // FENE bond past the LAMMPS error limit
   ERR_BUCKET_OVERFLOW = 1u << 4,  // candidate list longer than the kernel bound
+  ERR_NLIST_OVERFLOW = 1u << 5,   // more pair partners within the list radius than the list holds
 };
 
 template <typename T> struct cpx_t;
@@ -102,9 +103,16 @@ template <typename T> __device__ __forceinline__ T peskin4(T r) {
   return T(0);
 }
 
+// p mod n in [0, n).  Arguments within one period of [0, n) (stencil and
+// neighbour-cell offsets of in-box positions) take two compares; the integer
+// division only runs for the rest.
 __device__ __forceinline__ int wrapi(int p, int n) {
-  p %= n;
-  return p < 0 ? p + n : p;
+  int q = p < 0 ? p + n : (p >= n ? p - n : p);
+  if ((unsigned)q >= (unsigned)n) {
+    q = p % n;
+    if (q < 0) q += n;
+  }
+  return q;
 }
 
 // ---------------------------------------------------------------- FFT plans

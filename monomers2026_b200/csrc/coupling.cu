@@ -126,27 +126,20 @@ __global__ void k_bin_scatter(const int* __restrict__ bucket_of, int M, int* __r
   unsorted[pos] = p;
 }
 
-// One warp per bucket: rank of every member by monomer index.  Buckets with
-// more than kWarpSortMax members (dense clusters, or every monomer of a job
+// One thread per bucket: rank of every member by monomer index.  Buckets with
+// more than kThreadSortMax members (dense clusters, or every monomer of a job
 // whose state went non-finite) are queued for k_bucket_sort_big instead.
-constexpr int kWarpSortMax = 256;
+constexpr int kThreadSortMax = 32;
 __global__ void k_bucket_sort(const int* __restrict__ offsets, int nbuckets, const int* __restrict__ unsorted,
-                              int* __restrict__ sorted, int* __restrict__ big_list, int* __restrict__ big_count,
-                              int presorted_max) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= nbuckets) return;
-  const int s = offsets[warp], e = offsets[warp + 1];
-  const int n = e - s;
-  if (n <= presorted_max) {  // the consumer orders these itself
-    for (int i = lane; i < n; i += 32) sorted[s + i] = unsorted[s + i];
+                              int* __restrict__ sorted, int* __restrict__ big_list, int* __restrict__ big_count) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbuckets) return;
+  const int s = offsets[b], n = offsets[b + 1] - s;
+  if (n > kThreadSortMax) {
+    big_list[atomicAdd(big_count, 1)] = b;
     return;
   }
-  if (n > kWarpSortMax) {
-    if (lane == 0) big_list[atomicAdd(big_count, 1)] = warp;
-    return;
-  }
-  for (int i = lane; i < n; i += 32) {
+  for (int i = 0; i < n; i++) {
     const int id = unsorted[s + i];
     int rank = 0;
     for (int j = 0; j < n; j++) rank += (unsorted[s + j] < id);
@@ -182,8 +175,6 @@ __global__ void __launch_bounds__(kBigSortThreads) k_bucket_sort_big(const int* 
   }
 }
 
-constexpr int kSpreadChunk = 192;  // candidates per accumulation round of k_spread_tiles
-
 // ---- exclusive scan over n ints (two levels of 4096-element blocks)
 constexpr int kScanThreads = 1024, kScanIpt = 4, kScanBlock = kScanThreads * kScanIpt;
 
@@ -215,7 +206,9 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* sh_warp, int& to
   return r;
 }
 
-__global__ void k_scan_block(const int* __restrict__ in, int* __restrict__ out, long n, int* __restrict__ bsum) {
+__global__ void k_scan_block(const int* __restrict__ in, int* __restrict__ out, long n, int* __restrict__ bsum,
+                             const int* __restrict__ flag) {
+  if (flag && *flag == 0) return;
   __shared__ int sh[33];
   const long base = (long)blockIdx.x * kScanBlock + (long)threadIdx.x * kScanIpt;
   int v[kScanIpt];
@@ -235,11 +228,11 @@ __global__ void k_scan_block(const int* __restrict__ in, int* __restrict__ out, 
   if (threadIdx.x == 0 && bsum) bsum[blockIdx.x] = total;
 }
 
-__global__ void k_scan_add(int* __restrict__ out, long n, const int* __restrict__ boff) {
-  const long base = (long)blockIdx.x * kScanBlock;
-  const int add = boff[blockIdx.x];
-  for (int t = threadIdx.x; t < kScanBlock; t += blockDim.x)
-    if (base + t < n) out[base + t] += add;
+// one element per thread: every block-level offset is added by an independent load and store
+__global__ void k_scan_add(int* __restrict__ out, long n, const int* __restrict__ boff, const int* __restrict__ flag) {
+  if (flag && *flag == 0) return;
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && i >= kScanBlock) out[i] += boff[i / kScanBlock];
 }
 
 long scan_tmp_size(long n) {
@@ -247,21 +240,21 @@ long scan_tmp_size(long n) {
   return 2 * nb + 2;
 }
 
-static cudaError_t exclusive_scan(const int* in, int* out, long n, int* tmp, cudaStream_t st) {
+cudaError_t exclusive_scan(const int* in, int* out, long n, int* tmp, cudaStream_t st, const int* flag) {
   const long nb = (n + kScanBlock - 1) / kScanBlock;
   if (nb > kScanBlock) return cudaErrorInvalidValue;
   if (nb == 1) {
-    k_scan_block<<<1, kScanThreads, 0, st>>>(in, out, n, nullptr);
+    k_scan_block<<<1, kScanThreads, 0, st>>>(in, out, n, nullptr, flag);
     count_launches(1);
     return cudaGetLastError();
   }
   int* bsum = tmp;
   int* boff = tmp + nb;
-  k_scan_block<<<(unsigned)nb, kScanThreads, 0, st>>>(in, out, n, bsum);
+  k_scan_block<<<(unsigned)nb, kScanThreads, 0, st>>>(in, out, n, bsum, flag);
   count_launches(1);
-  k_scan_block<<<1, kScanThreads, 0, st>>>(bsum, boff, nb, nullptr);
+  k_scan_block<<<1, kScanThreads, 0, st>>>(bsum, boff, nb, nullptr, flag);
   count_launches(1);
-  k_scan_add<<<(unsigned)nb, 256, 0, st>>>(out, n, boff);
+  k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(out, n, boff, flag);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -281,15 +274,17 @@ cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBu
   if ((e = cudaMemcpyAsync(bb.cursor, bb.offsets, sizeof(int) * nbk, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
     return e;
   if (M > 0) {
-    if (bs.mode == 2)
-      k_bin_scatter_multi<<<(M + 255) / 256, 256, 0, st>>>(x, rec_b, rec_stride, M, bs, bb.cursor, bb.unsorted);
-    else k_bin_scatter<<<(M + 255) / 256, 256, 0, st>>>(bb.bucket_of, M, bb.cursor, bb.unsorted);
+    if (bs.mode == 2) {
+      // spread tiles: the fixed-point spread does not depend on the order inside a bucket
+      k_bin_scatter_multi<<<(M + 255) / 256, 256, 0, st>>>(x, rec_b, rec_stride, M, bs, bb.cursor, bb.sorted);
+      count_launches(1);
+      return cudaGetLastError();
+    }
+    k_bin_scatter<<<(M + 255) / 256, 256, 0, st>>>(bb.bucket_of, M, bb.cursor, bb.unsorted);
     count_launches(1);
     if ((e = cudaMemsetAsync(bb.big_count, 0, sizeof(int), st)) != cudaSuccess) return e;
-    // spread tiles sort buckets of up to one candidate chunk themselves
-    const int presorted_max = (bs.mode == 2) ? kSpreadChunk : 0;
-    k_bucket_sort<<<(unsigned)((nbk * 32 + 255) / 256), 256, 0, st>>>(bb.offsets, (int)nbk, bb.unsorted, bb.sorted,
-                                                                      bb.big_list, bb.big_count, presorted_max);
+    k_bucket_sort<<<(unsigned)((nbk + 255) / 256), 256, 0, st>>>(bb.offsets, (int)nbk, bb.unsorted, bb.sorted,
+                                                                 bb.big_list, bb.big_count);
     count_launches(1);
     k_bucket_sort_big<<<148, kBigSortThreads, 0, st>>>(bb.offsets, bb.unsorted, bb.sorted, bb.big_list, bb.big_count);
     count_launches(1);
@@ -466,178 +461,180 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
 // Tiles of kTX x kTY x kTZ cells.  bin_particles (mode 2) files every monomer
 // under each tile its union stencil reaches (5 cells per axis,
 // floor(g - 1/2) - 1 .. floor(g) + 2), so a tile's bucket is exactly its list
-// of candidates, ordered by monomer index.  A block per tile stages the
-// candidates' weights in shared memory; one thread per (component, y row,
-// z row) owns a row of kTX cells and subtracts the contributions of the
-// candidates that reach it, in candidate order.
+// of candidates, in no particular order.  A block per tile accumulates the
+// tile in shared memory; a thread takes one z-plane kz of one candidate's
+// component d (12 per candidate), reads the candidate's stencil record, and
+// adds the plane's in-tile points -tf_d wz[kz] wy[jy] wx[ix].
+//
+// Accumulation is in fixed point with shared-memory integer atomics, so the
+// result does not depend on candidate order or thread scheduling (integer
+// addition is exact and associative; no sort, no floating-point atomics).
+// Each contribution carries the impulse pre-scaled by 2^S, chosen per tile
+// from its largest impulse m and its candidate count n, and is rounded to an
+// integer v:
+//   wide   (FP64 grids, or n > 2^16): one 64-bit accumulator per cell,
+//          n m 2^S < 2^61, a step of about n m 2^-61;
+//   split  (FP32 grids): two 32-bit accumulators per cell, v = hi 2^L + lo
+//          with 0 <= lo < 2^L, L = 32 - k and k = ceil(log2 n), so that
+//          neither the sum of the lo parts nor that of the hi parts can
+//          overflow for |v| < 2^(62 - 2k); a step of m 2^-(62-2k), 2^-44 of
+//          the tile's largest impulse for n <= 512.  Shared-memory 32-bit
+//          integer atomics are native; 64-bit ones are not.
 constexpr int kTX = 16, kTY = 8, kTZ = 8;
-constexpr int kSpreadThreads = 3 * kTY * kTZ;
-static_assert(kTY == kTZ && kSpreadThreads == kSpreadChunk, "spread tile rows and chunk size");
-constexpr int kRowPad = kTX + 1;  // odd row stride of the shared accumulators
+constexpr int kSpreadThreads = 3 * kTY * kTZ;  // also the number of tile rows (component, y, z)
+constexpr int kSpreadCells = 3 * kTZ * kTY * kTX;
+static_assert(kTX == 16, "spread_rot assumes 16-cell rows");
 
-template <typename T> struct SpreadCand {
-  int rb[3][2];                       // stencil base relative to the tile, in [0, n): [axis][unshifted, shifted]
-  T w[3][2][4];                       // weight factors [axis][unshifted, shifted][point]
-  T tf[3];                            // impulse per component
-  unsigned char ymask[2], zmask[2];   // tile rows the stencil reaches: [unshifted, shifted]
-};
+// Accumulator slot of cell (cx, cy, cz) of component d.  The x position is
+// rotated by cy + 4 cz within its 16-cell row, so that the four z-planes of
+// one candidate's component (consecutive cz, same cx and cy) fall on distinct
+// banks.
+__device__ __forceinline__ int spread_row(int d, int cy, int cz) { return ((d * kTZ + cz) * kTY + cy) * kTX; }
+__device__ __forceinline__ int spread_rot(int cx, int cy, int cz) { return (cx + cy + 4 * cz) & (kTX - 1); }
 
-// Row (d, ry, rz) of the tile: the candidates that reach it are the set bits
-// of my & mz (candidate masks of this chunk); they are taken in increasing
-// candidate order, so every cell sums its contributions in a fixed order.
-template <typename T>
-__device__ __forceinline__ void spread_rows(const SpreadCand<T>* __restrict__ cand, const unsigned* __restrict__ my,
-                                            const unsigned* __restrict__ mz, int nwords, int d, int ry, int rz,
-                                            int nx, int ny, int nz, int extx, T* __restrict__ acc) {
-  const int sx = (d == 0) ? 0 : 1, sy = (d == 1) ? 0 : 1, sz = (d == 2) ? 0 : 1;
-  for (int wi = 0; wi < nwords; wi++) {
-    unsigned m = my[wi] & mz[wi];
-    while (m) {
-      const int c = wi * 32 + __ffs(m) - 1;
-      m &= m - 1;
-      const SpreadCand<T>& C = cand[c];
-      int jy = ry - C.rb[1][sy];
-      if (jy < 0) jy += ny;
-      int kz = rz - C.rb[2][sz];
-      if (kz < 0) kz += nz;
-      const T dj = (T(1) * C.w[2][sz][kz]) * C.w[1][sy][jy];
-      const T tfd = C.tf[d];
-      const int rbx = C.rb[0][sx];
-#pragma unroll
-      for (int ix = 0; ix < 4; ix++) {
-        int cx = rbx + ix;
-        if (cx >= nx) cx -= nx;
-        if (cx < extx) acc[cx] -= tfd * (dj * C.w[0][sx][ix]);
-      }
-    }
-  }
-}
+__device__ __forceinline__ long long to_fixed(float v) { return __float2ll_rn(v); }
+__device__ __forceinline__ long long to_fixed(double v) { return __double2ll_rn(v); }
+
+template <typename T> struct alignas(4 * sizeof(T)) Vec4 { T v[4]; };
 
 template <typename T>
 __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__ fgrid, int accumulate,
                                                                  const double* __restrict__ x_old,
                                                                  const double* __restrict__ tf, BinSpec bs,
                                                                  const int* __restrict__ offsets,
-                                                                 const int* __restrict__ sorted,
+                                                                 const int* __restrict__ entries,
                                                                  const WRec<T>* __restrict__ rec, CouplingArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  SpreadCand<T>* cand = reinterpret_cast<SpreadCand<T>*>(smem_raw);
-  T* accs = reinterpret_cast<T*>(smem_raw + sizeof(SpreadCand<T>) * kSpreadThreads);
+  __shared__ unsigned long long acc[kSpreadCells];  // wide mode; split mode uses it as lo[cells], hi[cells]
+  __shared__ double wmax[kSpreadThreads / 32];
+  __shared__ int wbad[kSpreadThreads / 32];
+  unsigned* acc_lo = reinterpret_cast<unsigned*>(acc);
+  unsigned* acc_hi = acc_lo + kSpreadCells;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int tb = blockIdx.x;
   const int tbx = tb % bs.nb[0], tby = (tb / bs.nb[0]) % bs.nb[1], tbz = tb / (bs.nb[0] * bs.nb[1]);
-  const int t0[3] = {tbx * kTX, tby * kTY, tbz * kTZ};
-  const int ext[3] = {min(kTX, nx - t0[0]), min(kTY, ny - t0[1]), min(kTZ, nz - t0[2])};
-  const int nn[3] = {nx, ny, nz};
-  const int tid = threadIdx.x;
-  const int d = tid / (kTY * kTZ), r = tid % (kTY * kTZ), ry = r % kTY, rz = r / kTY;
+  const int t0x = tbx * kTX, t0y = tby * kTY, t0z = tbz * kTZ;
+  const int ex = min(kTX, nx - t0x), ey = min(kTY, ny - t0y), ez = min(kTZ, nz - t0z);
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const long N = (long)nx * ny * nz;
-  const bool row_ok = (ry < ext[1]) && (rz < ext[2]);
-  T* row = fgrid + d * N + ((long)(t0[2] + rz) * ny + (t0[1] + ry)) * nx + t0[0];
-  T* acc = accs + tid * kRowPad;
-  for (int cx = 0; cx < kTX; cx++) acc[cx] = (accumulate && row_ok && cx < ext[0]) ? row[cx] : T(0);
-  // candidate masks of the current chunk: [d][row][word], for y rows and z rows
-  __shared__ unsigned masky[3][kTY][kSpreadThreads / 32];
-  __shared__ unsigned maskz[3][kTZ][kSpreadThreads / 32];
-  __shared__ int ids[kSpreadThreads];
-  const int lane = tid & 31, wid = tid >> 5;
-  const int s = offsets[tb], e = offsets[tb + 1];
-  const bool self_sort = (e - s) <= kSpreadThreads;  // larger buckets arrive ordered by monomer index
-  for (int base = s; base < e; base += kSpreadThreads) {
-    const int q = base + tid;
-    unsigned cym[2] = {0u, 0u}, czm[2] = {0u, 0u};
-    int slot = tid;
-    int p = -1;
-    if (self_sort) {
-      if (q < e) ids[tid] = sorted[q];
-      __syncthreads();
-      if (q < e) {
-        p = ids[tid];
-        int r = 0;
-        for (int j = 0; j < e - s; j++) r += (ids[j] < p);
-        slot = r;
-      }
-    } else if (q < e) {
-      p = sorted[q];
+  const int s = offsets[tb], e = offsets[tb + 1], n = e - s;
+  for (int i = tid; i < kSpreadCells; i += kSpreadThreads) acc[i] = 0ull;
+  // fixed-point scale of this tile from its largest impulse component
+  double m = 0.0;
+  int bad = 0;
+  for (int q = s + tid; q < e; q += kSpreadThreads) {
+    const int p = entries[q];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double v = fabs(tf[3L * p + c]);
+      bad |= !(v <= 1.0e300);
+      m = fmax(m, v);
     }
-    if (q < e) {
-      SpreadCand<T> c;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  bad = __any_sync(0xffffffffu, bad);
+  if (lane == 0) {
+    wmax[wid] = m;
+    wbad[wid] = bad;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int w = 0; w < kSpreadThreads / 32; w++) {
+    m = fmax(m, wmax[w]);
+    bad |= wbad[w];
+  }
+  const int k = (n > 1) ? 32 - __clz(n - 1) : 1;  // ceil(log2 n)
+  const bool split = (sizeof(T) == 4) && k <= 16;
+  const int L = 32 - k;
+  int em = 0;
+  if (m > 0.0 && !bad) frexp(split ? m : m * (double)n, &em);  // m (or n m) < 2^em
+  const int S = max(-1000, min(1000, (split ? 62 - 2 * k : 61) - em));
+  const double scale = ldexp(1.0, S), inv_scale = ldexp(1.0, -S);
+  if (!bad) {
+    const int total = 12 * n;
+    for (int u = tid; u < total; u += kSpreadThreads) {
+      const int c = u / 12, r = u - 12 * c;
+      const int d = r >> 2, kz = r & 3;
+      const int sx = (d != 0), sy = (d != 1), sz = (d != 2);
+      const int p = entries[s + c];
+      int bx, by, bz;
+      Vec4<T> wx, wy;
+      T wzk;
       if (rec) {
         const WRec<T>& R = rec[p];
-#pragma unroll
-        for (int ax = 0; ax < 3; ax++)
-#pragma unroll
-          for (int sh = 0; sh < 2; sh++) {
-            int rb = R.b[ax][sh] - t0[ax];
-            if (rb < 0) rb += nn[ax];
-            c.rb[ax][sh] = rb;
-#pragma unroll
-            for (int i = 0; i < 4; i++) c.w[ax][sh][i] = R.w[ax][sh][i];
-          }
-      } else
-#pragma unroll
-      for (int ax = 0; ax < 3; ax++) {
-        const double g = (x_old[3L * p + ax] - a.lo) / a.dx;
-        const double gs = g - 0.5;
-        const int b0 = (int)floor(g) - 1, b1 = (int)floor(gs) - 1;
-        c.rb[ax][0] = wrapi(b0 - t0[ax], nn[ax]);
-        c.rb[ax][1] = wrapi(b1 - t0[ax], nn[ax]);
+        bx = R.b[0][sx];
+        by = R.b[1][sy];
+        bz = R.b[2][sz];
+        wx = *reinterpret_cast<const Vec4<T>*>(R.w[0][sx]);
+        wy = *reinterpret_cast<const Vec4<T>*>(R.w[1][sy]);
+        wzk = R.w[2][sz][kz];
+      } else {
+        const double gx = (x_old[3L * p] - a.lo) / a.dx - (sx ? 0.5 : 0.0);
+        const double gy = (x_old[3L * p + 1] - a.lo) / a.dx - (sy ? 0.5 : 0.0);
+        const double gz = (x_old[3L * p + 2] - a.lo) / a.dx - (sz ? 0.5 : 0.0);
+        const int fx = (int)floor(gx) - 1, fy = (int)floor(gy) - 1, fz = (int)floor(gz) - 1;
+        bx = wrapi(fx, nx);
+        by = wrapi(fy, ny);
+        bz = wrapi(fz, nz);
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-          c.w[ax][0][i] = ref_weight<T>(fabs(g - (double)(b0 + i)));
-          c.w[ax][1][i] = ref_weight<T>(fabs(gs - (double)(b1 + i)));
+          wx.v[i] = ref_weight<T>(fabs(gx - (double)(fx + i)));
+          wy.v[i] = ref_weight<T>(fabs(gy - (double)(fy + i)));
         }
+        wzk = ref_weight<T>(fabs(gz - (double)(fz + kz)));
       }
+      // tile-relative plane and rows
+      int cz = bz + kz - t0z;
+      if (cz < 0) cz += nz;
+      if (cz >= nz) cz -= nz;
+      if (cz >= ez) continue;
+      int cx0 = bx - t0x;
+      if (cx0 < 0) cx0 += nx;
+      int cy0 = by - t0y;
+      if (cy0 < 0) cy0 += ny;
+      const T fz = (T)(-tf[3L * p + d] * scale) * wzk;
 #pragma unroll
-      for (int sh = 0; sh < 2; sh++) {
-        unsigned ym = 0, zm = 0;
-        for (int rr = 0; rr < 8; rr++) {
-          int jy = rr - c.rb[1][sh];
-          if (jy < 0) jy += ny;
-          int kz = rr - c.rb[2][sh];
-          if (kz < 0) kz += nz;
-          ym |= (unsigned)(jy < 4 && rr < ext[1]) << rr;
-          zm |= (unsigned)(kz < 4 && rr < ext[2]) << rr;
-        }
-        c.ymask[sh] = (unsigned char)ym;
-        c.zmask[sh] = (unsigned char)zm;
-        cym[sh] = ym;
-        czm[sh] = zm;
-      }
+      for (int jy = 0; jy < 4; jy++) {
+        int cy = cy0 + jy;
+        if (cy >= ny) cy -= ny;
+        if (cy < ey) {
+          const T rowf = fz * wy.v[jy];
+          const int row = spread_row(d, cy, cz);
 #pragma unroll
-      for (int dd = 0; dd < 3; dd++) c.tf[dd] = (T)tf[3L * p + dd];
-      cand[slot] = c;
-    }
-    if (self_sort) {
-      __syncthreads();
-      if (q < e)
-#pragma unroll
-        for (int sh = 0; sh < 2; sh++) {
-          cym[sh] = cand[tid].ymask[sh];
-          czm[sh] = cand[tid].zmask[sh];
-        }
-    }
-    // warp ballots: which of this warp's 32 candidates (slots) reach each row
-#pragma unroll
-    for (int dd = 0; dd < 3; dd++) {
-      const int shy = (dd == 1) ? 0 : 1, shz = (dd == 2) ? 0 : 1;
-#pragma unroll
-      for (int rr = 0; rr < kTY; rr++) {
-        const unsigned by = __ballot_sync(0xffffffffu, (cym[shy] >> rr) & 1u);
-        const unsigned bz = __ballot_sync(0xffffffffu, (czm[shz] >> rr) & 1u);
-        if (lane == 0) {
-          masky[dd][rr][wid] = by;
-          maskz[dd][rr][wid] = bz;
+          for (int ix = 0; ix < 4; ix++) {
+            int cx = cx0 + ix;
+            if (cx >= nx) cx -= nx;
+            if (cx < ex) {
+              const long long v = to_fixed(rowf * wx.v[ix]);
+              const int slot = row + spread_rot(cx, cy, cz);
+              if (split) {
+                atomicAdd(acc_lo + slot, (unsigned)v & (0xffffffffu >> k));
+                atomicAdd(acc_hi + slot, (unsigned)(v >> L));
+              } else {
+                atomicAdd(acc + slot, (unsigned long long)v);
+              }
+            }
+          }
         }
       }
     }
-    __syncthreads();
-    const int nwords = (min(kSpreadThreads, e - base) + 31) / 32;
-    if (row_ok) spread_rows(cand, masky[d][ry], maskz[d][rz], nwords, d, ry, rz, nx, ny, nz, ext[0], acc);
-    __syncthreads();
   }
-  if (row_ok)
-    for (int cx = 0; cx < ext[0]; cx++) row[cx] = acc[cx];
+  __syncthreads();
+  // cells out, a half-warp per 16-cell row
+  // a non-finite impulse makes the whole tile non-finite, as a floating-point sum would
+  const double nan_or_zero = bad ? __longlong_as_double(0x7ff8000000000000LL) : 0.0;
+  for (int idx = tid; idx < kSpreadCells; idx += kSpreadThreads) {
+    const int row = idx / kTX, cx = idx % kTX;
+    const int cy = row % kTY, cz = (row / kTY) % kTZ, d = row / (kTY * kTZ);
+    if (cx < ex && cy < ey && cz < ez) {
+      T* dst = fgrid + d * N + ((long)(t0z + cz) * ny + (t0y + cy)) * nx + t0x + cx;
+      const int slot = row * kTX + spread_rot(cx, cy, cz);
+      const long long sum = split ? (long long)(int)acc_hi[slot] * (1ll << L) + (long long)acc_lo[slot]
+                                  : (long long)acc[slot];
+      const double add = (double)sum * inv_scale + nan_or_zero;
+      *dst = accumulate ? (T)((double)*dst + add) : (T)add;
+    }
+  }
 }
 
 BinSpec spread_bin_spec(const int dims[3], double lo, double dx) {
@@ -685,16 +682,8 @@ cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const 
     return cudaMemsetAsync(fgrid, 0, sizeof(T) * 3L * a.nx * a.ny * a.nz, st);
   }
   if (bs.mode != 2 || bs.tile[0] != kTX || bs.tile[1] != kTY || bs.tile[2] != kTZ) return cudaErrorInvalidValue;
-  const size_t sm = sizeof(SpreadCand<T>) * kSpreadThreads + sizeof(T) * kSpreadThreads * kRowPad;
-  static bool attr_set = false;  // set once per precision, outside any stream capture after the first call
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute((const void*)k_spread_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sm);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
-  k_spread_tiles<T><<<ntiles, kSpreadThreads, sm, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets, sorted,
-                                                         rec, a);
+  k_spread_tiles<T><<<ntiles, kSpreadThreads, 0, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets, sorted,
+                                                        rec, a);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -705,16 +694,8 @@ template cudaError_t interp_update<double>(const double*, const double*, double*
 template cudaError_t interp_update<float>(const float*, const double*, double*, double*, double*, const double*,
                                           double*, const int*, WRec<float>*, const CouplingArgs&, uint32_t*,
                                           cudaStream_t);
-// sets the shared-memory attribute of the spread kernels ahead of any stream capture
-cudaError_t spread_prepare_attributes() {
-  const size_t s64 = sizeof(SpreadCand<double>) * kSpreadThreads + sizeof(double) * kSpreadThreads * kRowPad;
-  const size_t s32 = sizeof(SpreadCand<float>) * kSpreadThreads + sizeof(float) * kSpreadThreads * kRowPad;
-  cudaError_t e = cudaFuncSetAttribute((const void*)k_spread_tiles<double>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s64);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute((const void*)k_spread_tiles<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)s32);
-}
+// the spread kernels use static shared memory only (kept for the engine's set-up order)
+cudaError_t spread_prepare_attributes() { return cudaSuccess; }
 
 template cudaError_t spread_gather<double>(double*, bool, const double*, const double*, const BinSpec&, const int*,
                                            const int*, const CouplingArgs&, cudaStream_t, const WRec<double>*);

@@ -359,7 +359,7 @@ template <typename T, int N> constexpr size_t smem_xy_fast() {
 }
 template <typename T> constexpr int wb_fast() { return sizeof(T) == 8 ? 8 : 16; }
 template <typename T, int N> constexpr size_t smem_z_fast() {
-  return sizeof(cpx<T>) * (2 * (size_t)N * 3 * wb_fast<T>() + N);
+  return sizeof(cpx<T>) * ((size_t)N * 3 * wb_fast<T>() + N);
 }
 
 template <typename T, int N> static cudaError_t fast_attrs() {
@@ -387,9 +387,8 @@ static void fast_launch(const T* fp, cpx<T>* work, cpx<T>* uhat, T* u, const ZGe
   count_launches(1);
   prof_mark(s, "xy_forward", false);
   prof_mark(s, "z_update", true);
-  const int nblk = (zg.nxh + WB - 1) / WB;
-  k_z_update_fast<T, N, WB><<<(unsigned)(ny * nblk), 256, smem_z_fast<T, N>(), st>>>(work, uhat, zg, tb.wz_f, symx,
-                                                                                      symy, symz);
+  k_z_update_fast<T, N, WB><<<(unsigned)z_blocks<WB>(zg.nxh, ny), 256, smem_z_fast<T, N>(), st>>>(
+      work, uhat, zg, tb.wz_f, symx, symy, symz);
   count_launches(1);
   prof_mark(s, "z_update", false);
   prof_mark(s, "xy_inverse", true);
@@ -626,8 +625,7 @@ template <typename T> static int fused_step_t(selm_sim* s) {
     CUF(interp_update<T>((const T*)z->u, xo, xn, s->v, s->f, s->m, s->tf, nullptr, rec, a, s->err, s->st));
     prof_mark(s, "interp_update", false);
     prof_mark(s, "bin", true);
-    CUF(bin_particles(xo, s->M, s->tiles, s->tbb, s->st, reinterpret_cast<const int*>(rec),
-                      (int)(sizeof(WRec<T>) / sizeof(int))));
+    CUF(bin_particles(xo, s->M, s->tiles, s->tbb, s->st, wrec_bases(rec), wrec_stride<T>()));
     prof_mark(s, "bin", false);
     prof_mark(s, "spread", true);
     CUF(spread_gather<T>((T*)z->fp, false, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st, rec));

@@ -3,9 +3,11 @@
 // Same arithmetic contract as the generic kernels of fluid_fused.cu:
 //   k_xy_forward_fast : per (component, z) plane, x r2c (two rows per complex
 //                       line) and y FFT -> half spectrum [c][z][y][x];
-//   k_z_update_fast   : per (y, block of Wb x modes): z FFT, the spectral
-//                       update (viscous factor, projection, Philox noise, zero
-//                       mode), inverse z FFT with the 1/N normalisation;
+//   k_z_update_fast   : per block of Wb z-lines (Wb x modes of one y, or the
+//                       last x mode of Wb y rows): z FFT, the spectral update
+//                       (viscous factor, projection, Philox noise, zero mode)
+//                       with u_hat read and written in place, inverse z FFT
+//                       with the 1/N normalisation;
 //   k_xy_inverse_fast : inverse y FFT and x c2r, writing u.
 // Shared-memory lines are stored line-fastest (element t of line l at
 // t*stride + l), so threads of consecutive lines touch consecutive words.
@@ -206,6 +208,16 @@ __device__ __forceinline__ void noise_draw_fast(const ZGeom& g, uint64_t step, i
   }
 }
 
+// Column blocks of the z kernel.  A "main" block takes WB consecutive
+// x-columns i0 .. i0+WB-1 (all below the last column nxh-1) of one y-row; a
+// "tail" block takes the last column i = nxh-1 of WB consecutive y-rows, so
+// that no block runs with a single line (for even nx that column is the
+// Nyquist plane).  Blocks 0 .. ny*nmb-1 are main blocks, the rest tail blocks.
+template <int WB> __host__ __device__ __forceinline__ int z_main_blocks(int nxh) { return (nxh - 1 + WB - 1) / WB; }
+template <int WB> __host__ __device__ __forceinline__ int z_blocks(int nxh, int ny) {
+  return ny * z_main_blocks<WB>(nxh) + (ny + WB - 1) / WB;
+}
+
 template <typename T, int N, int WB>
 __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work, cpx<T>* __restrict__ uhat, ZGeom g,
                                                        const cpx<T>* __restrict__ twz,
@@ -217,116 +229,134 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
   constexpr int NL = 3 * WB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* A = reinterpret_cast<C*>(smem_raw);  // element t of line (c, w) at t*NL + c*WB + w
-  C* U = A + N * NL;                      // u_hat block, mode k of line (c, w) at k*NL + c*WB + w
-  C* tw = U + N * NL;
+  C* tw = A + N * NL;
   const int nxh = g.nxh, ny = g.ny;
-  const int nblk = (nxh + WB - 1) / WB;
-  const int j = blockIdx.x / nblk;
-  const int i0 = (blockIdx.x % nblk) * WB;
-  const int wn = min(WB, nxh - i0);
+  const int nmb = z_main_blocks<WB>(nxh);
+  const bool tail = (int)blockIdx.x >= ny * nmb;
+  int i0, j0, wn;
+  if (!tail) {
+    j0 = blockIdx.x / nmb;
+    i0 = (blockIdx.x % nmb) * WB;
+    wn = min(WB, nxh - 1 - i0);
+  } else {
+    i0 = nxh - 1;
+    j0 = (blockIdx.x - ny * nmb) * WB;
+    wn = min(WB, ny - j0);
+  }
   const long plane = (long)ny * nxh;
+  const long cstep = tail ? nxh : 1;  // main lines step in x, tail lines in y
+  const long col0 = (long)j0 * nxh + i0;
   for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twz[t];
   __syncthreads();
   // pass A forward, loading straight from global: thread (line, n2)
   for (int u = threadIdx.x; u < NL * N2; u += blockDim.x) {
     const int l = u % NL, n2 = u / NL;
     const int c = l / WB, w = l % WB;
+    const bool ok = w < wn;
+    const long cb = (long)c * N * plane + col0 + w * cstep;
     C v[N1];
 #pragma unroll
-    for (int n1 = 0; n1 < N1; n1++) {
-      const long gi = ((long)c * N + (N2 * n1 + n2)) * plane + (long)j * nxh + i0 + w;
-      const bool ok = w < wn;
-      v[n1] = ok ? work[gi] : fftk::mk<C>(T(0), T(0));
-      U[(N2 * n1 + n2) * NL + l] = ok ? uhat[gi] : fftk::mk<C>(T(0), T(0));
-    }
+    for (int n1 = 0; n1 < N1; n1++) v[n1] = ok ? work[cb + (N2 * n1 + n2) * plane] : fftk::mk<C>(T(0), T(0));
     fftk::dft<N1, -1>(v);
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) A[(N2 * k1 + n2) * NL + l] = (k1 == 0) ? v[0] : cmul(v[k1], tw[n2 * k1]);
   }
   __syncthreads();
-  // pass B forward, update, pass B inverse: thread (w, k1) for all three components
+  // pass B forward in place: thread (line, k1); position N2 k1 + k2 then holds mode k1 + N1 k2
+  for (int u = threadIdx.x; u < NL * N1; u += blockDim.x) {
+    const int l = u % NL, k1 = u / NL;
+    C v[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; n2++) v[n2] = A[(N2 * k1 + n2) * NL + l];
+    fftk::dft<N2, -1>(v);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) A[(N2 * k1 + k2) * NL + l] = v[k2];
+  }
+  __syncthreads();
+  // spectral update: thread (w, k) for all three components, u_hat read and written in place
   const uint64_t step = *g.step;
   const T invN = (T)(1.0 / ((double)g.nx * ny * N));
-  for (int u = threadIdx.x; u < WB * N1; u += blockDim.x) {
-    const int w = u % WB, k1 = u / WB;
+  const double idx2 = 1.0 / (g.dx * g.dx);
+  const T idx1 = (T)(1.0 / g.dx);
+  const T irho = (T)(1.0 / g.rho);
+  const long cplane = (long)N * plane;
+#pragma unroll 1
+  for (int u = threadIdx.x; u < WB * N; u += blockDim.x) {
+    const int w = u % WB, k = u / WB;
     if (w >= wn) continue;
-    const int i = i0 + w;
-    C X[3][N2];
+    const int i = tail ? i0 : i0 + w, j = tail ? j0 + w : j0;
+    const long gk = (long)k * plane + col0 + w * cstep;
+    const int pa = dpos<N1, N2>(k) * NL + w;
+    C X[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-#pragma unroll
-      for (int n2 = 0; n2 < N2; n2++) X[c][n2] = A[(N2 * k1 + n2) * NL + c * WB + w];
-      fftk::dft<N2, -1>(X[c]);
-    }
+    for (int c = 0; c < 3; c++) X[c] = A[pa + c * WB];
     const double cx = symx[2 * i], sx = symx[2 * i + 1];
     const double cy = symy[2 * j], sy = symy[2 * j + 1];
-    const double idx2 = 1.0 / (g.dx * g.dx);
-    const T idx1 = (T)(1.0 / g.dx);
-    const T irho = (T)(1.0 / g.rho);
+    const double cz = symz[2 * k], sz = symz[2 * k + 1];
+    if (g.stochastic) {
+      double2 Xn[3];
+      noise_draw_fast<T, N>(g, step, i, j, k, cx, cy, cz, Xn);
+      if (i == 0 || ((g.nx & 1) == 0 && i == g.nx / 2)) {
+        const int jc = (ny - j) % ny, kc = (N - k) % N;
+        if (jc != j || kc != k) {
+          double2 Xc[3];
+          noise_draw_fast<T, N>(g, step, i, jc, kc, cx, symy[2 * jc], symz[2 * kc], Xc);
+          const double s = (g.noise_mode == 1) ? 0.7071067811865476 : 0.5;
 #pragma unroll
-    for (int k2 = 0; k2 < N2; k2++) {
-      const int k = k1 + N1 * k2;
-      const double cz = symz[2 * k], sz = symz[2 * k + 1];
-      if (g.stochastic) {
-        double2 Xn[3];
-        noise_draw_fast<T, N>(g, step, i, j, k, cx, cy, cz, Xn);
-        if (i == 0 || ((g.nx & 1) == 0 && i == g.nx / 2)) {
-          const int jc = (ny - j) % ny, kc = (N - k) % N;
-          if (jc != j || kc != k) {
-            double2 Xc[3];
-            noise_draw_fast<T, N>(g, step, i, jc, kc, cx, symy[2 * jc], symz[2 * kc], Xc);
-            const double s = (g.noise_mode == 1) ? 0.7071067811865476 : 0.5;
+          for (int c = 0; c < 3; c++) Xn[c] = make_double2((Xn[c].x + Xc[c].x) * s, (Xn[c].y - Xc[c].y) * s);
+        } else {
 #pragma unroll
-            for (int c = 0; c < 3; c++) Xn[c] = make_double2((Xn[c].x + Xc[c].x) * s, (Xn[c].y - Xc[c].y) * s);
-          } else {
-#pragma unroll
-            for (int c = 0; c < 3; c++) Xn[c].y = 0.0;
-          }
+          for (int c = 0; c < 3; c++) Xn[c].y = 0.0;
         }
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          X[c][k2].x += (T)(g.noise_amp * Xn[c].x);
-          X[c][k2].y += (T)(g.noise_amp * Xn[c].y);
-        }
-      }
-      C un[3];
-      if (i == 0 && j == 0 && k == 0) {
-#pragma unroll
-        for (int c = 0; c < 3; c++) un[c] = fftk::mk<C>(T(0), T(0));
-      } else {
-        const double Lk = 2.0 * (cx + cy + cz) * idx2;
-        const T visc = (T)(1.0 + g.mu * g.dt * Lk / g.rho);
-        C us[3];
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          const C uh = U[k * NL + c * WB + w];
-          us[c] = fftk::mk<C>(uh.x * visc + X[c][k2].x * irho, uh.y * visc + X[c][k2].y * irho);
-        }
-        const C D[3] = {fftk::mk<C>((T)cx * idx1, (T)sx * idx1), fftk::mk<C>((T)cy * idx1, (T)sy * idx1),
-                        fftk::mk<C>((T)cz * idx1, (T)sz * idx1)};
-        C s = cmul(D[0], us[0]);
-        s = cadd(s, cmul(D[1], us[1]));
-        s = cadd(s, cmul(D[2], us[2]));
-        const T iL = (T)(1.0 / Lk);
-        s = fftk::mk<C>(s.x * iL, s.y * iL);
-#pragma unroll
-        for (int c = 0; c < 3; c++) un[c] = csub(us[c], cmul(fftk::mk<C>(-D[c].x, D[c].y), s));
       }
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        U[k * NL + c * WB + w] = un[c];
-        X[c][k2] = fftk::mk<C>(un[c].x * invN, un[c].y * invN);
+        X[c].x += (T)(g.noise_amp * Xn[c].x);
+        X[c].y += (T)(g.noise_amp * Xn[c].y);
       }
+    }
+    C un[3];
+    if (i == 0 && j == 0 && k == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) un[c] = fftk::mk<C>(T(0), T(0));
+    } else {
+      const double Lk = 2.0 * (cx + cy + cz) * idx2;
+      const T visc = (T)(1.0 + g.mu * g.dt * Lk / g.rho);
+      C us[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const C uh = uhat[gk + c * cplane];
+        us[c] = fftk::mk<C>(uh.x * visc + X[c].x * irho, uh.y * visc + X[c].y * irho);
+      }
+      const C D[3] = {fftk::mk<C>((T)cx * idx1, (T)sx * idx1), fftk::mk<C>((T)cy * idx1, (T)sy * idx1),
+                      fftk::mk<C>((T)cz * idx1, (T)sz * idx1)};
+      C s = cmul(D[0], us[0]);
+      s = cadd(s, cmul(D[1], us[1]));
+      s = cadd(s, cmul(D[2], us[2]));
+      const T iL = (T)(1.0 / Lk);
+      s = fftk::mk<C>(s.x * iL, s.y * iL);
+#pragma unroll
+      for (int c = 0; c < 3; c++) un[c] = csub(us[c], cmul(fftk::mk<C>(-D[c].x, D[c].y), s));
     }
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      fftk::dft<N2, +1>(X[c]);
+      uhat[gk + c * cplane] = un[c];
+      A[pa + c * WB] = fftk::mk<C>(un[c].x * invN, un[c].y * invN);
+    }
+  }
+  __syncthreads();
+  // pass B inverse in place: thread (line, k1)
+  for (int u = threadIdx.x; u < NL * N1; u += blockDim.x) {
+    const int l = u % NL, k1 = u / NL;
+    C v[N2];
 #pragma unroll
-      for (int n2 = 0; n2 < N2; n2++) {
-        C w2 = tw[n2 * k1];
-        w2.y = -w2.y;
-        A[(N2 * k1 + n2) * NL + c * WB + w] = (n2 == 0 || k1 == 0) ? X[c][n2] : cmul(X[c][n2], w2);
-      }
+    for (int k2 = 0; k2 < N2; k2++) v[k2] = A[(N2 * k1 + k2) * NL + l];
+    fftk::dft<N2, +1>(v);
+#pragma unroll
+    for (int n2 = 0; n2 < N2; n2++) {
+      C w2 = tw[n2 * k1];
+      w2.y = -w2.y;
+      A[(N2 * k1 + n2) * NL + l] = (n2 == 0 || k1 == 0) ? v[n2] : cmul(v[n2], w2);
     }
   }
   __syncthreads();
@@ -339,12 +369,9 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
     for (int k1 = 0; k1 < N1; k1++) v[k1] = A[(N2 * k1 + n2) * NL + l];
     fftk::dft<N1, +1>(v);
     if (w < wn) {
+      const long cb = (long)c * N * plane + col0 + w * cstep;
 #pragma unroll
-      for (int n1 = 0; n1 < N1; n1++) {
-        const long gi = ((long)c * N + (N2 * n1 + n2)) * plane + (long)j * nxh + i0 + w;
-        work[gi] = v[n1];
-        uhat[gi] = U[(N2 * n1 + n2) * NL + l];
-      }
+      for (int n1 = 0; n1 < N1; n1++) work[cb + (N2 * n1 + n2) * plane] = v[n1];
     }
   }
 }

@@ -5,32 +5,168 @@
 // Here one thread per monomer gathers, in a fixed order, its incident bonds
 // (bond_style harmonic E = K(r-r0)^2, or fene: -K R0^2/2 ln(1-(r/R0)^2) plus
 // the WCA core below 2^(1/6) sigma), incident angles (angle_style harmonic
-// E = K(theta-theta0)^2), lj/cut pairs from the 27 neighbouring force cells
+// E = K(theta-theta0)^2), lj/cut pairs from its Verlet neighbour list
 // (special_bonds weights applied), then the uniform body force.  No atomics,
 // so the force on every monomer is reproducible bit for bit.
+//
+// The neighbour list (partners within the largest cutoff plus a skin, sorted
+// by index, pairs of special weight 0 left out) is rebuilt from force cells
+// of edge >= that radius whenever some monomer has moved more than half the
+// skin since the last build, as LAMMPS' neighbor ... check yes does; between
+// rebuilds the rebuild kernels return at once, so a captured step graph is
+// the same every step.
 #include "common.cuh"
 #include "selm_kernels.h"
 
 namespace selm {
 
-__device__ __forceinline__ double min_img(double d, double L) { return d - L * rint(d / L); }
-
-// monomers in cell order: xs[q] = (x, y, z, type) of sorted[q]
-__global__ void k_gather_cells(const double* __restrict__ x, const int* __restrict__ type, const int* __restrict__ sorted,
-                               int M, double4* __restrict__ xs) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= M) return;
-  const int p = sorted[q];
-  xs[q] = make_double4(x[3 * p], x[3 * p + 1], x[3 * p + 2], (double)type[p]);
+// d - L rint(d / L); the quotient rounds to 0 whenever |d| < 0.49 L, so the
+// division is skipped there (same result bit for bit)
+__device__ __forceinline__ double min_img(double d, double L) {
+  if (fabs(d) < 0.49 * L) return d;
+  return d - L * rint(d / L);
 }
 
-__global__ void k_forces(const double* __restrict__ x, double* __restrict__ f, ForceTopo t, BinSpec cells,
-                         const int* __restrict__ offsets, const int* __restrict__ sorted,
-                         const double4* __restrict__ xcell, uint32_t* err) {
-  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= t.M) return;
-  // threads follow the cell order when a pair list exists, so a warp's monomers are neighbours
-  const int i = (t.pair_style && t.M > 1) ? sorted[slot] : slot;
+// ---------------------------------------------------------------- neighbour list
+__device__ __forceinline__ int force_cell(double x, double lo, double L, int nc) {
+  return wrapi((int)floor((x - lo) / L * nc), nc);
+}
+
+// a rebuild is due when some monomer moved more than skin/2 since the last build
+__global__ void k_nl_check(const double* __restrict__ x, const double* __restrict__ xb, int M, double L,
+                           double half_skin2, int* __restrict__ flag) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  bool move = false;
+  if (p < M) {
+    const double dx = min_img(x[3 * p] - xb[3 * p], L), dy = min_img(x[3 * p + 1] - xb[3 * p + 1], L),
+                 dz = min_img(x[3 * p + 2] - xb[3 * p + 2], L);
+    move = !(dx * dx + dy * dy + dz * dz <= half_skin2);  // a non-finite position rebuilds too
+  }
+  if (__any_sync(0xffffffffu, move) && (threadIdx.x & 31) == 0) *flag = 1;
+}
+
+__global__ void k_nl_count(const double* __restrict__ x, int M, double lo, double L, int nc,
+                           int* __restrict__ counts, int* __restrict__ cellof, const int* __restrict__ flag) {
+  if (*flag == 0) return;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= M) return;
+  const int c = (force_cell(x[3 * p + 2], lo, L, nc) * nc + force_cell(x[3 * p + 1], lo, L, nc)) * nc +
+                force_cell(x[3 * p], lo, L, nc);
+  cellof[p] = c;
+  atomicAdd(&counts[c], 1);
+}
+
+// members[] grouped by cell (in no particular order within a cell); counts
+// return to zero, ready for the next rebuild
+__global__ void k_nl_scatter(const int* __restrict__ cellof, int M, const int* __restrict__ offsets,
+                             int* __restrict__ counts, int* __restrict__ members, const int* __restrict__ flag) {
+  if (*flag == 0) return;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= M) return;
+  const int c = cellof[p];
+  members[offsets[c] + atomicSub(&counts[c], 1) - 1] = p;
+}
+
+// thread per member slot q (so a warp covers neighbouring cells): partners of
+// i = members[q] within rl from the 27 cells, inserted in index order
+__global__ void k_nl_build(const double* __restrict__ x, ForceTopo t, int nc, const int* __restrict__ offsets,
+                           const int* __restrict__ members, NeighborList nl, uint32_t* err,
+                           const int* __restrict__ flag) {
+  if (*flag == 0) return;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= t.M) return;
+  const int M = t.M;
+  const int i = members[q];
+  const double L = t.hi - t.lo;
+  const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
+  int* out = nl.idx + i;  // entry k at out[k * M]
+  int n = 0;
+  bool over = false;
+  auto scan = [&](int q0, int q1) {
+    for (int r = q0; r < q1; r++) {
+      const int j = members[r];
+      if (j == i) continue;
+      const double dx = min_img(xi - x[3 * j], L), dy = min_img(yi - x[3 * j + 1], L),
+                   dz = min_img(zi - x[3 * j + 2], L);
+      if (!(dx * dx + dy * dy + dz * dz < nl.rl2)) continue;
+      int cls = 0;
+      for (int s = t.sp_off[i]; s < t.sp_off[i + 1]; s++)
+        if (t.sp_nbr[s] == j) {
+          const double w = t.sp_w[s];
+          cls = (w == nl.wtab[1]) ? 1 : (w == nl.wtab[2]) ? 2 : 3;
+          break;
+        }
+      if (nl.wtab[cls] == 0.0) continue;
+      if (n == nl.cap) {
+        over = true;
+        continue;
+      }
+      // insertion by partner index
+      int k = n;
+      while (k > 0 && (out[(long)(k - 1) * M] & 0x3fffffff) > j) {
+        out[(long)k * M] = out[(long)(k - 1) * M];
+        k--;
+      }
+      out[(long)k * M] = (int)((unsigned)j | ((unsigned)cls << 30));
+      n++;
+    }
+  };
+  if (nc == 1) {
+    scan(offsets[0], offsets[1]);
+  } else {
+    const int cx = force_cell(xi, t.lo, L, nc), cy = force_cell(yi, t.lo, L, nc), cz = force_cell(zi, t.lo, L, nc);
+    // the three x-neighbour cells of a (y, z) row are contiguous in the cell
+    // order, except across the periodic edge (two ranges there)
+    for (int oz = -1; oz <= 1; oz++) {
+      const int zc = wrapi(cz + oz, nc) * nc;
+      for (int oy = -1; oy <= 1; oy++) {
+        const int rowc = (zc + wrapi(cy + oy, nc)) * nc;
+        if (cx >= 1 && cx <= nc - 2) {
+          scan(offsets[rowc + cx - 1], offsets[rowc + cx + 2]);
+        } else if (cx == 0) {
+          scan(offsets[rowc + nc - 1], offsets[rowc + nc]);
+          scan(offsets[rowc], offsets[rowc + 2]);
+        } else {
+          scan(offsets[rowc + nc - 2], offsets[rowc + nc]);
+          scan(offsets[rowc], offsets[rowc + 1]);
+        }
+      }
+    }
+  }
+  nl.cnt[i] = n;
+  nl.xb[3 * i] = xi;
+  nl.xb[3 * i + 1] = yi;
+  nl.xb[3 * i + 2] = zi;
+  if (over) atomicOr(err, ERR_NLIST_OVERFLOW);
+}
+
+cudaError_t neighbor_update(const double* x, const ForceTopo& t, const BinSpec& cells, const BinBuffers& bb,
+                            const NeighborList& nl, uint32_t* err, cudaStream_t st) {
+  const int M = t.M;
+  if (M <= 1 || !t.pair_style) return cudaSuccess;
+  const int nc = cells.n[0];
+  const long nbk = (long)nc * nc * nc;
+  const double L = t.hi - t.lo;
+  const unsigned g = (unsigned)((M + 255) / 256);
+  k_nl_check<<<g, 256, 0, st>>>(x, nl.xb, M, L, nl.half_skin2, nl.flag);
+  count_launches(1);
+  k_nl_count<<<g, 256, 0, st>>>(x, M, t.lo, L, nc, bb.counts, bb.bucket_of, nl.flag);
+  count_launches(1);
+  cudaError_t e = exclusive_scan(bb.counts, bb.offsets, nbk + 1, bb.scan_tmp, st, nl.flag);
+  if (e != cudaSuccess) return e;
+  k_nl_scatter<<<g, 256, 0, st>>>(bb.bucket_of, M, bb.offsets, bb.counts, bb.sorted, nl.flag);
+  count_launches(1);
+  k_nl_build<<<(unsigned)((M + 127) / 128), 128, 0, st>>>(x, t, nc, bb.offsets, bb.sorted, nl, err, nl.flag);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- forces
+__global__ void __launch_bounds__(128) k_forces(const double* __restrict__ x, double* __restrict__ f, ForceTopo t,
+                                                NeighborList nl, int use_nl, uint32_t* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (use_nl && i == 0) *nl.flag = 0;  // the list is current; the next check decides again
+  if (i >= t.M) return;
   const double L = t.hi - t.lo;
   const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
   double fx = 0.0, fy = 0.0, fz = 0.0;
@@ -90,47 +226,26 @@ __global__ void k_forces(const double* __restrict__ x, double* __restrict__ f, F
       if (i == a3) { fx += f3x; fy += f3y; fz += f3z; }
     }
   }
-  if (t.pair_style && t.M > 1) {
-    const int nc = cells.n[0];
+  if (use_nl) {
+    const int M = t.M;
     const int nt1 = t.ntypes + 1;
     const int ti = t.type[i];
-    int c3[3];
-    const double xs[3] = {xi, yi, zi};
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      int c = (int)floor((xs[a] - t.lo) / L * nc);
-      c3[a] = wrapi(c, nc);
-    }
-    const int span = (nc == 1) ? 0 : 1;
+    const int n = nl.cnt[i];
     double px = 0.0, py = 0.0, pz = 0.0;
-    for (int oz = -span; oz <= span; oz++)
-      for (int oy = -span; oy <= span; oy++)
-        for (int ox = -span; ox <= span; ox++) {
-          const int cc = (wrapi(c3[2] + oz, nc) * nc + wrapi(c3[1] + oy, nc)) * nc + wrapi(c3[0] + ox, nc);
-          const int qe = offsets[cc + 1];
-          for (int q = offsets[cc]; q < qe; q++) {
-            if (q == slot) continue;
-            const double4 xj = xcell[q];
-            const double dx = min_img(xi - xj.x, L), dy = min_img(yi - xj.y, L), dz = min_img(zi - xj.z, L);
-            const double rsq = dx * dx + dy * dy + dz * dz;
-            if (rsq >= t.rc2max) continue;
-            const int j = sorted[q];
-            double w = 1.0;
-            for (int s = t.sp_off[i]; s < t.sp_off[i + 1]; s++)
-              if (t.sp_nbr[s] == j) {
-                w = t.sp_w[s];
-                break;
-              }
-            if (w == 0.0) continue;
-            const double* pc = t.pair_coeff + 3 * (ti * nt1 + (int)xj.w);
-            if (rsq >= pc[2] * pc[2] || rsq <= 0.0) continue;
-            const double r2i = 1.0 / rsq, s2 = pc[1] * pc[1] * r2i, s6 = s2 * s2 * s2;
-            const double fp = w * 24.0 * pc[0] * s6 * (2.0 * s6 - 1.0) * r2i;
-            px += dx * fp;
-            py += dy * fp;
-            pz += dz * fp;
-          }
-        }
+    for (int k = 0; k < n; k++) {
+      const int e = nl.idx[(long)k * M + i];
+      const int j = e & 0x3fffffff, cls = (int)((unsigned)e >> 30);
+      const double dx = min_img(xi - x[3 * j], L), dy = min_img(yi - x[3 * j + 1], L),
+                   dz = min_img(zi - x[3 * j + 2], L);
+      const double rsq = dx * dx + dy * dy + dz * dz;
+      const double* pc = t.pair_coeff + 3 * (ti * nt1 + t.type[j]);
+      if (rsq >= pc[2] * pc[2] || rsq <= 0.0) continue;
+      const double r2i = 1.0 / rsq, s2 = pc[1] * pc[1] * r2i, s6 = s2 * s2 * s2;
+      const double fp = nl.wtab[cls] * 24.0 * pc[0] * s6 * (2.0 * s6 - 1.0) * r2i;
+      px += dx * fp;
+      py += dy * fp;
+      pz += dz * fp;
+    }
     fx += px;
     fy += py;
     fz += pz;
@@ -144,14 +259,11 @@ __global__ void k_forces(const double* __restrict__ x, double* __restrict__ f, F
   if (warn) atomicOr(err, warn);
 }
 
-cudaError_t compute_forces(const double* x, double* f, const ForceTopo& t, const BinSpec& cells, const int* offsets,
-                           const int* sorted, double4* xs, uint32_t* err, cudaStream_t st) {
+cudaError_t compute_forces(const double* x, double* f, const ForceTopo& t, const NeighborList* nl, uint32_t* err,
+                           cudaStream_t st) {
   if (t.M <= 0) return cudaSuccess;
-  if (t.pair_style && t.M > 1) {
-    k_gather_cells<<<(t.M + 255) / 256, 256, 0, st>>>(x, t.type, sorted, t.M, xs);
-    count_launches(1);
-  }
-  k_forces<<<(t.M + 127) / 128, 128, 0, st>>>(x, f, t, cells, offsets, sorted, xs, err);
+  const int use_nl = (t.pair_style && t.M > 1 && nl) ? 1 : 0;
+  k_forces<<<(t.M + 127) / 128, 128, 0, st>>>(x, f, t, use_nl ? *nl : NeighborList{}, use_nl, err);
   count_launches(1);
   return cudaGetLastError();
 }

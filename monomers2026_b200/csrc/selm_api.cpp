@@ -424,31 +424,58 @@ extern "C" int selm_set_topology(selm_sim* s, const selm_topology* tp) {
   for (int a = 0; a < 3; a++) T.body[a] = tp->body_force[a];
   T.lo = s->lo;
   T.hi = s->hi;
-  // force cells: as many cells of size >= the largest cutoff as fit (1 if < 3)
-  double rcmax = 0.0;
+  // neighbour list of the pair style: skin 0.3 sigma (LAMMPS' default for lj
+  // units), force cells of edge >= cutoff + skin
+  double rcmax = 0.0, sigmin = 0.0;
   if (tp->pair_style && tp->pair_coeff)
-    for (size_t q = 0; q < (size_t)(nt + 1) * (nt + 1); q++) rcmax = std::max(rcmax, tp->pair_coeff[3 * q + 2]);
+    for (int a = 1; a <= nt; a++)
+      for (int b = 1; b <= nt; b++) {
+        const double* c = tp->pair_coeff + 3 * ((size_t)a * (nt + 1) + b);
+        rcmax = std::max(rcmax, c[2]);
+        if (c[2] > 0 && c[1] > 0) sigmin = (sigmin > 0) ? std::min(sigmin, c[1]) : c[1];
+      }
   const double L = s->hi - s->lo;
-  int nc = rcmax > 0 ? (int)std::floor(L / rcmax) : 1;
-  // no more cells than about two per monomer: cells stay >= the cutoff, the
-  // bucket arrays stay proportional to the monomers
-  nc = std::min(nc, std::max(3, (int)std::cbrt(2.0 * M)));
-  if (nc < 3) nc = 1;
-  if (nc > 1024) nc = 1024;
-  BinSpec& fc = s->fcells;
-  fc.mode = 1;
-  fc.lo = s->lo;
-  fc.dx = s->dx;
-  fc.L = L;
-  for (int a = 0; a < 3; a++) {
-    fc.n[a] = nc;
-    fc.tile[a] = 1;
-    fc.nb[a] = nc;
-  }
   T.rc2max = rcmax * rcmax;
-  if (tp->pair_style && M > 1) {
+  s->nlist = NeighborList{};
+  if (tp->pair_style && M > 1 && rcmax > 0) {
+    NeighborList& NL = s->nlist;
+    const double sig = (sigmin > 0) ? sigmin : rcmax;
+    const double skin = 0.3 * sig;
+    const double rl = rcmax + skin;
+    int nc = (int)std::floor(L / rl);
+    // no more cells than about two per monomer: cells stay >= rl, the bucket
+    // arrays stay proportional to the monomers
+    nc = std::min(nc, std::max(3, (int)std::cbrt(2.0 * M)));
+    if (nc < 3) nc = 1;
+    if (nc > 1024) nc = 1024;
+    BinSpec& fc = s->fcells;
+    fc.mode = 1;
+    fc.lo = s->lo;
+    fc.dx = s->dx;
+    fc.L = L;
+    for (int a = 0; a < 3; a++) {
+      fc.n[a] = nc;
+      fc.tile[a] = 1;
+      fc.nb[a] = nc;
+    }
+    // partners within rl at close packing (sqrt(2) per sigma^3) with a 25% margin
+    const double r = rl / sig;
+    int cap = (int)std::ceil(4.0 / 3.0 * kPi * r * r * r * std::sqrt(2.0) * 1.25) + 8;
+    cap = std::max(32, std::min(1024, (cap + 7) / 8 * 8));
+    NL.cap = cap;
+    NL.rl2 = rl * rl;
+    NL.half_skin2 = 0.25 * skin * skin;
+    NL.wtab[0] = 1.0;
+    for (int k = 0; k < 3; k++) NL.wtab[k + 1] = tp->special_lj[k];
     if ((rc = alloc_bins(s, s->fcells, s->fbb, M))) return rc;
-    if ((rc = dalloc(s, &s->fxs, M))) return rc;
+    const long nbk = (long)nc * nc * nc;
+    CU(cudaMemset(s->fbb.counts, 0, sizeof(int) * (nbk + 1)));
+    if ((rc = dalloc(s, &NL.idx, (size_t)cap * M))) return rc;
+    if ((rc = dalloc(s, &NL.cnt, M))) return rc;
+    if ((rc = dalloc(s, &NL.xb, 3L * M))) return rc;
+    if ((rc = dalloc(s, &NL.flag, 1))) return rc;
+    const int one = 1;  // first build at the next force evaluation
+    CU(cudaMemcpy(NL.flag, &one, sizeof(int), cudaMemcpyHostToDevice));
   }
   s->have_topo = true;
   s->cb = nullptr;
@@ -471,12 +498,9 @@ int engine_forces(selm_sim* s) {
   double* x = s->x[s->cx];
   if (s->have_topo) {
     prof_mark(s, "forces", true);
-    if (s->topo.pair_style && s->M > 1) {
-      CU(bin_particles(x, s->M, s->fcells, s->fbb, s->st));
-      CU(compute_forces(x, s->f, s->topo, s->fcells, s->fbb.offsets, s->fbb.sorted, s->fxs, s->err, s->st));
-    } else {
-      CU(compute_forces(x, s->f, s->topo, s->fcells, nullptr, nullptr, nullptr, s->err, s->st));
-    }
+    const bool pairs = s->nlist.cap > 0;
+    if (pairs) CU(neighbor_update(x, s->topo, s->fcells, s->fbb, s->nlist, s->err, s->st));
+    CU(compute_forces(x, s->f, s->topo, pairs ? &s->nlist : nullptr, s->err, s->st));
     prof_mark(s, "forces", false);
     return SELM_OK;
   }
@@ -537,8 +561,7 @@ static int plain_step(selm_sim* s) {
     CU(interp_update<double>(s->u64[s->cu], xo, xn, s->v, s->f, s->m, s->tf, nullptr, rec, a, s->err, s->st));
     prof_mark(s, "interp_update", false);
     prof_mark(s, "bin", true);
-    CU(bin_particles(xo, s->M, s->tiles, s->tbb, s->st, reinterpret_cast<const int*>(rec),
-                     (int)(sizeof(WRec<double>) / sizeof(int))));
+    CU(bin_particles(xo, s->M, s->tiles, s->tbb, s->st, wrec_bases(rec), wrec_stride<double>()));
     prof_mark(s, "bin", false);
     prof_mark(s, "spread", true);
     CU(spread_gather<double>(s->fg64, true, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st, rec));

@@ -41,7 +41,7 @@ struct selm_sim {
   selm::FftTables<float> tb32{};
   selm::BinSpec tiles{}, fcells{};
   selm::BinBuffers tbb{}, fbb{};
-  double4* fxs = nullptr;  // monomers in force-cell order
+  selm::NeighborList nlist{};  // Verlet list of the pair style
   bool have_topo = false;
   selm::ForceTopo topo{};
   selm_force_fn cb = nullptr;

@@ -1,5 +1,6 @@
 // selm_kernels.h - host-side launchers of the SELM device kernels (internal).
 #pragma once
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -65,10 +66,18 @@ cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBu
 // ---- coupling and monomer update
 // Per-monomer stencil of one step: wrapped base cell of the 4-point stencil and
 // its weight factors, per axis, unshifted and shifted by half a cell.
-template <typename T> struct WRec {
-  int b[3][2];
-  T w[3][2][4];
+template <typename T> struct alignas(16) WRec {
+  T w[3][2][4];  // weight factors [axis][unshifted, shifted][point] (16-byte aligned rows)
+  int b[3][2];   // stencil bases wrapped into [0, n): [axis][unshifted, shifted]
 };
+// the bases of record 0 and the record stride in ints, for the binning kernels
+template <typename T> inline const int* wrec_bases(const WRec<T>* rec) {
+  return reinterpret_cast<const int*>(reinterpret_cast<const char*>(rec) + offsetof(WRec<T>, b));
+}
+template <typename T> constexpr int wrec_stride() {
+  static_assert(sizeof(WRec<T>) % sizeof(int) == 0, "record size");
+  return (int)(sizeof(WRec<T>) / sizeof(int));
+}
 struct CouplingArgs {
   int nx, ny, nz;
   double lo, hi, dx, dt, upsilon, coef;
@@ -112,7 +121,29 @@ struct ForceTopo {
   double lo, hi;
   double rc2max;          // largest pair cutoff squared (quick reject)
 };
-cudaError_t compute_forces(const double* x, double* f, const ForceTopo& t, const BinSpec& cells, const int* offsets,
-                           const int* sorted, double4* xs, uint32_t* err, cudaStream_t st);
+// Verlet neighbour list of the pair style: every partner j within
+// rl = (largest cutoff + skin) of i, pairs of special weight 0 left out,
+// sorted by j.  Rebuilt from the force cells when some monomer has moved more
+// than skin/2 since the last build (minimum image), which keeps every pair
+// within the cutoff on the list.
+struct NeighborList {
+  int cap = 0;             // entries per monomer
+  int* idx = nullptr;      // [cap][M]: partner j | weight class << 30
+  int* cnt = nullptr;      // [M]
+  double* xb = nullptr;    // [3M] positions at the last build
+  int* flag = nullptr;     // rebuild requested: set by the check, cleared by the forces kernel
+  double rl2 = 0.0;        // list radius squared
+  double half_skin2 = 0.0; // (skin / 2)^2
+  double wtab[4] = {1.0, 1.0, 1.0, 1.0};  // pair weight by class: 1, special_lj[0..2]
+};
+// check displacements and, where needed, rebuild (every kernel returns at
+// once when no rebuild is due, so the launch sequence is the same every step)
+cudaError_t neighbor_update(const double* x, const ForceTopo& t, const BinSpec& cells, const BinBuffers& bb,
+                            const NeighborList& nl, uint32_t* err, cudaStream_t st);
+// bonds, angles, pairs from the list (nl may be null without a pair style), body force
+cudaError_t compute_forces(const double* x, double* f, const ForceTopo& t, const NeighborList* nl, uint32_t* err,
+                           cudaStream_t st);
+// exclusive scan over n ints; when flag is non-null the kernels return at once while *flag == 0
+cudaError_t exclusive_scan(const int* in, int* out, long n, int* tmp, cudaStream_t st, const int* flag = nullptr);
 
 }  // namespace selm
