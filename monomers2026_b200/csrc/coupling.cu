@@ -16,6 +16,7 @@
 //                     floating-point atomics; results do not depend on
 //                     scheduling.
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "selm_kernels.h"
@@ -366,31 +367,74 @@ __global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, 
     for (int i = 0; i < 4; i++) w[ax][i] = ref_weight<T>(fabs(r[ax] - (double)(base[ax] + i)));
   }
   const T* ud = u + d * N;
-  int ix[4];
-#pragma unroll
-  for (int i = 0; i < 4; i++) ix[i] = wrapi(base[0] + i, a.nx);
   T val = T(0);
+  // rows of 4 consecutive x-points: 16-byte vector loads over an aligned
+  // window when the rows are 16-byte aligned (nx a multiple of the vector
+  // width), with zero weights outside the stencil (the non-zero terms are
+  // added in the same order as point by point); scalar loads otherwise
+  constexpr int V = 16 / sizeof(T), NV = (4 + V - 1) / V + 1, W = NV * V;
+  using Vec = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  if (a.nx % V == 0) {
+    const int x0 = wrapi(base[0], a.nx);
+    const int a0 = x0 & ~(V - 1), off = x0 - a0;
+    int vs[NV];
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const T dk = T(1) * w[2][k];
-    const long zoff = (long)wrapi(base[2] + k, a.nz) * a.ny;
+    for (int m = 0; m < NV; m++) {
+      const int q = a0 + m * V;
+      vs[m] = (q >= a.nx) ? q - a.nx : q;
+    }
+    T wsel[W];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const T dj = dk * w[1][j];
-      const T* row = ud + (zoff + wrapi(base[1] + j, a.ny)) * a.nx;
+    for (int t = 0; t < W; t++) {
+      const int i = t - off;
+      wsel[t] = (i == 0) ? w[0][0] : (i == 1) ? w[0][1] : (i == 2) ? w[0][2] : (i == 3) ? w[0][3] : T(0);
+    }
 #pragma unroll
-      for (int i = 0; i < 4; i++) val += __ldg(row + ix[i]) * (dj * w[0][i]);
+    for (int k = 0; k < 4; k++) {
+      const T dk = T(1) * w[2][k];
+      const long zoff = (long)wrapi(base[2] + k, a.nz) * a.ny;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const T dj = dk * w[1][j];
+        const T* row = ud + (zoff + wrapi(base[1] + j, a.ny)) * a.nx;
+#pragma unroll
+        for (int m = 0; m < NV; m++) {
+          const Vec q = __ldg(reinterpret_cast<const Vec*>(row + vs[m]));
+          const T* e = reinterpret_cast<const T*>(&q);
+#pragma unroll
+          for (int t = 0; t < V; t++) val += e[t] * (dj * wsel[m * V + t]);
+        }
+      }
+    }
+  } else {
+    int ix[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) ix[i] = wrapi(base[0] + i, a.nx);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const T dk = T(1) * w[2][k];
+      const long zoff = (long)wrapi(base[2] + k, a.nz) * a.ny;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const T dj = dk * w[1][j];
+        const T* row = ud + (zoff + wrapi(base[1] + j, a.ny)) * a.nx;
+#pragma unroll
+        for (int i = 0; i < 4; i++) val += __ldg(row + ix[i]) * (dj * w[0][i]);
+      }
     }
   }
   if (rec) {
+    // axis d unshifted and axis d+1 shifted (static indices keep w in registers)
     const int a1 = (d + 1) % 3;
     WRec<T>& R = rec[p];
-    R.b[d][0] = wrapi(base[d], nn[d]);
-    R.b[a1][1] = wrapi(base[a1], nn[a1]);
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      R.w[d][0][i] = w[d][i];
-      R.w[a1][1][i] = w[a1][i];
+    for (int ax = 0; ax < 3; ax++) {
+      if (ax == d || ax == a1) {
+        const int sh = (ax == d) ? 0 : 1;
+        R.b[ax][sh] = wrapi(base[ax], nn[ax]);
+#pragma unroll
+        for (int i = 0; i < 4; i++) R.w[ax][sh][i] = w[ax][i];
+      }
     }
   }
   const double vg = v[g];
@@ -486,11 +530,11 @@ constexpr int kSpreadCells = 3 * kTZ * kTY * kTX;
 static_assert(kTX == 16, "spread_rot assumes 16-cell rows");
 
 // Accumulator slot of cell (cx, cy, cz) of component d.  The x position is
-// rotated by cy + 4 cz within its 16-cell row, so that the four z-planes of
-// one candidate's component (consecutive cz, same cx and cy) fall on distinct
-// banks.
+// rotated by 4 cz within its 16-cell row, so that the four z-planes of one
+// candidate's component (consecutive cz, same cx and cy), which neighbouring
+// lanes add at the same time, fall on distinct banks.
 __device__ __forceinline__ int spread_row(int d, int cy, int cz) { return ((d * kTZ + cz) * kTY + cy) * kTX; }
-__device__ __forceinline__ int spread_rot(int cx, int cy, int cz) { return (cx + cy + 4 * cz) & (kTX - 1); }
+__device__ __forceinline__ int spread_rot(int cx, int cz) { return (cx + 4 * cz) & (kTX - 1); }
 
 __device__ __forceinline__ long long to_fixed(float v) { return __float2ll_rn(v); }
 __device__ __forceinline__ long long to_fixed(double v) { return __double2ll_rn(v); }
@@ -593,20 +637,29 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
       int cy0 = by - t0y;
       if (cy0 < 0) cy0 += ny;
       const T fz = (T)(-tf[3L * p + d] * scale) * wzk;
+      // x-points of the plane: slot within a row and whether inside the tile
+      int xo[4];
+      bool xin[4];
+#pragma unroll
+      for (int ix = 0; ix < 4; ix++) {
+        int cx = cx0 + ix;
+        if (cx >= nx) cx -= nx;
+        xin[ix] = cx < ex;
+        xo[ix] = spread_rot(cx, cz);
+      }
+      const int plane = spread_row(d, 0, cz);
 #pragma unroll
       for (int jy = 0; jy < 4; jy++) {
         int cy = cy0 + jy;
         if (cy >= ny) cy -= ny;
         if (cy < ey) {
           const T rowf = fz * wy.v[jy];
-          const int row = spread_row(d, cy, cz);
+          const int row = plane + cy * kTX;
 #pragma unroll
           for (int ix = 0; ix < 4; ix++) {
-            int cx = cx0 + ix;
-            if (cx >= nx) cx -= nx;
-            if (cx < ex) {
+            if (xin[ix]) {
               const long long v = to_fixed(rowf * wx.v[ix]);
-              const int slot = row + spread_rot(cx, cy, cz);
+              const int slot = row + xo[ix];
               if (split) {
                 atomicAdd(acc_lo + slot, (unsigned)v & (0xffffffffu >> k));
                 atomicAdd(acc_hi + slot, (unsigned)(v >> L));
@@ -628,7 +681,7 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
     const int cy = row % kTY, cz = (row / kTY) % kTZ, d = row / (kTY * kTZ);
     if (cx < ex && cy < ey && cz < ez) {
       T* dst = fgrid + d * N + ((long)(t0z + cz) * ny + (t0y + cy)) * nx + t0x + cx;
-      const int slot = row * kTX + spread_rot(cx, cy, cz);
+      const int slot = row * kTX + spread_rot(cx, cz);
       const long long sum = split ? (long long)(int)acc_hi[slot] * (1ll << L) + (long long)acc_lo[slot]
                                   : (long long)acc[slot];
       const double add = (double)sum * inv_scale + nan_or_zero;

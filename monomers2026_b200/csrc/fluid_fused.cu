@@ -348,18 +348,29 @@ template <typename T> static FusedPlan plan_for(int nx, int ny, int nz) {
 }
 
 // ---------------------------------------------------------------- fast-path dispatch
+// Row pairs per x-pass chunk of the plane kernels: the largest divisor RP of
+// N/2 (halving from N/2) at which two blocks share an SM, else the largest
+// at which one block fits.
+template <typename T, int N> constexpr size_t smem_xy_for(int rp) {
+  return sizeof(cpx<T>) * ((size_t)N * (N / 2 + 2) + (size_t)N * (rp + 1) + N);
+}
 template <typename T, int N> constexpr int rows_per_chunk_fast() {
-  constexpr size_t c = sizeof(cpx<T>);
-  constexpr size_t full = c * ((size_t)N * (N / 2 + 2) + (size_t)N * (N / 2 + 1) + N);
-  return (full <= 200 * 1024 || (N % 4) != 0) ? N / 2 : N / 4;
+  constexpr size_t kSm = 227 * 1024;
+  int rp = N / 2;
+  while (2 * smem_xy_for<T, N>(rp) > kSm && rp % 2 == 0 && rp > 8) rp /= 2;
+  if (2 * smem_xy_for<T, N>(rp) <= kSm) return rp;
+  rp = N / 2;
+  while (smem_xy_for<T, N>(rp) > kSm && rp % 2 == 0) rp /= 2;
+  return rp;
 }
-template <typename T, int N> constexpr size_t smem_xy_fast() {
-  constexpr int RP = rows_per_chunk_fast<T, N>();
-  return sizeof(cpx<T>) * ((size_t)N * (N / 2 + 2) + (size_t)N * (RP + 1) + N);
-}
+template <typename T, int N> constexpr size_t smem_xy_fast() { return smem_xy_for<T, N>(rows_per_chunk_fast<T, N>()); }
 template <typename T> constexpr int wb_fast() { return sizeof(T) == 8 ? 8 : 16; }
+// The request is raised to 60 KB so that at most three blocks share an SM:
+// with the 128^3 FP32 kernel, four resident blocks per SM measured slower
+// than three (the same kernel at 64 registers and 50 KB).
 template <typename T, int N> constexpr size_t smem_z_fast() {
-  return sizeof(cpx<T>) * ((size_t)N * 3 * wb_fast<T>() + N);
+  constexpr size_t need = sizeof(cpx<T>) * ((size_t)N * 3 * wb_fast<T>() + N);
+  return need < 60 * 1024 ? 60 * 1024 : need;
 }
 
 template <typename T, int N> static cudaError_t fast_attrs() {
@@ -566,6 +577,7 @@ template <typename T> static int fused_fluid_t(selm_sim* s) {
     zg.rho = g.rho;
     zg.dt = g.dt;
     zg.noise_amp = g.noise_amp;
+    zg.idx2 = 1.0 / (g.dx * g.dx);
     zg.stochastic = g.stochastic;
     zg.noise_mode = g.noise_mode;
     zg.seed = g.seed;

@@ -175,6 +175,7 @@ __global__ void __launch_bounds__(512) k_xy_inverse_fast(const cpx<T>* __restric
 struct ZGeom {
   int ny, nxh, nx;
   double dx, mu, rho, dt, noise_amp;
+  double idx2;  // 1/dx^2
   int stochastic, noise_mode;
   uint64_t seed;
   const uint64_t* step;
@@ -182,28 +183,36 @@ struct ZGeom {
 
 // reference noise draw of a half-spectrum mode (cuda/SELM_Kernel.cu:56-79); the
 // amplitude sqrt(lambda_h) comes from the symbol tables (cm = cos - 1).  The
-// FP64 forms draw FP64 normals (same stream as the plain form); the FP32 form
-// draws FP32 normals from the same Philox counters.
+// FP64 forms draw FP64 normals (same stream as the plain form) and scale them
+// in FP64; the FP32 form draws FP32 normals from the same Philox counters and
+// scales them in FP32.
 template <typename T, int N>
 __device__ __forceinline__ void noise_draw_fast(const ZGeom& g, uint64_t step, int i, int j, int k, double cmx,
-                                                double cmy, double cmz, double2 out[3]) {
-  const double lam = -2.0 * (cmx + cmy + cmz) / (g.dx * g.dx);
-  const double coef = sqrt(fmax(lam, 0.0));
-  const int k1 = (N - k) % N, j1 = (g.ny - j) % g.ny, i1 = (g.nx - i) % g.nx;
+                                                double cmy, double cmz, cpx<T> out[3]) {
+  const int k1 = (k == 0) ? 0 : N - k, j1 = (j == 0) ? 0 : g.ny - j, i1 = (i == 0) ? 0 : g.nx - i;
   const bool selfc = (k1 == k && j1 == j && i1 == i);
-  const double re = selfc ? coef : coef * 0.7071067811865476;
-  const double im = selfc ? 0.0 : re;
   const uint32_t q = (uint32_t)(((long)k * g.ny + j) * g.nxh + i);
+  if constexpr (sizeof(T) == 8) {
+    const double lam = -2.0 * (cmx + cmy + cmz) / (g.dx * g.dx);
+    const double coef = sqrt(fmax(lam, 0.0));
+    const double re = selfc ? coef : coef * 0.7071067811865476;
+    const double im = selfc ? 0.0 : re;
 #pragma unroll
-  for (int d = 0; d < 3; d++) {
-    if constexpr (sizeof(T) == 8) {
+    for (int d = 0; d < 3; d++) {
       double z0, z1;
       philox_normal2(g.seed, q, (uint32_t)d, step, z0, z1);
       out[d] = make_double2(z0 * re, z1 * im);
-    } else {
+    }
+  } else {
+    const float lam = (float)(-2.0 * (cmx + cmy + cmz) * g.idx2);
+    const float coef = sqrtf(fmaxf(lam, 0.0f));
+    const float re = selfc ? coef : coef * 0.70710678f;
+    const float im = selfc ? 0.0f : re;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
       float z0, z1;
       philox_normal2_f32(g.seed, q, (uint32_t)d, step, z0, z1);
-      out[d] = make_double2((double)z0 * re, (double)z1 * im);
+      out[d] = make_float2(z0 * re, z1 * im);
     }
   }
 }
@@ -294,25 +303,26 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
     const double cy = symy[2 * j], sy = symy[2 * j + 1];
     const double cz = symz[2 * k], sz = symz[2 * k + 1];
     if (g.stochastic) {
-      double2 Xn[3];
+      C Xn[3];
       noise_draw_fast<T, N>(g, step, i, j, k, cx, cy, cz, Xn);
       if (i == 0 || ((g.nx & 1) == 0 && i == g.nx / 2)) {
-        const int jc = (ny - j) % ny, kc = (N - k) % N;
+        const int jc = (j == 0) ? 0 : ny - j, kc = (k == 0) ? 0 : N - k;
         if (jc != j || kc != k) {
-          double2 Xc[3];
+          C Xc[3];
           noise_draw_fast<T, N>(g, step, i, jc, kc, cx, symy[2 * jc], symz[2 * kc], Xc);
-          const double s = (g.noise_mode == 1) ? 0.7071067811865476 : 0.5;
+          const T s = (g.noise_mode == 1) ? T(0.7071067811865476) : T(0.5);
 #pragma unroll
-          for (int c = 0; c < 3; c++) Xn[c] = make_double2((Xn[c].x + Xc[c].x) * s, (Xn[c].y - Xc[c].y) * s);
+          for (int c = 0; c < 3; c++) Xn[c] = fftk::mk<C>((Xn[c].x + Xc[c].x) * s, (Xn[c].y - Xc[c].y) * s);
         } else {
 #pragma unroll
-          for (int c = 0; c < 3; c++) Xn[c].y = 0.0;
+          for (int c = 0; c < 3; c++) Xn[c].y = T(0);
         }
       }
+      const T amp = (T)g.noise_amp;
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        X[c].x += (T)(g.noise_amp * Xn[c].x);
-        X[c].y += (T)(g.noise_amp * Xn[c].y);
+        X[c].x += amp * Xn[c].x;
+        X[c].y += amp * Xn[c].y;
       }
     }
     C un[3];
