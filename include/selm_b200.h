@@ -41,7 +41,12 @@ extern "C" {
 #define SELM_FORM_FUSED32 2  /* same in FP32 with FP64 positions, zero mode and noise prefactor */
 
 #define SELM_INTEGRATOR_INERTIAL 0     /* reference scheme (cuda/SELM_Kernel.cu:155-195,302-373) */
-#define SELM_INTEGRATOR_QUASI_STEADY 1 /* overdamped: u = P f / (mu |k_h|^2), x += Gamma u dt */
+/* Overdamped form, no counterpart in the reference (fused forms only):
+ * u = P (F_hat / dV + g_hat) / (mu lambda_h) with the conservative forces F
+ * spread at x^n and thermal forcing of variance 2 kB T mu lambda_h / (dt dV)
+ * per mode; v = Gamma u (x^n), x^{n+1} = x^n + dt v; f keeps the
+ * conservative force. */
+#define SELM_INTEGRATOR_QUASI_STEADY 1
 
 #define SELM_NOISE_REF_COMPAT 0 /* reference draw: x=0 and x=Nx/2 planes Hermitian-averaged by the c2r */
 #define SELM_NOISE_EXACT 1      /* Hermitian-correct draw: full variance on those planes */

@@ -336,37 +336,25 @@ __device__ __forceinline__ T interp_one(double rx, double ry, double rz, int Nx,
   return rv;
 }
 
-// lagrangian_update() of cuda/SELM_Kernel.cu:302-373, one thread per
-// (monomer, component); the spread part lives in k_spread_tiles.  The thread
-// of component d also stores, for the spread of the same step, the stencil
-// bases and weights of axis d (unshifted) and axis d+1 (shifted) in the
-// monomer's record, so the three threads together fill it.
+// Staggered stencil of component d at grid coordinates (gx, gy, gz): bases
+// floor(r) - 1 and the weight factors of each axis (axis d unshifted, the
+// others shifted by -1/2, the MAC face positions).
 template <typename T>
-__global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, const double* __restrict__ x_old,
-                                                       double* __restrict__ x_new, double* __restrict__ v,
-                                                       double* __restrict__ f, const double* __restrict__ m,
-                                                       double* __restrict__ tf_out, const int* __restrict__ order,
-                                                       WRec<T>* __restrict__ rec, CouplingArgs a,
-                                                       uint32_t* __restrict__ err) {
-  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= 3L * a.M) return;
-  const int s = (int)(gid / 3), d = (int)(gid % 3);
-  const int p = order ? order[s] : s;
-  const long g = 3L * p + d;
-  const long N = (long)a.nx * a.ny * a.nz;
-  const double gx = (x_old[3L * p] - a.lo) / a.dx, gy = (x_old[3L * p + 1] - a.lo) / a.dx,
-               gz = (x_old[3L * p + 2] - a.lo) / a.dx;
+__device__ __forceinline__ void stencil_of(double gx, double gy, double gz, int d, int base[3], T w[3][4]) {
   const double r[3] = {d == 0 ? gx : gx - 0.5, d == 1 ? gy : gy - 0.5, d == 2 ? gz : gz - 0.5};
-  const int nn[3] = {a.nx, a.ny, a.nz};
-  int base[3];
-  T w[3][4];
 #pragma unroll
   for (int ax = 0; ax < 3; ax++) {
     base[ax] = (int)floor(r[ax]) - 1;
 #pragma unroll
     for (int i = 0; i < 4; i++) w[ax][i] = ref_weight<T>(fabs(r[ax] - (double)(base[ax] + i)));
   }
-  const T* ud = u + d * N;
+}
+
+// Gamma_d u: the weighted sum over the 4^3 stencil of component d, in the
+// reference's loop and product order (cuda/SELM_Kernel.cu:375-422).
+template <typename T>
+__device__ __forceinline__ T stencil_gather(const T* __restrict__ ud, const int base[3], const T w[3][4],
+                                            const CouplingArgs& a) {
   T val = T(0);
   // rows of 4 consecutive x-points: 16-byte vector loads over an aligned
   // window when the rows are 16-byte aligned (nx a multiple of the vector
@@ -423,20 +411,52 @@ __global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, 
       }
     }
   }
-  if (rec) {
-    // axis d unshifted and axis d+1 shifted (static indices keep w in registers)
-    const int a1 = (d + 1) % 3;
-    WRec<T>& R = rec[p];
+  return val;
+}
+
+// The stencil parts a thread of component d stores in the monomer's record:
+// axis d unshifted and axis d+1 shifted (static indices keep w in registers).
+template <typename T>
+__device__ __forceinline__ void record_store(WRec<T>& R, int d, const int base[3], const T w[3][4],
+                                             const CouplingArgs& a) {
+  const int nn[3] = {a.nx, a.ny, a.nz};
+  const int a1 = (d + 1) % 3;
 #pragma unroll
-    for (int ax = 0; ax < 3; ax++) {
-      if (ax == d || ax == a1) {
-        const int sh = (ax == d) ? 0 : 1;
-        R.b[ax][sh] = wrapi(base[ax], nn[ax]);
+  for (int ax = 0; ax < 3; ax++) {
+    if (ax == d || ax == a1) {
+      const int sh = (ax == d) ? 0 : 1;
+      R.b[ax][sh] = wrapi(base[ax], nn[ax]);
 #pragma unroll
-        for (int i = 0; i < 4; i++) R.w[ax][sh][i] = w[ax][i];
-      }
+      for (int i = 0; i < 4; i++) R.w[ax][sh][i] = w[ax][i];
     }
   }
+}
+
+// lagrangian_update() of cuda/SELM_Kernel.cu:302-373, one thread per
+// (monomer, component); the spread part lives in k_spread_tiles.  The thread
+// of component d also stores, for the spread of the same step, the stencil
+// bases and weights of axis d (unshifted) and axis d+1 (shifted) in the
+// monomer's record, so the three threads together fill it.
+template <typename T>
+__global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, const double* __restrict__ x_old,
+                                                       double* __restrict__ x_new, double* __restrict__ v,
+                                                       double* __restrict__ f, const double* __restrict__ m,
+                                                       double* __restrict__ tf_out, const int* __restrict__ order,
+                                                       WRec<T>* __restrict__ rec, CouplingArgs a,
+                                                       uint32_t* __restrict__ err) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 3L * a.M) return;
+  const int s = (int)(gid / 3), d = (int)(gid % 3);
+  const int p = order ? order[s] : s;
+  const long g = 3L * p + d;
+  const long N = (long)a.nx * a.ny * a.nz;
+  const double gx = (x_old[3L * p] - a.lo) / a.dx, gy = (x_old[3L * p + 1] - a.lo) / a.dx,
+               gz = (x_old[3L * p + 2] - a.lo) / a.dx;
+  int base[3];
+  T w[3][4];
+  stencil_of<T>(gx, gy, gz, d, base, w);
+  const T val = stencil_gather<T>(u + d * N, base, w, a);
+  if (rec) record_store<T>(rec[p], d, base, w, a);
   const double vg = v[g];
   double t_f = -a.upsilon * (vg - (double)val) * a.dt;
   if (a.stochastic) {
@@ -459,6 +479,78 @@ __global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, 
   v[g] = vn;
   if (!isfinite(vn) || !isfinite(tx)) atomicOr(err, ERR_NONFINITE);
 }
+
+// ---- quasi-steady (overdamped) form, no reference counterpart
+// Before the fluid solve: the stencil records at x^n for binning and spreading,
+// and the impulse array the spread subtracts, tf = -F / dV, so that the grid
+// receives the force density +F / dV of the conservative forces.
+template <typename T>
+__global__ void __launch_bounds__(256) k_qs_prepare(const double* __restrict__ x, const double* __restrict__ f,
+                                                    double* __restrict__ tf_out, WRec<T>* __restrict__ rec,
+                                                    CouplingArgs a, double inv_dv) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 3L * a.M) return;
+  const int p = (int)(gid / 3), d = (int)(gid % 3);
+  const double gx = (x[3L * p] - a.lo) / a.dx, gy = (x[3L * p + 1] - a.lo) / a.dx, gz = (x[3L * p + 2] - a.lo) / a.dx;
+  int base[3];
+  T w[3][4];
+  stencil_of<T>(gx, gy, gz, d, base, w);
+  record_store<T>(rec[p], d, base, w, a);
+  tf_out[gid] = -f[gid] * inv_dv;
+}
+
+// After the fluid solve: v = Gamma u (x^n), x^{n+1} = x^n + dt v with the
+// inertial form's single periodic wrap; f keeps the conservative force.
+template <typename T>
+__global__ void __launch_bounds__(384) k_qs_move(const T* __restrict__ u, const double* __restrict__ x_old,
+                                                 double* __restrict__ x_new, double* __restrict__ v, CouplingArgs a,
+                                                 uint32_t* __restrict__ err) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 3L * a.M) return;
+  const int p = (int)(gid / 3), d = (int)(gid % 3);
+  const long N = (long)a.nx * a.ny * a.nz;
+  const double gx = (x_old[3L * p] - a.lo) / a.dx, gy = (x_old[3L * p + 1] - a.lo) / a.dx,
+               gz = (x_old[3L * p + 2] - a.lo) / a.dx;
+  int base[3];
+  T w[3][4];
+  stencil_of<T>(gx, gy, gz, d, base, w);
+  const double vel = (double)stencil_gather<T>(u + d * N, base, w, a);
+  const double tmp = vel * a.dt;
+  const double L = a.hi - a.lo;
+  if (fabs(tmp) > L / 2) atomicOr(err, ERR_DISPLACEMENT);
+  double tx = x_old[gid] + tmp;
+  if (tx > a.hi) tx -= L;
+  else if (tx < a.lo) tx += L;
+  x_new[gid] = tx;
+  v[gid] = vel;
+  if (!isfinite(vel) || !isfinite(tx)) atomicOr(err, ERR_NONFINITE);
+}
+
+template <typename T>
+cudaError_t qs_prepare(const double* x, const double* f, double* tf, WRec<T>* rec, const CouplingArgs& a,
+                       double inv_dv, cudaStream_t st) {
+  if (a.M <= 0) return cudaSuccess;
+  k_qs_prepare<T><<<(unsigned)((3L * a.M + 255) / 256), 256, 0, st>>>(x, f, tf, rec, a, inv_dv);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t qs_move(const T* u, const double* x_old, double* x_new, double* v, const CouplingArgs& a, uint32_t* err,
+                    cudaStream_t st) {
+  if (a.M <= 0) return cudaSuccess;
+  k_qs_move<T><<<(unsigned)((3L * a.M + 383) / 384), 384, 0, st>>>(u, x_old, x_new, v, a, err);
+  count_launches(1);
+  return cudaGetLastError();
+}
+template cudaError_t qs_prepare<double>(const double*, const double*, double*, WRec<double>*, const CouplingArgs&,
+                                        double, cudaStream_t);
+template cudaError_t qs_prepare<float>(const double*, const double*, double*, WRec<float>*, const CouplingArgs&,
+                                       double, cudaStream_t);
+template cudaError_t qs_move<double>(const double*, const double*, double*, double*, const CouplingArgs&, uint32_t*,
+                                     cudaStream_t);
+template cudaError_t qs_move<float>(const float*, const double*, double*, double*, const CouplingArgs&, uint32_t*,
+                                    cudaStream_t);
 
 // Pure interpolation (operator entry point): out[p][d] = Gamma_d u (x_p)
 template <typename T>

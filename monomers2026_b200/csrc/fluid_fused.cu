@@ -258,7 +258,8 @@ __global__ void __launch_bounds__(256) k_z_update(cpx<T>* __restrict__ work, cpx
         if (jc != j || kc != k) {
           double2 Xc[3];
           noise_draw(g, step, i, jc, kc, Xc);
-          const double s = (g.noise_mode == 1) ? 0.7071067811865476 : 0.5;
+          const double s = (g.noise_mode == 1 || g.integrator == SELM_INTEGRATOR_QUASI_STEADY) ? 0.7071067811865476
+                                                                                               : 0.5;
 #pragma unroll
           for (int c = 0; c < 3; c++) X[c] = make_double2((X[c].x + Xc[c].x) * s, (X[c].y - Xc[c].y) * s);
         } else {
@@ -273,9 +274,25 @@ __global__ void __launch_bounds__(256) k_z_update(cpx<T>* __restrict__ work, cpx
       }
     }
     C un[3];
+    const bool qs = g.integrator == SELM_INTEGRATOR_QUASI_STEADY;
     if (i == 0 && j == 0 && k == 0) {
 #pragma unroll
       for (int c = 0; c < 3; c++) un[c] = cmk<C>(T(0), T(0));
+    } else if (qs) {
+      // steady Stokes: u_hat = P f_hat / (mu lambda_h), lambda_h = -L_h > 0
+      const T idx1 = (T)(1.0 / g.dx);
+      const C D[3] = {cmk<C>((T)cx * idx1, (T)sx * idx1), cmk<C>((T)cy * idx1, (T)sy * idx1),
+                      cmk<C>((T)cz * idx1, (T)sz * idx1)};
+      C s = cmul(D[0], Fk[0]);
+      s = cadd(s, cmul(D[1], Fk[1]));
+      s = cadd(s, cmul(D[2], Fk[2]));
+      const T iL = (T)(1.0 / Lk), imuL = (T)(-1.0 / (g.mu * Lk));
+      s = cmk<C>(s.x * iL, s.y * iL);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const C pf = csub(Fk[c], cmul(cmk<C>(-D[c].x, D[c].y), s));
+        un[c] = cmk<C>(pf.x * imuL, pf.y * imuL);
+      }
     } else {
       const T visc = (T)(1.0 + g.mu * g.dt * Lk / g.rho);
       const T irho = (T)(1.0 / g.rho);
@@ -302,7 +319,7 @@ __global__ void __launch_bounds__(256) k_z_update(cpx<T>* __restrict__ work, cpx
     }
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      uhat[(long)c * nz * plane + gidx] = un[c];
+      if (!qs) uhat[(long)c * nz * plane + gidx] = un[c];
       F[k * nl + c * Wb + w] = cmk<C>(un[c].x * (T)invN, un[c].y * (T)invN);
     }
   }
@@ -555,7 +572,14 @@ static FusedGeom geom_of(selm_sim* s) {
   g.integrator = s->prm.integrator;
   g.seed = s->prm.seed;
   const double N = (double)s->N;
-  g.noise_amp = sqrt(2 * s->prm.KB * s->prm.T * s->prm.dt * s->prm.mu / N) * N;  // cuda/SELM_Eulerian_Period.cu:141
+  if (s->prm.integrator == SELM_INTEGRATOR_QUASI_STEADY) {
+    // thermal force density of variance 2 kB T mu lambda_h / (dt dV) per mode (times N, the
+    // unnormalised DFT), so that u = P g / (mu lambda_h) gives dt Gamma u the covariance 2 kB T dt M
+    const double dv = s->dx * s->dx * s->dx;
+    g.noise_amp = sqrt(2 * s->prm.KB * s->prm.T * s->prm.mu * N / (s->prm.dt * dv));
+  } else {
+    g.noise_amp = sqrt(2 * s->prm.KB * s->prm.T * s->prm.dt * s->prm.mu / N) * N;  // cuda/SELM_Eulerian_Period.cu:141
+  }
   g.step = s->fz->d_step;
   return g;
 }
@@ -578,6 +602,7 @@ template <typename T> static int fused_fluid_t(selm_sim* s) {
     zg.dt = g.dt;
     zg.noise_amp = g.noise_amp;
     zg.idx2 = 1.0 / (g.dx * g.dx);
+    zg.qs = (g.integrator == SELM_INTEGRATOR_QUASI_STEADY);
     zg.stochastic = g.stochastic;
     zg.noise_mode = g.noise_mode;
     zg.seed = g.seed;
@@ -631,6 +656,32 @@ template <typename T> static int fused_step_t(selm_sim* s) {
   count_launches(1);
   double* xo = s->x[s->cx];
   double* xn = s->x[s->cx ^ 1];
+  if (s->prm.integrator == SELM_INTEGRATOR_QUASI_STEADY) {
+    // overdamped: spread the conservative forces at x^n as a force density,
+    // solve steady Stokes with thermal forcing, move with the interpolated velocity
+    if (s->M > 0) {
+      WRec<T>* rec = static_cast<WRec<T>*>(s->wrec);
+      prof_mark(s, "interp_update", true);
+      CUF(qs_prepare<T>(xo, s->f, s->tf, rec, a, 1.0 / (s->dx * s->dx * s->dx), s->st));
+      prof_mark(s, "interp_update", false);
+      prof_mark(s, "bin", true);
+      CUF(bin_particles(xo, s->M, s->tiles, s->tbb, s->st, wrec_bases(rec), wrec_stride<T>()));
+      prof_mark(s, "bin", false);
+      prof_mark(s, "spread", true);
+      CUF(spread_gather<T>((T*)z->fp, false, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st, rec));
+      prof_mark(s, "spread", false);
+    } else {
+      CUF(cudaMemsetAsync(z->fp, 0, sizeof(T) * 3 * s->N, s->st));
+    }
+    int rc = fused_fluid_t<T>(s);
+    if (rc) return rc;
+    if (s->M > 0) {
+      prof_mark(s, "interp_update", true);
+      CUF(qs_move<T>((const T*)z->u, xo, xn, s->v, a, s->err, s->st));
+      prof_mark(s, "interp_update", false);
+    }
+    return SELM_OK;
+  }
   if (s->M > 0) {
     WRec<T>* rec = static_cast<WRec<T>*>(s->wrec);
     prof_mark(s, "interp_update", true);

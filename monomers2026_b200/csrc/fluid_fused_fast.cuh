@@ -176,6 +176,7 @@ struct ZGeom {
   int ny, nxh, nx;
   double dx, mu, rho, dt, noise_amp;
   double idx2;  // 1/dx^2
+  int qs;       // quasi-steady: u_hat = P (F_hat + noise) / (mu lambda_h), no state
   int stochastic, noise_mode;
   uint64_t seed;
   const uint64_t* step;
@@ -310,7 +311,7 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
         if (jc != j || kc != k) {
           C Xc[3];
           noise_draw_fast<T, N>(g, step, i, jc, kc, cx, symy[2 * jc], symz[2 * kc], Xc);
-          const T s = (g.noise_mode == 1) ? T(0.7071067811865476) : T(0.5);
+          const T s = (g.noise_mode == 1 || g.qs) ? T(0.7071067811865476) : T(0.5);
 #pragma unroll
           for (int c = 0; c < 3; c++) Xn[c] = fftk::mk<C>((Xn[c].x + Xc[c].x) * s, (Xn[c].y - Xc[c].y) * s);
         } else {
@@ -329,6 +330,21 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
     if (i == 0 && j == 0 && k == 0) {
 #pragma unroll
       for (int c = 0; c < 3; c++) un[c] = fftk::mk<C>(T(0), T(0));
+    } else if (g.qs) {
+      // steady Stokes: u_hat = P f_hat / (mu lambda_h), lambda_h = -L_h > 0
+      const double Lk = 2.0 * (cx + cy + cz) * idx2;
+      const C D[3] = {fftk::mk<C>((T)cx * idx1, (T)sx * idx1), fftk::mk<C>((T)cy * idx1, (T)sy * idx1),
+                      fftk::mk<C>((T)cz * idx1, (T)sz * idx1)};
+      C s = cmul(D[0], X[0]);
+      s = cadd(s, cmul(D[1], X[1]));
+      s = cadd(s, cmul(D[2], X[2]));
+      const T iL = (T)(1.0 / Lk), imuL = (T)(-1.0 / (g.mu * Lk));
+      s = fftk::mk<C>(s.x * iL, s.y * iL);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const C pf = csub(X[c], cmul(fftk::mk<C>(-D[c].x, D[c].y), s));
+        un[c] = fftk::mk<C>(pf.x * imuL, pf.y * imuL);
+      }
     } else {
       const double Lk = 2.0 * (cx + cy + cz) * idx2;
       const T visc = (T)(1.0 + g.mu * g.dt * Lk / g.rho);
@@ -350,7 +366,7 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
     }
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      uhat[gk + c * cplane] = un[c];
+      if (!g.qs) uhat[gk + c * cplane] = un[c];
       A[pa + c * WB] = fftk::mk<C>(un[c].x * invN, un[c].y * invN);
     }
   }

@@ -100,6 +100,15 @@ cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const 
                           const WRec<T>* rec = nullptr);
 
 // ---- conservative forces (FP64)
+// quasi-steady form: stencil records at x and tf = -F inv_dv before the
+// spread; v = Gamma u (x_old), x_new = x_old + dt v after the fluid solve
+template <typename T>
+cudaError_t qs_prepare(const double* x, const double* f, double* tf, WRec<T>* rec, const CouplingArgs& a,
+                       double inv_dv, cudaStream_t st);
+template <typename T>
+cudaError_t qs_move(const T* u, const double* x_old, double* x_new, double* v, const CouplingArgs& a, uint32_t* err,
+                    cudaStream_t st);
+
 struct ForceTopo {
   int M, ntypes;
   const int* type;        // [M] 1-based

@@ -55,6 +55,9 @@ def lib():
         L.orc_forces.restype = C.c_int
         L.orc_sim_initial.argtypes = [C.c_void_p]
         L.orc_sim_step.argtypes = [C.c_void_p]
+        L.orc_qs_velocity.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                      C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_uint64,
+                                      C.c_uint64, _dp]
         _lib = L
     return _lib
 
@@ -112,6 +115,16 @@ def fluid_run(u: np.ndarray, fgrid: np.ndarray, dx, mu, rho, dt) -> np.ndarray:
     out = np.zeros(u.size)
     lib().orc_fluid_run(_c(u).ravel(), out, _c(fgrid).ravel(), nx, ny, nz, dx, mu, rho, dt)
     return out.reshape(u.shape)
+
+
+def qs_velocity(dims, lo, dx, x, F, mu, kB=0.0, T=0.0, dt=1.0, stochastic=False, seed=0, step=1) -> np.ndarray:
+    """Quasi-steady Stokes velocity [3][Nz][Ny][Nx] of the monomer forces F (orc_qs_velocity)."""
+    nx, ny, nz = dims
+    x = _c(x).reshape(-1, 3)
+    out = np.zeros((3, nz, ny, nx))
+    lib().orc_qs_velocity(x.ravel(), _c(F).ravel(), len(x), nx, ny, nz, lo, dx, mu, kB, T, dt, int(stochastic),
+                          int(seed), int(step), out.ravel())
+    return out
 
 
 def noise_from_normals(dims, dx, scale, xi, noise_mode=0) -> np.ndarray:
@@ -216,14 +229,16 @@ class _Sim(C.Structure):
         ("seed", C.c_uint64), ("step", C.c_uint64),
         ("x", C.c_void_p), ("v", C.c_void_p), ("f", C.c_void_p), ("m", C.c_void_p),
         ("u", C.c_void_p), ("fgrid", C.c_void_p), ("scratch", C.c_void_p), ("ff", C.c_void_p),
+        ("integrator", C.c_int),
     ]
 
 
 class Sim:
-    """FP64 oracle of the whole inertial SELM step (reference driver order)."""
+    """FP64 oracle of the whole SELM step: the inertial scheme in the reference's
+    driver order (integrator 0), or the project's quasi-steady form (integrator 1)."""
 
     def __init__(self, dims, lo, hi, dt, mu, rho, kB, T, x, m, v=None, stochastic=False, seed=0,
-                 noise_mode=0, ff: ForceField | None = None):
+                 noise_mode=0, ff: ForceField | None = None, integrator=0):
         nx, ny, nz = dims
         N = nx * ny * nz
         M = len(m)
@@ -245,6 +260,7 @@ class Sim:
         s.x, s.v, s.f, s.m = (self.x.ctypes.data, self.v.ctypes.data, self.f.ctypes.data, self.m.ctypes.data)
         s.u, s.fgrid, s.scratch = self.u.ctypes.data, self.fgrid.ctypes.data, self.scratch.ctypes.data
         s.ff = C.addressof(ff.struct) if ff is not None else None
+        s.integrator = int(integrator)
         self.s = s
         self.N = N
 

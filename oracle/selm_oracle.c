@@ -744,6 +744,108 @@ static void remap_initial(orc_sim *s) {
   }
 }
 
+/* ====================================================================== */
+/* Quasi-steady (overdamped) form.  Project-defined: the reference has only  */
+/* the inertial scheme, so this restates the project's own definition (same */
+/* discrete MAC operators as the inertial projection) for testing the GPU   */
+/* form; it has no reference parity.                                        */
+/* ====================================================================== */
+static double sin_sq_half(int t, int n) { const double q = sin(M_PI * t / n); return q * q; }
+
+void orc_qs_velocity(const double *x, const double *F, int M, int nx, int ny, int nz, double lo,
+                     double dx, double mu, double kB, double T, double dt, int stochastic,
+                     uint64_t seed, uint64_t step, double *u) {
+  const int nxh = nx / 2 + 1;
+  const size_t N = (size_t)nx * ny * nz, N2 = (size_t)nxh * ny * nz;
+  const double dv = dx * dx * dx, dxsq = dx * dx;
+  double *fg = (double *)calloc(3 * N, sizeof(double));
+  double *tf = (double *)malloc(sizeof(double) * 3 * (size_t)(M > 0 ? M : 1));
+  double *Fh = (double *)malloc(sizeof(double) * 2 * 3 * N2);
+  for (int q = 0; q < 3 * M; q++) tf[q] = -F[q] / dv; /* orc_spread subtracts tf */
+  orc_spread(fg, nx, ny, nz, lo, dx, x, tf, M);
+  for (int d = 0; d < 3; d++) orc_fft3_r2c(nx, ny, nz, fg + (size_t)d * N, Fh + 2 * (size_t)d * N2);
+  if (stochastic) {
+    double *xi = (double *)malloc(sizeof(double) * 2 * 3 * N2);
+    orc_fluid_normals(seed, step, nx, ny, nz, xi);
+    const double amp = sqrt(2.0 * kB * T * mu * (double)N / (dt * dv));
+    for (int d = 0; d < 3; d++) {
+      size_t n = 0;
+      for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++)
+          for (int i = 0; i < nxh; i++, n++) {
+            const double lam = 4.0 * (sin_sq_half(i, nx) + sin_sq_half(j, ny) + sin_sq_half(k, nz)) / dxsq;
+            const double coef = sqrt(lam);
+            const int k1 = (nz - k) % nz, j1 = (ny - j) % ny, i1 = (nx - i) % nx;
+            const int selfc = (k1 == k && j1 == j && i1 == i);
+            double re = selfc ? coef : coef / sqrt(2.0), im = selfc ? 0.0 : re;
+            /* the c2r averages these planes with their conjugate partners:
+             * doubled amplitude gives them the full Hermitian variance */
+            if (!selfc && (i == 0 || (nx % 2 == 0 && i == nx / 2))) { re *= sqrt(2.0); im *= sqrt(2.0); }
+            const double *z = xi + 2 * ((size_t)d * N2 + n);
+            Fh[2 * ((size_t)d * N2 + n)] += amp * z[0] * re;
+            Fh[2 * ((size_t)d * N2 + n) + 1] += amp * z[1] * im;
+          }
+    }
+    free(xi);
+  }
+  size_t n = 0;
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nxh; i++, n++) {
+        double *f0 = Fh + 2 * n, *f1 = Fh + 2 * (N2 + n), *f2 = Fh + 2 * (2 * N2 + n);
+        double *fd[3] = {f0, f1, f2};
+        if (i == 0 && j == 0 && k == 0) {
+          for (int d = 0; d < 3; d++) fd[d][0] = fd[d][1] = 0.0;
+          continue;
+        }
+        const int tt[3] = {i, j, k}, nn[3] = {nx, ny, nz};
+        double cm[3], sn[3];
+        for (int d = 0; d < 3; d++) {
+          cm[d] = -2.0 * sin_sq_half(tt[d], nn[d]);
+          sn[d] = sin(2.0 * M_PI * tt[d] / nn[d]);
+        }
+        const double L = 2.0 * (cm[0] + cm[1] + cm[2]) / dxsq; /* = -lambda_h */
+        /* s = (D . F) / L with D_d = (cm + i sn)/dx */
+        double sr = 0, si = 0;
+        for (int d = 0; d < 3; d++) {
+          const double dr = cm[d] / dx, di = sn[d] / dx;
+          sr += dr * fd[d][0] - di * fd[d][1];
+          si += dr * fd[d][1] + di * fd[d][0];
+        }
+        sr /= L;
+        si /= L;
+        for (int d = 0; d < 3; d++) {
+          const double gr = -cm[d] / dx, gi = sn[d] / dx; /* G_d = (-cm + i sn)/dx */
+          const double pr = fd[d][0] - (gr * sr - gi * si), pi = fd[d][1] - (gr * si + gi * sr);
+          fd[d][0] = pr / (-mu * L);
+          fd[d][1] = pi / (-mu * L);
+        }
+      }
+  for (int d = 0; d < 3; d++) {
+    double *out = u + (size_t)d * N;
+    orc_fft3_c2r(nx, ny, nz, Fh + 2 * (size_t)d * N2, out);
+    for (size_t q = 0; q < N; q++) out[q] /= (double)N;
+  }
+  free(fg);
+  free(tf);
+  free(Fh);
+}
+
+static void sim_step_qs(orc_sim *s) {
+  const uint64_t n = ++s->step;
+  const double L = s->hi - s->lo;
+  orc_qs_velocity(s->x, s->f, s->M, s->nx, s->ny, s->nz, s->lo, s->dx, s->mu, s->kB, s->T, s->dt,
+                  s->stochastic, s->seed, n, s->u);
+  orc_interp(s->u, s->nx, s->ny, s->nz, s->lo, s->dx, s->x, s->M, s->v);
+  for (int q = 0; q < 3 * s->M; q++) {
+    double tx = s->x[q] + s->v[q] * s->dt;
+    if (tx > s->hi) tx -= L;
+    else if (tx < s->lo) tx += L;
+    s->x[q] = tx;
+  }
+  if (s->ff) orc_forces(s->ff, s->x, s->f);
+}
+
 void orc_sim_initial(orc_sim *s) {
   const size_t N = (size_t)s->nx * s->ny * s->nz;
   s->step = 0;
@@ -754,6 +856,10 @@ void orc_sim_initial(orc_sim *s) {
 }
 
 void orc_sim_step(orc_sim *s) {
+  if (s->integrator == 1) {
+    sim_step_qs(s);
+    return;
+  }
   const size_t N = (size_t)s->nx * s->ny * s->nz;
   const uint64_t n = ++s->step;
   const double upsilon = 6.0 * M_PI * 2 * s->dx * s->mu;

@@ -96,7 +96,19 @@ typedef struct {
   double *fgrid;         /* [3][N] forcing for the next fluid update */
   double *scratch;       /* [3][N] */
   const orc_ff *ff;      /* may be NULL: no conservative force update */
+  int integrator;        /* 0 inertial (reference), 1 quasi-steady (project-defined) */
 } orc_sim;
+
+/* ---------------- quasi-steady (overdamped) form ---------------- */
+/* Project-defined, no counterpart in the reference: the steady periodic
+ * Stokes velocity of the force density Lambda F / dV plus thermal forcing,
+ * u = c2r(P (F_hat + g_hat) / (mu lambda_h)) / N, lambda_h = sum_d
+ * 4 sin^2(theta_d / 2) / dx^2, zero mode 0; g_hat = sqrt(2 kB T mu N /
+ * (dt dV)) xi sqrt(lambda_h) from the step's Philox normals, full Hermitian
+ * variance on the x = 0 and x = Nx/2 planes. */
+void orc_qs_velocity(const double *x, const double *F, int M, int nx, int ny, int nz, double lo,
+                     double dx, double mu, double kB, double T, double dt, int stochastic,
+                     uint64_t seed, uint64_t step, double *u /* [3][N] */);
 
 void orc_sim_initial(orc_sim *s);
 void orc_sim_step(orc_sim *s);
