@@ -166,6 +166,29 @@ int selm_op_spread_noalloc(int precision, const int dims[3], double lo, double d
 int selm_op_fft3_r2c(int precision, const int dims[3], const double* in, double* out);
 int selm_op_fft3_c2r(int precision, const int dims[3], const double* in, double* out);
 
+/* ---- batches: many simulations stepped by one graph launch ----
+ * The reference runs one instance per process (cuda/main.cu:5-12, Selm::run
+ * cuda/SELM.cu:70-98); these entry points replace running that executable
+ * once per replica.  A batch steps fused-form simulations of any grid size and
+ * monomer count together: each member's captured step graph becomes a child
+ * of one graph, launched once per step on the batch's stream.  Members run on
+ * the batch's stream while they belong to it (their own stream comes back when
+ * they leave), are stepped only through the batch, and give the same results
+ * bit for bit as when stepped alone.  Joining and leaving take effect at the
+ * next selm_batch_step (the batch graph is rebuilt then). */
+typedef struct selm_batch selm_batch;
+int selm_batch_create(void* stream /* NULL: the batch owns a stream */, selm_batch** out);
+int selm_batch_add(selm_batch* b, selm_sim* s);    /* s initialised, fused form, no host force callback */
+int selm_batch_remove(selm_batch* b, selm_sim* s); /* waits for the batch's work */
+int selm_batch_step(selm_batch* b, int nsteps);    /* asynchronous, like selm_step */
+int selm_batch_size(selm_batch* b);
+void* selm_batch_get_stream(selm_batch* b);
+int selm_batch_synchronize(selm_batch* b);
+int selm_batch_destroy(selm_batch* b); /* members leave (not destroyed) */
+/* device memory this simulation holds (for admission against an HBM budget);
+ * the reference allocates per object in initial() (cuda/SELM_Eulerian_Period.cu:33-60) */
+int selm_device_bytes(selm_sim* s, unsigned long long* bytes);
+
 /* kernels this library has launched since it was loaded (all simulations) */
 unsigned long long selm_kernel_launches(void);
 

@@ -19,6 +19,8 @@ EXPORTED = [
     "selm_get_stream", "selm_synchronize", "selm_profile_enable", "selm_profile_read",
     "selm_op_interp", "selm_op_spread", "selm_op_spread_noalloc", "selm_op_fft3_r2c", "selm_op_fft3_c2r", "selm_kernel_launches",
     "selm_last_error", "selm_version",
+    "selm_batch_create", "selm_batch_add", "selm_batch_remove", "selm_batch_step", "selm_batch_size",
+    "selm_batch_get_stream", "selm_batch_synchronize", "selm_batch_destroy", "selm_device_bytes",
 ]
 
 SELM_OK = 0
@@ -88,6 +90,16 @@ def load():
     L.selm_op_fft3_c2r.argtypes = [C.c_int, ip, dp, dp]
     L.selm_kernel_launches.argtypes = []
     L.selm_kernel_launches.restype = C.c_ulonglong
+    L.selm_batch_create.argtypes = [vp, C.POINTER(vp)]
+    L.selm_batch_add.argtypes = [vp, vp]
+    L.selm_batch_remove.argtypes = [vp, vp]
+    L.selm_batch_step.argtypes = [vp, C.c_int]
+    L.selm_batch_size.argtypes = [vp]
+    L.selm_batch_get_stream.argtypes = [vp]
+    L.selm_batch_get_stream.restype = vp
+    L.selm_batch_synchronize.argtypes = [vp]
+    L.selm_batch_destroy.argtypes = [vp]
+    L.selm_device_bytes.argtypes = [vp, C.POINTER(C.c_ulonglong)]
     L.selm_last_error.restype = C.c_char_p
     L.selm_version.restype = C.c_char_p
     _lib = L

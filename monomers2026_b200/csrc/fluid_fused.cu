@@ -479,7 +479,8 @@ struct FusedState {
   double *symx = nullptr, *symy = nullptr, *symz = nullptr;
   uint64_t* d_step = nullptr;
   FusedPlan plan{};
-  // one captured step per parity of the double-buffered positions
+  // one captured step per parity of the double-buffered positions (graph kept for batches)
+  cudaGraph_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   unsigned long long graph_kernels[2] = {0, 0};
   bool fast = false;  // compile-time four-step kernels for this grid size
@@ -500,6 +501,7 @@ template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
       return selm_fail(SELM_ERR_NOMEM, "cudaMalloc failed (fused form)");
     }
     s->allocs.push_back(*p);
+    s->dev_bytes += bytes;
     return SELM_OK;
   };
   int rc;
@@ -546,8 +548,10 @@ int fused_allocate(selm_sim* s) {
 
 void fused_release(selm_sim* s) {
   if (!s->fz) return;
-  for (int q = 0; q < 2; q++)
+  for (int q = 0; q < 2; q++) {
     if (s->fz->gexec[q]) cudaGraphExecDestroy(s->fz->gexec[q]);
+    if (s->fz->graph[q]) cudaGraphDestroy(s->fz->graph[q]);
+  }
   delete s->fz;
   s->fz = nullptr;
 }
@@ -727,8 +731,61 @@ void fused_invalidate_graphs(selm_sim* s) {
   if (!s->fz) return;
   for (int q = 0; q < 2; q++) {
     if (s->fz->gexec[q]) cudaGraphExecDestroy(s->fz->gexec[q]);
+    if (s->fz->graph[q]) cudaGraphDestroy(s->fz->graph[q]);
     s->fz->gexec[q] = nullptr;
+    s->fz->graph[q] = nullptr;
   }
+  if (s->batch) batch_mark_dirty(s->batch);
+}
+
+// Capture the step of parity par (x[par] -> x[par ^ 1]) once: the graph is
+// kept (a batch adds it as a child graph) and instantiated for single steps.
+static int fused_capture(selm_sim* s, int par) {
+  FusedState* z = s->fz;
+  if (z->gexec[par]) return SELM_OK;
+  const int saved = s->cx;
+  if (s->M > 0) s->cx = par;
+  const unsigned long long l0 = launches_total();
+  cudaError_t eb = cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal);
+  if (eb != cudaSuccess) {
+    s->cx = saved;
+    return selm_fail(SELM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(eb));
+  }
+  const int rc = fused_body(s);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(s->st, &g);
+  s->cx = saved;
+  const unsigned long long k = launches_total() - l0;
+  uncount_launches(k);  // recorded, not run
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (ec != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+  const cudaError_t ei = cudaGraphInstantiate(&z->gexec[par], g, 0);
+  if (ei != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return selm_fail(SELM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+  }
+  z->graph[par] = g;
+  z->graph_kernels[par] = k;
+  return SELM_OK;
+}
+
+void fused_step_taken(selm_sim* s) {
+  s->step += 1;
+  if (s->M > 0) s->cx ^= 1;
+}
+
+int fused_step_graph(selm_sim* s, int par, cudaGraph_t* graph, unsigned long long* kernels) {
+  if (!s->fz) return selm_fail(SELM_ERR_STATE, "only the fused forms step in a batch");
+  if (s->cb || s->prof) return selm_fail(SELM_ERR_STATE, "a host force callback or profiling needs single steps");
+  const int rc = fused_capture(s, (s->M > 0) ? par : 0);
+  if (rc) return rc;
+  const int q = (s->M > 0) ? par : 0;
+  *graph = s->fz->graph[q];
+  *kernels = s->fz->graph_kernels[q];
+  return SELM_OK;
 }
 
 int fused_step(selm_sim* s) {
@@ -737,31 +794,15 @@ int fused_step(selm_sim* s) {
   const bool graph = !s->cb && !s->prof;
   const int par = (s->M > 0) ? s->cx : 0;
   if (graph) {
-    if (!z->gexec[par]) {
-      const unsigned long long l0 = launches_total();
-      CUF(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-      const int rc = fused_body(s);
-      cudaGraph_t g = nullptr;
-      const cudaError_t ec = cudaStreamEndCapture(s->st, &g);
-      if (rc) {
-        if (g) cudaGraphDestroy(g);
-        return rc;
-      }
-      if (ec != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
-      const cudaError_t ei = cudaGraphInstantiate(&z->gexec[par], g, 0);
-      cudaGraphDestroy(g);
-      if (ei != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
-      z->graph_kernels[par] = launches_total() - l0;
-    } else {
-      count_launches((unsigned)z->graph_kernels[par]);
-    }
+    const int rc = fused_capture(s, par);
+    if (rc) return rc;
+    count_launches((unsigned)z->graph_kernels[par]);
     CUF(cudaGraphLaunch(z->gexec[par], s->st));
   } else {
     const int rc = fused_body(s);
     if (rc) return rc;
   }
-  s->step += 1;
-  if (s->M > 0) s->cx ^= 1;
+  fused_step_taken(s);
   return SELM_OK;
 }
 

@@ -26,6 +26,7 @@ static std::atomic<unsigned long long> g_launches{0};
 
 namespace selm {
 void count_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void uncount_launches(unsigned long long n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 unsigned long long launches_total() { return g_launches.load(); }
 }  // namespace selm
 
@@ -52,6 +53,7 @@ template <typename T> static int dalloc(selm_sim* s, T** p, size_t n) {
     return selm_fail(SELM_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
   }
   s->allocs.push_back(*p);
+  s->dev_bytes += sizeof(T) * n;
   return SELM_OK;
 }
 
@@ -599,6 +601,7 @@ extern "C" int selm_initial(selm_sim* s) {
 extern "C" int selm_step(selm_sim* s, int nsteps) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
   if (!s->initialized) return selm_fail(SELM_ERR_STATE, "selm_initial has not been called");
+  if (s->batch) return selm_fail(SELM_ERR_STATE, "the simulation belongs to a batch: step it with selm_batch_step");
   if (nsteps < 0) return selm_fail(SELM_ERR_INVALID, "nsteps < 0");
   for (int i = 0; i < nsteps; i++) {
     const int rc = (s->prm.form == SELM_FORM_PLAIN64) ? plain_step(s) : fused_step(s);
@@ -609,6 +612,7 @@ extern "C" int selm_step(selm_sim* s, int nsteps) {
 
 extern "C" int selm_destroy(selm_sim* s) {
   if (!s) return SELM_OK;
+  batch_detach(s);
   if (s->st) cudaStreamSynchronize(s->st);
   for (auto& ev : s->pending) {
     cudaEventDestroy(ev.a);
@@ -680,6 +684,7 @@ extern "C" int selm_status(selm_sim* s, unsigned int* word) {
 
 extern "C" int selm_set_stream(selm_sim* s, void* stream) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  if (s->batch) return selm_fail(SELM_ERR_STATE, "the simulation belongs to a batch and runs on its stream");
   CU(cudaStreamSynchronize(s->st));
   if (s->own_st) cudaStreamDestroy(s->st);
   if (stream) {
@@ -702,6 +707,7 @@ extern "C" int selm_synchronize(selm_sim* s) {
 
 extern "C" int selm_profile_enable(selm_sim* s, int enable) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  if (s->batch && enable) return selm_fail(SELM_ERR_STATE, "a batch member is timed through its batch, not per kernel");
   prof_collect(s);
   s->prof = enable != 0;
   if (enable) s->prof_acc.clear();

@@ -17,6 +17,7 @@ struct ProfEvent {
 };
 
 struct FusedState;  // spectral-form buffers (fluid_fused.cu)
+struct selm_batch;  // batched stepping of several simulations (batch.cpp)
 
 struct selm_sim {
   selm_params prm{};
@@ -26,6 +27,8 @@ struct selm_sim {
   cudaStream_t st = nullptr;
   bool own_st = false;
   std::vector<void*> allocs;
+  unsigned long long dev_bytes = 0;  // device bytes allocated for this simulation
+  selm_batch* batch = nullptr;       // the batch this simulation steps in, if any
   // monomers (Lagrangian::d_x/d_v/d_f/d_m, cuda/SELM_Lagrangian.cuh:22-25); x double-buffered
   int M = 0;
   double* x[2] = {nullptr, nullptr};
@@ -74,3 +77,11 @@ int fused_set_field(selm_sim* s, int which, const double* in);
 int fused_stream_changed(selm_sim* s);
 void fused_invalidate_graphs(selm_sim* s);
 void fused_release(selm_sim* s);
+// the captured step of positions x[par] -> x[par ^ 1] (captured on first use, kept)
+int fused_step_graph(selm_sim* s, int par, cudaGraph_t* graph, unsigned long long* kernels);
+// host bookkeeping of one step taken by a graph launched elsewhere
+void fused_step_taken(selm_sim* s);
+
+// batches (batch.cpp)
+void batch_mark_dirty(selm_batch* b);
+int batch_detach(selm_sim* s);

@@ -10,6 +10,7 @@ namespace selm {
 
 // kernels launched by this library since load (process-wide, host side)
 void count_launches(unsigned n);
+void uncount_launches(unsigned long long n);  // launches recorded into a graph capture, not run
 unsigned long long launches_total();
 
 constexpr int kSumParts = 296;  // fixed number of partial sums (2 per SM)

@@ -164,8 +164,18 @@ class Selm:
 
     def final(self) -> None:
         if self._h:
-            self._L.selm_destroy(self._h)
+            b = getattr(self, "_batch", None)
+            if b is not None:
+                b._members.remove(self)
+                self._batch = None
+            self._L.selm_destroy(self._h)  # leaves its batch first
             self._h = None
+
+    def device_bytes(self) -> int:
+        """Device memory this simulation holds (selm_device_bytes)."""
+        n = C.c_ulonglong()
+        check(self._L.selm_device_bytes(self._h, C.byref(n)))
+        return int(n.value)
 
     def __del__(self):
         try:
@@ -217,6 +227,64 @@ class Selm:
         n = C.c_long()
         check(self._L.selm_profile_read(self._h, name.encode(), C.byref(ms), C.byref(n)))
         return float(ms.value), int(n.value)
+
+
+class Batch:
+    """Simulations of the fused forms stepped together by one graph launch per
+    step (selm_batch_*).  Members run on the batch's stream while they belong
+    to it, are stepped only through it, and give the same results bit for bit
+    as when stepped alone."""
+
+    def __init__(self, stream_handle: int | None = None):
+        L = _lib.load()
+        self._L = L
+        h = C.c_void_p()
+        check(L.selm_batch_create(C.c_void_p(stream_handle) if stream_handle else None, C.byref(h)))
+        self._h = h
+        self._members: list[Selm] = []
+
+    def add(self, sim: Selm) -> None:
+        check(self._L.selm_batch_add(self._h, sim._h))
+        sim._batch = self
+        self._members.append(sim)
+
+    def remove(self, sim: Selm) -> None:
+        check(self._L.selm_batch_remove(self._h, sim._h))
+        sim._batch = None
+        self._members.remove(sim)
+
+    def run(self, nsteps: int = 1) -> None:
+        check(self._L.selm_batch_step(self._h, int(nsteps)))
+
+    step = run
+
+    def __len__(self) -> int:
+        return int(self._L.selm_batch_size(self._h))
+
+    @property
+    def members(self) -> list:
+        return list(self._members)
+
+    @property
+    def stream(self) -> int:
+        return int(self._L.selm_batch_get_stream(self._h) or 0)
+
+    def synchronize(self) -> None:
+        check(self._L.selm_batch_synchronize(self._h))
+
+    def final(self) -> None:
+        if self._h:
+            for m in self._members:
+                m._batch = None
+            self._members = []
+            self._L.selm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.final()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------- operators

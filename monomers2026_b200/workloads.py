@@ -162,3 +162,36 @@ def config(idx: int, kT: float | None = None, form: str = "plain64", body: float
 
 def fene_chain_count_for(M: int, length: int = 100) -> int:
     return max(1, int(math.ceil(M / length)))
+
+
+def replica(n: int, nchains: int, length: int, kT: float, seed: int, form: str = "fused32",
+            integrator: str = "inertial") -> Workload:
+    """One replica of the batched ensemble: FENE + WCA chains (same force field as
+    configurations 2-3) in a periodic box L = n on an n^3 grid (dx = 1), its own
+    geometry and Philox seed."""
+    rng = np.random.default_rng(seed)
+    L = float(n)
+    x = random_walk_chains(nchains, length, L, 0.0, rng, min_sep=0.95)
+    topo = fene_wca_topology(nchains, length)
+    p = Params(numMeshPtsPerDir=(n, n, n), box_lo=0.0, box_hi=L, rho=1.0, mu=1.0, KB=1.0, T=kT, dt=0.005,
+               form=form, integrator=integrator)
+    p.flagStochasticDriving = int(kT > 0)
+    p.SELM_Seed = seed
+    M = len(x)
+    return Workload(name=f"replica{seed}", params=p, x=x, mass=np.ones(M), topology=topo, nsteps=0)
+
+
+def ensemble(nrep: int = 256, grids=(32, 48, 64, 96), m_range=(50, 2000), length: int = 50,
+             kT_range=(0.5, 2.0), seed: int = 1004, form: str = "fused32") -> list:
+    """Configuration 4: nrep replicas, grid uniform over ``grids`` (L = N, dx = 1),
+    monomer count log-uniform in ``m_range`` as chains of ``length``, kT uniform in
+    ``kT_range``; replica r has geometry and Philox seed ``seed * 1000 + r``."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for r in range(nrep):
+        n = int(rng.choice(grids))
+        M = float(np.exp(rng.uniform(np.log(m_range[0]), np.log(m_range[1]))))
+        nch = max(1, int(round(M / length)))
+        kT = float(rng.uniform(*kT_range))
+        out.append(replica(n, nch, length, kT, seed * 1000 + r, form=form))
+    return out
