@@ -22,6 +22,7 @@ oracle/) on the host cores, one rank only.
 from __future__ import annotations
 
 import argparse
+from dataclasses import replace
 import json
 import os
 import statistics
@@ -314,6 +315,11 @@ def run_ours(args, rank, world, local_rank):
                 "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "algorithmic_bytes": ab,
                 "traffic": traffic_from_profiles(dom, args.form, N)}
 
+    # ---- batched ensemble and serving (rank 0 at N=1)
+    batched = serving = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched, serving = batched_and_serving(args)
+
     # ---- CPU baseline (rank 0 at N=1): the FP64 oracle port on a bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -345,11 +351,56 @@ def run_ours(args, rank, world, local_rank):
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "batched": batched,
+            "serving": serving,
             "gpu_launches": int(launches),
             "clocks": clocks,
             "status_word": status,
         }
         print(json.dumps(out))
+
+
+def batched_and_serving(args):
+    """Batched ensemble (256 replicas over {32,48,64,96}^3, one graph launch per
+    step) against the same replicas stepped one after another in the plain FP64
+    form; FP32 against FP64 velocities on 8 sampled replicas; a bounded serving
+    run (Poisson arrivals at 200/s, steps scaled by 1/50, HBM budget 150 GB)."""
+    from monomers2026_b200 import serving as SV
+    from monomers2026_b200 import workloads as W
+    from monomers2026_b200.selm import Selm
+
+    log("batched ensemble: 256 replicas")
+    ens = W.ensemble(256)
+    b = SV.run_ensemble(ens, steps=args.batch_steps, warmup=3)
+    log(f"batched: {b['replica_steps_per_s']:.0f} replica-steps/s, step p50 {b['step_ms']['p50']:.2f} ms")
+    seq = SV.run_sequential(ens, steps=2, form="plain64")
+    b["sequential_plain64_replica_steps_per_s"] = seq["replica_steps_per_s"]
+    b["speedup_vs_sequential_plain64"] = b["replica_steps_per_s"] / seq["replica_steps_per_s"]
+    log(f"sequential plain64: {seq['replica_steps_per_s']:.0f} replica-steps/s")
+    errs = []
+    for w in ens[::32][:8]:
+        v = {}
+        for form in ("fused32", "fused64"):
+            s = Selm(replace(w.params, form=form), w.x, w.mass, topology=w.topology)
+            s.initial()
+            s.run(10)
+            v[form] = s.particles()[1]
+            s.final()
+        errs.append(float(np.abs(v["fused32"] - v["fused64"]).max() / np.abs(v["fused64"]).max()))
+    b["fp32_vs_fp64_velocity_rel_err"] = {"max": max(errs), "replicas": len(errs), "steps": 10}
+    b["config"] = {"workload": "256 replicas, grid uniform over {32,48,64,96}^3 (L=N), monomers log-uniform "
+                               "in 50-2000 as FENE+WCA chains of 50, kT uniform in [0.5,2], own Philox seed each",
+                   "form": "fused32", "l2": "not flushed: the ensemble's fields (GBs) exceed L2"}
+    log("serving run")
+    jobs = SV.serving_jobs(64, steps_scale=0.02)
+    srv = SV.Server(budget_bytes=150 * 10**9)
+    sv = srv.run(jobs)
+    srv.final()
+    sv["config"] = {"workload": "64 jobs, Poisson arrivals at 200/s, grid {32,48,64,96,128}^3 w.p. "
+                                ".3/.3/.2/.15/.05, one chain of U[20,5000] monomers, U[500,5000] steps x 0.02",
+                    "budget_bytes": 150 * 10**9, "form": "fused32"}
+    log(f"serving: {sv['jobs']} jobs, step p99 {sv['step_ms']['p99']:.2f} ms")
+    return b, sv
 
 
 def cpu_baseline(wl, budget_s=20.0):
@@ -433,6 +484,8 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other forms")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-ensemble and serving runs")
+    ap.add_argument("--batch-steps", type=int, default=20)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

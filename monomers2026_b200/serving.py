@@ -1,0 +1,251 @@
+"""Batched ensembles and a continuous-batching server on one GPU.
+
+The reference runs one simulation per process.  Here many simulations of
+the fused forms live on the device at once and step together, one CUDA-graph
+launch per step (``Batch``):
+
+* ``run_ensemble`` steps a fixed set of replicas (the batched-ensemble
+  configuration) and reports replica-steps/s and the per-step latency of
+  the batch launch (CUDA events on the batch stream, p50/p99);
+* ``run_sequential`` steps the same replicas one after another with single
+  launches (the plain FP64 form for the reference-structured baseline);
+* ``Server`` admits jobs as they arrive while their device memory fits an
+  HBM budget, adds them to the running batch between steps, and retires each
+  job when its steps are done (state read back, memory freed): continuous
+  batching.  A job's result does not depend on what else is in the batch
+  (each member keeps its own buffers and Philox counters).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import time
+from collections import deque
+
+import numpy as np
+
+from .selm import Batch, Selm
+
+_FP = {"fused32": 4, "fused64": 8, "plain64": 8}
+
+
+def estimate_device_bytes(params, natoms: int, pairs: bool = True) -> int:
+    """Upper estimate of the device memory of one simulation (for admission
+    before it is created): fields, spectra, monomer arrays, stencil records,
+    tile and force-cell buckets and the neighbour list."""
+    nx, ny, nz = (int(v) for v in params.numMeshPtsPerDir)
+    N = nx * ny * nz
+    N2 = (nx // 2 + 1) * ny * nz
+    s = _FP[params.form]
+    if params.form == "plain64":
+        grid = 8 * (3 * N * 4 + N * 3) + 16 * 3 * N2
+    else:
+        grid = 2 * 3 * N * s + 2 * 3 * N2 * 2 * s
+    tiles = (nx // 16 + 1) * (ny // 8 + 1) * (nz // 8 + 1)
+    M = max(1, int(natoms))
+    mono = M * (2 * 24 + 3 * 24 + 8 + (128 if s == 4 else 224)) + 4 * (4 * tiles + 20 * M)
+    nl = 0
+    if pairs:
+        nc3 = min(2 * M, N) + 1
+        nl = 4 * (64 * M + 2 * M) + 24 * M + 4 * (4 * nc3 + 4 * M)
+    return int(1.1 * (grid + mono + nl)) + (1 << 20)
+
+
+def _make(wl, form=None) -> Selm:
+    p = wl.params
+    if form is not None:
+        p = dataclasses.replace(p, form=form)
+    s = Selm(p, wl.x, wl.mass, v=wl.v, topology=wl.topology)
+    s.initial()
+    return s
+
+
+def _pcts(ms):
+    a = np.asarray(ms, dtype=float)
+    return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)), "mean": float(a.mean())}
+
+
+def run_ensemble(workloads, steps: int, warmup: int = 3, form: str = "fused32"):
+    """Step all replicas together; device-timed per batch launch."""
+    import torch
+
+    sims = [_make(w, form) for w in workloads]
+    b = Batch()
+    for s in sims:
+        b.add(s)
+    stream = torch.cuda.ExternalStream(b.stream)
+    b.run(warmup)
+    b.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, e in ev:
+        a.record(stream)
+        b.run(1)
+        e.record(stream)
+    b.synchronize()
+    per = [a.elapsed_time(e) for a, e in ev]
+    total_ms = float(sum(per))
+    cells = sum(int(np.prod(w.params.numMeshPtsPerDir)) for w in workloads)
+    status = [s.status() for s in sims]
+    out = {
+        "replicas": len(sims),
+        "steps": steps,
+        "replica_steps_per_s": len(sims) * steps / (total_ms / 1e3),
+        "cell_steps_per_s": cells * steps / (total_ms / 1e3),
+        "step_ms": _pcts(per),
+        "device_bytes": int(sum(s.device_bytes() for s in sims)),
+        "status_nonzero": int(sum(1 for w in status if w)),
+    }
+    b.final()
+    for s in sims:
+        s.final()
+    return out
+
+
+def run_sequential(workloads, steps: int, form: str = "plain64"):
+    """Each replica stepped alone, one after another (device-timed per replica)."""
+    import torch
+
+    total_ms = 0.0
+    for w in workloads:
+        s = _make(w, form)
+        st = torch.cuda.Stream()
+        s.set_stream(st.cuda_stream)
+        s.run(1)
+        s.synchronize()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s.run(steps)
+        e.record(st)
+        e.synchronize()
+        total_ms += a.elapsed_time(e)
+        s.final()
+    return {"replicas": len(workloads), "steps": steps,
+            "replica_steps_per_s": len(workloads) * steps / (total_ms / 1e3)}
+
+
+@dataclasses.dataclass
+class Job:
+    jid: int
+    workload: object
+    nsteps: int
+    arrival: float  # seconds after the start of the run
+    admitted: float = math.nan
+    done: float = math.nan
+    x: np.ndarray | None = None
+    v: np.ndarray | None = None
+    status: int = 0
+
+
+class Server:
+    """Continuous batching under an HBM budget.
+
+    ``run(jobs)`` plays the arrivals on the wall clock: between two batch
+    steps it admits every arrived job whose estimated memory fits the budget
+    (first come, first served), then steps the batch once; jobs whose steps
+    are done are read back and retired, freeing their memory for the queue."""
+
+    def __init__(self, budget_bytes: int, form: str = "fused32"):
+        self.budget = int(budget_bytes)
+        self.form = form
+        self.used = 0
+        self.peak = 0
+        self.batch = Batch()
+
+    def run(self, jobs: list[Job], max_seconds: float = 600.0):
+        import torch
+
+        stream = torch.cuda.ExternalStream(self.batch.stream)
+        pending = deque(sorted(jobs, key=lambda j: j.arrival))
+        queue: deque = deque()
+        active: list = []  # (job, sim, steps done, bytes)
+        step_ev = []
+        finished = []
+        t0 = time.perf_counter()
+        while pending or queue or active:
+            now = time.perf_counter() - t0
+            if now > max_seconds:
+                raise RuntimeError("serving run exceeded its time bound")
+            while pending and pending[0].arrival <= now:
+                queue.append(pending.popleft())
+            while queue:
+                j = queue[0]
+                est = estimate_device_bytes(dataclasses.replace(j.workload.params, form=self.form),
+                                            len(j.workload.mass))
+                if self.used + est > self.budget and active:
+                    break
+                queue.popleft()
+                s = _make(j.workload, self.form)
+                nb = s.device_bytes()
+                self.used += nb
+                self.peak = max(self.peak, self.used)
+                self.batch.add(s)
+                j.admitted = time.perf_counter() - t0
+                active.append([j, s, 0, nb])
+            if not active:
+                if pending:
+                    time.sleep(max(0.0, min(0.01, pending[0].arrival - (time.perf_counter() - t0))))
+                continue
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            self.batch.run(1)
+            e.record(stream)
+            step_ev.append((a, e, len(active)))
+            keep = []
+            for rec in active:
+                rec[2] += 1
+                j, s, k, nb = rec
+                if k >= j.nsteps:
+                    j.x, j.v, _ = s.particles()  # waits for the batch's work
+                    j.status = s.status()
+                    j.done = time.perf_counter() - t0
+                    self.batch.remove(s)
+                    s.final()
+                    self.used -= nb
+                    finished.append(j)
+                else:
+                    keep.append(rec)
+            active = keep
+        self.batch.synchronize()
+        per = [a.elapsed_time(e) for a, e, _ in step_ev]
+        wall = time.perf_counter() - t0
+        rs = sum(j.nsteps for j in finished)
+        cells = sum(int(np.prod(j.workload.params.numMeshPtsPerDir)) * j.nsteps for j in finished)
+        return {
+            "jobs": len(finished),
+            "batch_steps": len(per),
+            "max_batch": max((n for _, _, n in step_ev), default=0),
+            "step_ms": _pcts(per) if per else None,
+            "job_latency_s": _pcts([j.done - j.arrival for j in finished]),
+            "replica_steps_per_s_device": rs / (sum(per) / 1e3) if per else 0.0,
+            "replica_steps_per_s_wall": rs / wall,
+            "cell_steps_per_s_device": cells / (sum(per) / 1e3) if per else 0.0,
+            "peak_device_bytes": int(self.peak),
+            "wall_s": wall,
+            "status_nonzero": sum(1 for j in finished if j.status),
+        }
+
+    def final(self):
+        self.batch.final()
+
+
+def serving_jobs(njobs: int, rate: float = 200.0, grids=(32, 48, 64, 96, 128),
+                 weights=(0.3, 0.3, 0.2, 0.15, 0.05), m_range=(20, 5000), steps_range=(500, 5000),
+                 steps_scale: float = 1.0, seed: int = 1005, form: str = "fused32") -> list[Job]:
+    """Serving configuration: Poisson arrivals at ``rate``/s, grid by ``weights``,
+    one chain of U[m_range] monomers, U[steps_range] steps (times
+    ``steps_scale`` for a bounded run), kT in [0.5, 2]; job j has geometry and
+    Philox seed ``seed * 1000 + j``."""
+    from .workloads import replica
+
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    jobs = []
+    for jid in range(njobs):
+        t += rng.exponential(1.0 / rate)
+        n = int(rng.choice(grids, p=np.asarray(weights) / np.sum(weights)))
+        M = int(rng.integers(m_range[0], m_range[1] + 1))
+        steps = max(1, int(round(rng.integers(steps_range[0], steps_range[1] + 1) * steps_scale)))
+        kT = float(rng.uniform(0.5, 2.0))
+        wl = replica(n, 1, M, kT, seed * 1000 + jid, form=form)
+        jobs.append(Job(jid=jid, workload=wl, nsteps=steps, arrival=t))
+    return jobs

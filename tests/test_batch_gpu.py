@@ -99,3 +99,34 @@ def test_device_bytes_grow_with_the_grid():
     N = 48 ** 3
     N2 = 25 * 48 * 48
     assert bl > 4 * 3 * N * 2 + 8 * 3 * N2 * 2
+
+
+def test_server_results_same_alone_and_in_mix():
+    from monomers2026_b200.serving import Server, estimate_device_bytes, serving_jobs
+
+    jobs = serving_jobs(6, rate=2000.0, grids=(16, 24, 32), weights=(1, 1, 1), m_range=(20, 200),
+                        steps_range=(5, 20), seed=77)
+    # a budget of about three jobs: later arrivals wait in the queue for memory
+    per = [estimate_device_bytes(j.workload.params, len(j.workload.mass)) for j in jobs]
+    srv = Server(budget_bytes=int(3.2 * max(per)))
+    out = srv.run(jobs)
+    srv.final()
+    assert out["jobs"] == 6 and out["status_nonzero"] == 0
+    assert out["max_batch"] >= 2  # jobs overlapped on the device
+    for j in jobs:
+        s = _sim(j.workload)
+        s.run(j.nsteps)
+        x, v, _ = s.particles()
+        assert np.array_equal(x, j.x) and np.array_equal(v, j.v), j.jid
+        s.final()
+
+
+def test_estimate_covers_device_bytes():
+    from monomers2026_b200.serving import estimate_device_bytes
+
+    for n, M in ((16, 20), (32, 500), (64, 3000)):
+        wl = W.replica(n, 1, M, 1.0, 50 + n)
+        s = _sim(wl)
+        est = estimate_device_bytes(wl.params, M)
+        assert s.device_bytes() <= est < 3 * s.device_bytes() + (8 << 20), (n, M, s.device_bytes(), est)
+        s.final()
