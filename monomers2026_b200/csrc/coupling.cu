@@ -432,6 +432,81 @@ __device__ __forceinline__ void record_store(WRec<T>& R, int d, const int base[3
   }
 }
 
+// Tiles of one axis that the union stencil (cells c0 .. c0+4, wrapped)
+// reaches: up to three distinct ones (a partial last tile can add a third).
+__device__ __forceinline__ int axis_tile_set(double g, int a, const BinSpec& bs, int& t0, int& t1, int& t2) {
+  const int n = bs.n[a], T = bs.tile[a];
+  const int c0 = wrapi((int)floor(g - 0.5) - 1, n);
+  t0 = c0 / T;
+  t1 = -1;
+  t2 = -1;
+  int cnt = 1;
+#pragma unroll
+  for (int i = 1; i < 5; i++) {
+    int c = c0 + i;
+    if (c >= n) c -= n;
+    const int t = c / T;
+    if (t != t0 && t != t1 && t != t2) {
+      if (t1 < 0) t1 = t;
+      else t2 = t;
+      cnt++;
+    }
+  }
+  return cnt;
+}
+
+// File monomer p under every spread tile its union stencil reaches: a slot
+// of the tile while it has room, else the overflow list.
+__device__ __forceinline__ void tile_append(const TileSlots& ts, int p, double gx, double gy, double gz, uint32_t* err) {
+  const BinSpec& bs = ts.bs;
+  if (!isfinite(gx)) gx = 0.0;
+  if (!isfinite(gy)) gy = 0.0;
+  if (!isfinite(gz)) gz = 0.0;
+  int x0, x1, x2, y0, y1, y2, z0, z1, z2;
+  const int nxs = axis_tile_set(gx, 0, bs, x0, x1, x2);
+  const int nys = axis_tile_set(gy, 1, bs, y0, y1, y2);
+  const int nzs = axis_tile_set(gz, 2, bs, z0, z1, z2);
+  auto place = [&](int t, int slot) {
+    if (slot < ts.cap) {
+      ts.slots[(long)t * ts.cap + slot] = p;
+    } else {
+      const int q = atomicAdd(ts.ovf_count, 1);
+      if (q < ts.ovf_cap) ts.ovf[q] = make_int2(t, p);
+      else atomicOr(err, ERR_BUCKET_OVERFLOW);
+    }
+  };
+  if (nxs <= 2 && nys <= 2 && nzs <= 2) {
+    // at most 2 x 2 x 2 tiles (tiles of at least 5 cells): all counters bumped
+    // before any slot is written, so the atomics overlap
+    int tt[8], sl[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int i = c & 1, j = (c >> 1) & 1, k = c >> 2;
+      const bool ok = i < nxs && j < nys && k < nzs;
+      tt[c] = ok ? ((k ? z1 : z0) * bs.nb[1] + (j ? y1 : y0)) * bs.nb[0] + (i ? x1 : x0) : -1;
+      sl[c] = ok ? atomicAdd(&ts.count[tt[c]], 1) : 0;
+    }
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+      if (tt[c] >= 0) place(tt[c], sl[c]);
+    return;
+  }
+#pragma unroll 1
+  for (int k = 0; k < nzs; k++) {
+    const int tz = (k == 0) ? z0 : (k == 1) ? z1 : z2;
+#pragma unroll 1
+    for (int j = 0; j < nys; j++) {
+      const int ty = (j == 0) ? y0 : (j == 1) ? y1 : y2;
+#pragma unroll 1
+      for (int i = 0; i < nxs; i++) {
+        const int tx = (i == 0) ? x0 : (i == 1) ? x1 : x2;
+        const int t = (tz * bs.nb[1] + ty) * bs.nb[0] + tx;
+        place(t, atomicAdd(&ts.count[t], 1));
+      }
+    }
+  }
+}
+
 // lagrangian_update() of cuda/SELM_Kernel.cu:302-373, one thread per
 // (monomer, component); the spread part lives in k_spread_tiles.  The thread
 // of component d also stores, for the spread of the same step, the stencil
@@ -443,7 +518,7 @@ __global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, 
                                                        double* __restrict__ f, const double* __restrict__ m,
                                                        double* __restrict__ tf_out, const int* __restrict__ order,
                                                        WRec<T>* __restrict__ rec, CouplingArgs a,
-                                                       uint32_t* __restrict__ err) {
+                                                       uint32_t* __restrict__ err, TileSlots ts) {
   const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= 3L * a.M) return;
   const int s = (int)(gid / 3), d = (int)(gid % 3);
@@ -457,6 +532,7 @@ __global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, 
   stencil_of<T>(gx, gy, gz, d, base, w);
   const T val = stencil_gather<T>(u + d * N, base, w, a);
   if (rec) record_store<T>(rec[p], d, base, w, a);
+  if (ts.count && d == 0) tile_append(ts, p, gx, gy, gz, err);  // the spread of this step reads x_old
   const double vg = v[g];
   double t_f = -a.upsilon * (vg - (double)val) * a.dt;
   if (a.stochastic) {
@@ -487,7 +563,8 @@ __global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, 
 template <typename T>
 __global__ void __launch_bounds__(256) k_qs_prepare(const double* __restrict__ x, const double* __restrict__ f,
                                                     double* __restrict__ tf_out, WRec<T>* __restrict__ rec,
-                                                    CouplingArgs a, double inv_dv) {
+                                                    CouplingArgs a, double inv_dv, TileSlots ts,
+                                                    uint32_t* __restrict__ err) {
   const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= 3L * a.M) return;
   const int p = (int)(gid / 3), d = (int)(gid % 3);
@@ -496,6 +573,7 @@ __global__ void __launch_bounds__(256) k_qs_prepare(const double* __restrict__ x
   T w[3][4];
   stencil_of<T>(gx, gy, gz, d, base, w);
   record_store<T>(rec[p], d, base, w, a);
+  if (ts.count && d == 0) tile_append(ts, p, gx, gy, gz, err);
   tf_out[gid] = -f[gid] * inv_dv;
 }
 
@@ -528,9 +606,10 @@ __global__ void __launch_bounds__(384) k_qs_move(const T* __restrict__ u, const 
 
 template <typename T>
 cudaError_t qs_prepare(const double* x, const double* f, double* tf, WRec<T>* rec, const CouplingArgs& a,
-                       double inv_dv, cudaStream_t st) {
+                       double inv_dv, cudaStream_t st, const TileSlots* ts, uint32_t* err) {
   if (a.M <= 0) return cudaSuccess;
-  k_qs_prepare<T><<<(unsigned)((3L * a.M + 255) / 256), 256, 0, st>>>(x, f, tf, rec, a, inv_dv);
+  k_qs_prepare<T><<<(unsigned)((3L * a.M + 255) / 256), 256, 0, st>>>(x, f, tf, rec, a, inv_dv,
+                                                                      ts ? *ts : TileSlots{}, err);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -544,9 +623,9 @@ cudaError_t qs_move(const T* u, const double* x_old, double* x_new, double* v, c
   return cudaGetLastError();
 }
 template cudaError_t qs_prepare<double>(const double*, const double*, double*, WRec<double>*, const CouplingArgs&,
-                                        double, cudaStream_t);
+                                        double, cudaStream_t, const TileSlots*, uint32_t*);
 template cudaError_t qs_prepare<float>(const double*, const double*, double*, WRec<float>*, const CouplingArgs&,
-                                       double, cudaStream_t);
+                                       double, cudaStream_t, const TileSlots*, uint32_t*);
 template cudaError_t qs_move<double>(const double*, const double*, double*, double*, const CouplingArgs&, uint32_t*,
                                      cudaStream_t);
 template cudaError_t qs_move<float>(const float*, const double*, double*, double*, const CouplingArgs&, uint32_t*,
@@ -584,11 +663,11 @@ template cudaError_t interp_only<float>(const float*, const double*, int, int, i
 template <typename T>
 cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double* v, double* f, const double* m,
                           double* tf, const int* order, WRec<T>* rec, const CouplingArgs& a, uint32_t* err,
-                          cudaStream_t st) {
+                          cudaStream_t st, const TileSlots* ts) {
   if (a.M <= 0) return cudaSuccess;
   const long nt = 3L * a.M;
   k_interp_update<T><<<(unsigned)((nt + 383) / 384), 384, 0, st>>>(u, x_old, x_new, v, f, m, tf, order, rec, a,
-                                                                    err);
+                                                                    err, ts ? *ts : TileSlots{});
   count_launches(1);
   return cudaGetLastError();
 }
@@ -619,6 +698,8 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
 constexpr int kTX = 16, kTY = 8, kTZ = 8;
 constexpr int kSpreadThreads = 3 * kTY * kTZ;  // also the number of tile rows (component, y, z)
 constexpr int kSpreadCells = 3 * kTZ * kTY * kTX;
+constexpr int kSpreadPad = 32;  // per-lane dummy slots: points outside the tile add there (never read)
+constexpr int kAccWords = kSpreadCells + kSpreadPad;
 static_assert(kTX == 16, "spread_rot assumes 16-cell rows");
 
 // Accumulator slot of cell (cx, cy, cz) of component d.  The x position is
@@ -633,38 +714,175 @@ __device__ __forceinline__ long long to_fixed(double v) { return __double2ll_rn(
 
 template <typename T> struct alignas(4 * sizeof(T)) Vec4 { T v[4]; };
 
+// Tile geometry and fixed-point state shared by the plane additions of a block.
+struct SpreadTile {
+  int t0x, t0y, t0z, ex, ey, ez;
+  double scale;
+  int mode;  // kSplit20, kSplitK or kWide
+  int k, L;
+};
+// Fixed-point modes (v = rounded contribution, n candidates, k = ceil(log2 n)):
+//   kSplit20 (FP32, n <= 4096): lo = v mod 2^20, hi = v >> 20, |v| < 2^(50-k);
+//   kSplitK  (FP32, n <= 65536): lo = v mod 2^(32-k), hi = v >> (32-k), |v| < 2^(62-2k);
+//   kWide    (FP64, or more candidates): one 64-bit word, n |v| < 2^61.
+// In the split modes neither the lo sums (< n 2^L <= 2^32) nor the hi sums
+// (< 2^30 in magnitude) can overflow their 32-bit words.
+enum { kSplit20 = 0, kSplitK = 1, kWide = 2 };
+
+// Add the 16 points of z-plane kz of candidate p's component d (points
+// outside the tile go to the lane's dummy slot, so every lane does the same work).
+template <int MODE, typename T>
+__device__ __forceinline__ void spread_plane(int p, int d, int kz, const SpreadTile& tl, unsigned long long* acc,
+                                             const double* __restrict__ x_old, const double* __restrict__ tf,
+                                             const WRec<T>* __restrict__ rec, const CouplingArgs& a) {
+  unsigned* acc_lo = reinterpret_cast<unsigned*>(acc);
+  unsigned* acc_hi = acc_lo + kAccWords;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int sx = (d != 0), sy = (d != 1), sz = (d != 2);
+  int bx, by, bz;
+  Vec4<T> wx, wy;
+  T wzk;
+  if (rec) {
+    const WRec<T>& R = rec[p];
+    bx = R.b[0][sx];
+    by = R.b[1][sy];
+    bz = R.b[2][sz];
+    wx = *reinterpret_cast<const Vec4<T>*>(R.w[0][sx]);
+    wy = *reinterpret_cast<const Vec4<T>*>(R.w[1][sy]);
+    wzk = R.w[2][sz][kz];
+  } else {
+    const double gx = (x_old[3L * p] - a.lo) / a.dx - (sx ? 0.5 : 0.0);
+    const double gy = (x_old[3L * p + 1] - a.lo) / a.dx - (sy ? 0.5 : 0.0);
+    const double gz = (x_old[3L * p + 2] - a.lo) / a.dx - (sz ? 0.5 : 0.0);
+    const int fx = (int)floor(gx) - 1, fy = (int)floor(gy) - 1, fz = (int)floor(gz) - 1;
+    bx = wrapi(fx, nx);
+    by = wrapi(fy, ny);
+    bz = wrapi(fz, nz);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      wx.v[i] = ref_weight<T>(fabs(gx - (double)(fx + i)));
+      wy.v[i] = ref_weight<T>(fabs(gy - (double)(fy + i)));
+    }
+    wzk = ref_weight<T>(fabs(gz - (double)(fz + kz)));
+  }
+  // tile-relative plane and rows
+  int cz = bz + kz - tl.t0z;
+  if (cz < 0) cz += nz;
+  if (cz >= nz) cz -= nz;
+  if (cz >= tl.ez) return;
+  int cx0 = bx - tl.t0x;
+  if (cx0 < 0) cx0 += nx;
+  int cy0 = by - tl.t0y;
+  if (cy0 < 0) cy0 += ny;
+  const T fz = (T)(-tf[3L * p + d] * tl.scale) * wzk;
+  const int dummy = kSpreadCells + (threadIdx.x & (kSpreadPad - 1));
+  // x-points of the plane: slot within a row, or -1 outside the tile
+  int xo[4];
+#pragma unroll
+  for (int ix = 0; ix < 4; ix++) {
+    int cx = cx0 + ix;
+    if (cx >= nx) cx -= nx;
+    xo[ix] = (cx < tl.ex) ? spread_rot(cx, cz) : -1;
+  }
+  const int plane = spread_row(d, 0, cz);
+#pragma unroll
+  for (int jy = 0; jy < 4; jy++) {
+    int cy = cy0 + jy;
+    if (cy >= ny) cy -= ny;
+    const bool yin = cy < tl.ey;
+    const T rowf = fz * wy.v[jy];
+    const int row = plane + cy * kTX;
+#pragma unroll
+    for (int ix = 0; ix < 4; ix++) {
+      const int slot = (yin && xo[ix] >= 0) ? row + xo[ix] : dummy;
+      const long long v = to_fixed(rowf * wx.v[ix]);
+      if (MODE == kSplit20) {
+        atomicAdd(acc_lo + slot, (unsigned)v & 0xfffffu);
+        atomicAdd(acc_hi + slot, (unsigned)(v >> 20));
+      } else if (MODE == kSplitK) {
+        atomicAdd(acc_lo + slot, (unsigned)v & (0xffffffffu >> tl.k));
+        atomicAdd(acc_hi + slot, (unsigned)(v >> tl.L));
+      } else {
+        atomicAdd(acc + slot, (unsigned long long)v);
+      }
+    }
+  }
+}
+
+template <int MODE, typename T>
+__device__ __forceinline__ void spread_candidates(const int* __restrict__ ids, int n_prim, int n_ovf, const TileSlots& ts,
+                                                  int tb, const SpreadTile& tl, unsigned long long* acc,
+                                                  const double* __restrict__ x_old, const double* __restrict__ tf,
+                                                  const WRec<T>* __restrict__ rec, const CouplingArgs& a) {
+  for (int u = threadIdx.x; u < 12 * n_prim; u += kSpreadThreads) {
+    const int c = u / 12, r = u - 12 * c;
+    spread_plane<MODE, T>(ids[c], r >> 2, r & 3, tl, acc, x_old, tf, rec, a);
+  }
+  // beyond the tile's capacity (rare): a thread takes all planes of an entry
+  for (int q = threadIdx.x; q < n_ovf; q += kSpreadThreads) {
+    const int2 e = ts.ovf[q];
+    if (e.x == tb)
+      for (int r = 0; r < 12; r++) spread_plane<MODE, T>(e.y, r >> 2, r & 3, tl, acc, x_old, tf, rec, a);
+  }
+}
+
+// Candidates of tile tb: the CSR bucket offsets[tb] .. offsets[tb+1] of
+// `entries` (counting-sort binning), or, when ts.count is set, the tile's
+// slots plus its entries in the overflow list (slots filled during the
+// interpolation).
 template <typename T>
 __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__ fgrid, int accumulate,
                                                                  const double* __restrict__ x_old,
                                                                  const double* __restrict__ tf, BinSpec bs,
                                                                  const int* __restrict__ offsets,
-                                                                 const int* __restrict__ entries,
+                                                                 const int* __restrict__ entries, TileSlots ts,
                                                                  const WRec<T>* __restrict__ rec, CouplingArgs a) {
-  __shared__ unsigned long long acc[kSpreadCells];  // wide mode; split mode uses it as lo[cells], hi[cells]
+  __shared__ unsigned long long acc[kAccWords];  // wide mode; split modes use it as lo[kAccWords], hi[kAccWords]
   __shared__ double wmax[kSpreadThreads / 32];
   __shared__ int wbad[kSpreadThreads / 32];
-  unsigned* acc_lo = reinterpret_cast<unsigned*>(acc);
-  unsigned* acc_hi = acc_lo + kSpreadCells;
+  const unsigned* acc_lo = reinterpret_cast<const unsigned*>(acc);
+  const unsigned* acc_hi = acc_lo + kAccWords;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int tb = blockIdx.x;
   const int tbx = tb % bs.nb[0], tby = (tb / bs.nb[0]) % bs.nb[1], tbz = tb / (bs.nb[0] * bs.nb[1]);
-  const int t0x = tbx * kTX, t0y = tby * kTY, t0z = tbz * kTZ;
-  const int ex = min(kTX, nx - t0x), ey = min(kTY, ny - t0y), ez = min(kTZ, nz - t0z);
+  SpreadTile tl;
+  tl.t0x = tbx * kTX;
+  tl.t0y = tby * kTY;
+  tl.t0z = tbz * kTZ;
+  tl.ex = min(kTX, nx - tl.t0x);
+  tl.ey = min(kTY, ny - tl.t0y);
+  tl.ez = min(kTZ, nz - tl.t0z);
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const long N = (long)nx * ny * nz;
-  const int s = offsets[tb], e = offsets[tb + 1], n = e - s;
-  for (int i = tid; i < kSpreadCells; i += kSpreadThreads) acc[i] = 0ull;
+  const bool slots = ts.count != nullptr;
+  int n, n_prim;
+  const int* ids;
+  if (slots) {
+    n = ts.count[tb];
+    n_prim = min(n, ts.cap);
+    ids = ts.slots + (long)tb * ts.cap;
+  } else {
+    const int s0 = offsets[tb];
+    n = n_prim = offsets[tb + 1] - s0;
+    ids = entries + s0;
+  }
+  const int n_ovf = (n > n_prim) ? min(*ts.ovf_count, ts.ovf_cap) : 0;  // only a tile beyond its capacity scans it
+  for (int i = tid; i < kAccWords; i += kSpreadThreads) acc[i] = 0ull;
   // fixed-point scale of this tile from its largest impulse component
   double m = 0.0;
   int bad = 0;
-  for (int q = s + tid; q < e; q += kSpreadThreads) {
-    const int p = entries[q];
+  auto see = [&](int p) {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const double v = fabs(tf[3L * p + c]);
       bad |= !(v <= 1.0e300);
       m = fmax(m, v);
     }
+  };
+  for (int q = tid; q < n_prim; q += kSpreadThreads) see(ids[q]);
+  for (int q = tid; q < n_ovf; q += kSpreadThreads) {
+    const int2 e = ts.ovf[q];
+    if (e.x == tb) see(e.y);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -679,90 +897,19 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
     m = fmax(m, wmax[w]);
     bad |= wbad[w];
   }
-  const int k = (n > 1) ? 32 - __clz(n - 1) : 1;  // ceil(log2 n)
-  const bool split = (sizeof(T) == 4) && k <= 16;
-  const int L = 32 - k;
+  tl.k = (n > 1) ? 32 - __clz(n - 1) : 1;  // ceil(log2 n)
+  tl.mode = (sizeof(T) != 4 || tl.k > 16) ? kWide : (tl.k <= 12) ? kSplit20 : kSplitK;
+  tl.L = (tl.mode == kSplit20) ? 20 : 32 - tl.k;
   int em = 0;
-  if (m > 0.0 && !bad) frexp(split ? m : m * (double)n, &em);  // m (or n m) < 2^em
-  const int S = max(-1000, min(1000, (split ? 62 - 2 * k : 61) - em));
-  const double scale = ldexp(1.0, S), inv_scale = ldexp(1.0, -S);
+  if (m > 0.0 && !bad) frexp(tl.mode == kWide ? m * (double)n : m, &em);  // m (or n m) < 2^em
+  const int bits = (tl.mode == kSplit20) ? 50 - tl.k : (tl.mode == kSplitK) ? 62 - 2 * tl.k : 61;
+  const int S = max(-1000, min(1000, bits - em));
+  tl.scale = ldexp(1.0, S);
+  const double inv_scale = ldexp(1.0, -S);
   if (!bad) {
-    const int total = 12 * n;
-    for (int u = tid; u < total; u += kSpreadThreads) {
-      const int c = u / 12, r = u - 12 * c;
-      const int d = r >> 2, kz = r & 3;
-      const int sx = (d != 0), sy = (d != 1), sz = (d != 2);
-      const int p = entries[s + c];
-      int bx, by, bz;
-      Vec4<T> wx, wy;
-      T wzk;
-      if (rec) {
-        const WRec<T>& R = rec[p];
-        bx = R.b[0][sx];
-        by = R.b[1][sy];
-        bz = R.b[2][sz];
-        wx = *reinterpret_cast<const Vec4<T>*>(R.w[0][sx]);
-        wy = *reinterpret_cast<const Vec4<T>*>(R.w[1][sy]);
-        wzk = R.w[2][sz][kz];
-      } else {
-        const double gx = (x_old[3L * p] - a.lo) / a.dx - (sx ? 0.5 : 0.0);
-        const double gy = (x_old[3L * p + 1] - a.lo) / a.dx - (sy ? 0.5 : 0.0);
-        const double gz = (x_old[3L * p + 2] - a.lo) / a.dx - (sz ? 0.5 : 0.0);
-        const int fx = (int)floor(gx) - 1, fy = (int)floor(gy) - 1, fz = (int)floor(gz) - 1;
-        bx = wrapi(fx, nx);
-        by = wrapi(fy, ny);
-        bz = wrapi(fz, nz);
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          wx.v[i] = ref_weight<T>(fabs(gx - (double)(fx + i)));
-          wy.v[i] = ref_weight<T>(fabs(gy - (double)(fy + i)));
-        }
-        wzk = ref_weight<T>(fabs(gz - (double)(fz + kz)));
-      }
-      // tile-relative plane and rows
-      int cz = bz + kz - t0z;
-      if (cz < 0) cz += nz;
-      if (cz >= nz) cz -= nz;
-      if (cz >= ez) continue;
-      int cx0 = bx - t0x;
-      if (cx0 < 0) cx0 += nx;
-      int cy0 = by - t0y;
-      if (cy0 < 0) cy0 += ny;
-      const T fz = (T)(-tf[3L * p + d] * scale) * wzk;
-      // x-points of the plane: slot within a row and whether inside the tile
-      int xo[4];
-      bool xin[4];
-#pragma unroll
-      for (int ix = 0; ix < 4; ix++) {
-        int cx = cx0 + ix;
-        if (cx >= nx) cx -= nx;
-        xin[ix] = cx < ex;
-        xo[ix] = spread_rot(cx, cz);
-      }
-      const int plane = spread_row(d, 0, cz);
-#pragma unroll
-      for (int jy = 0; jy < 4; jy++) {
-        int cy = cy0 + jy;
-        if (cy >= ny) cy -= ny;
-        if (cy < ey) {
-          const T rowf = fz * wy.v[jy];
-          const int row = plane + cy * kTX;
-#pragma unroll
-          for (int ix = 0; ix < 4; ix++) {
-            if (xin[ix]) {
-              const long long v = to_fixed(rowf * wx.v[ix]);
-              const int slot = row + xo[ix];
-              if (split) {
-                atomicAdd(acc_lo + slot, (unsigned)v & (0xffffffffu >> k));
-                atomicAdd(acc_hi + slot, (unsigned)(v >> L));
-              } else {
-                atomicAdd(acc + slot, (unsigned long long)v);
-              }
-            }
-          }
-        }
-      }
-    }
+    if (tl.mode == kSplit20) spread_candidates<kSplit20, T>(ids, n_prim, n_ovf, ts, tb, tl, acc, x_old, tf, rec, a);
+    else if (tl.mode == kSplitK) spread_candidates<kSplitK, T>(ids, n_prim, n_ovf, ts, tb, tl, acc, x_old, tf, rec, a);
+    else spread_candidates<kWide, T>(ids, n_prim, n_ovf, ts, tb, tl, acc, x_old, tf, rec, a);
   }
   __syncthreads();
   // cells out, a half-warp per 16-cell row
@@ -771,13 +918,22 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
   for (int idx = tid; idx < kSpreadCells; idx += kSpreadThreads) {
     const int row = idx / kTX, cx = idx % kTX;
     const int cy = row % kTY, cz = (row / kTY) % kTZ, d = row / (kTY * kTZ);
-    if (cx < ex && cy < ey && cz < ez) {
-      T* dst = fgrid + d * N + ((long)(t0z + cz) * ny + (t0y + cy)) * nx + t0x + cx;
+    if (cx < tl.ex && cy < tl.ey && cz < tl.ez) {
+      T* dst = fgrid + d * N + ((long)(tl.t0z + cz) * ny + (tl.t0y + cy)) * nx + tl.t0x + cx;
       const int slot = row * kTX + spread_rot(cx, cz);
-      const long long sum = split ? (long long)(int)acc_hi[slot] * (1ll << L) + (long long)acc_lo[slot]
-                                  : (long long)acc[slot];
+      const long long sum = (tl.mode != kWide) ? (long long)(int)acc_hi[slot] * (1ll << tl.L) + (long long)acc_lo[slot]
+                                               : (long long)acc[slot];
       const double add = (double)sum * inv_scale + nan_or_zero;
       *dst = accumulate ? (T)((double)*dst + add) : (T)add;
+    }
+  }
+  if (slots && tid == 0) {
+    // every thread read count[tb] and the overflow counter before the barrier above
+    ts.count[tb] = 0;
+    __threadfence();
+    if (atomicAdd(ts.done, 1u) == gridDim.x - 1) {  // the last block to finish: no block reads it any more
+      *ts.ovf_count = 0;
+      *ts.done = 0u;
     }
   }
 }
@@ -828,17 +984,37 @@ cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const 
   }
   if (bs.mode != 2 || bs.tile[0] != kTX || bs.tile[1] != kTY || bs.tile[2] != kTZ) return cudaErrorInvalidValue;
   k_spread_tiles<T><<<ntiles, kSpreadThreads, 0, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets, sorted,
-                                                        rec, a);
+                                                        TileSlots{}, rec, a);
   count_launches(1);
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t spread_slots(T* fgrid, bool accumulate, const double* x_old, const double* tf, const TileSlots& ts,
+                         const CouplingArgs& a, cudaStream_t st, const WRec<T>* rec) {
+  const BinSpec& bs = ts.bs;
+  const int ntiles = bs.nb[0] * bs.nb[1] * bs.nb[2];
+  if (!accumulate && a.M == 0) {
+    return cudaMemsetAsync(fgrid, 0, sizeof(T) * 3L * a.nx * a.ny * a.nz, st);
+  }
+  if (bs.mode != 2 || bs.tile[0] != kTX || bs.tile[1] != kTY || bs.tile[2] != kTZ || !ts.count)
+    return cudaErrorInvalidValue;
+  k_spread_tiles<T><<<ntiles, kSpreadThreads, 0, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, nullptr, nullptr,
+                                                        ts, rec, a);
+  count_launches(1);
+  return cudaGetLastError();
+}
+template cudaError_t spread_slots<double>(double*, bool, const double*, const double*, const TileSlots&,
+                                          const CouplingArgs&, cudaStream_t, const WRec<double>*);
+template cudaError_t spread_slots<float>(float*, bool, const double*, const double*, const TileSlots&,
+                                         const CouplingArgs&, cudaStream_t, const WRec<float>*);
+
 template cudaError_t interp_update<double>(const double*, const double*, double*, double*, double*, const double*,
                                            double*, const int*, WRec<double>*, const CouplingArgs&, uint32_t*,
-                                           cudaStream_t);
+                                           cudaStream_t, const TileSlots*);
 template cudaError_t interp_update<float>(const float*, const double*, double*, double*, double*, const double*,
                                           double*, const int*, WRec<float>*, const CouplingArgs&, uint32_t*,
-                                          cudaStream_t);
+                                          cudaStream_t, const TileSlots*);
 // the spread kernels use static shared memory only (kept for the engine's set-up order)
 cudaError_t spread_prepare_attributes() { return cudaSuccess; }
 

@@ -638,7 +638,10 @@ template <typename T> static int fused_fluid_t(selm_sim* s) {
   return SELM_OK;
 }
 
-template <typename T> static int fused_step_t(selm_sim* s) {
+// forces_done: set when the step also issued the conservative forces at the
+// new positions (on the side stream, beside the fluid solve, joined at the end)
+template <typename T> static int fused_step_t(selm_sim* s, bool* forces_done) {
+  *forces_done = false;
   FusedState* z = s->fz;
   CouplingArgs a{};
   a.nx = s->nx;
@@ -666,13 +669,10 @@ template <typename T> static int fused_step_t(selm_sim* s) {
     if (s->M > 0) {
       WRec<T>* rec = static_cast<WRec<T>*>(s->wrec);
       prof_mark(s, "interp_update", true);
-      CUF(qs_prepare<T>(xo, s->f, s->tf, rec, a, 1.0 / (s->dx * s->dx * s->dx), s->st));
+      CUF(qs_prepare<T>(xo, s->f, s->tf, rec, a, 1.0 / (s->dx * s->dx * s->dx), s->st, &s->tslots, s->err));
       prof_mark(s, "interp_update", false);
-      prof_mark(s, "bin", true);
-      CUF(bin_particles(xo, s->M, s->tiles, s->tbb, s->st, wrec_bases(rec), wrec_stride<T>()));
-      prof_mark(s, "bin", false);
       prof_mark(s, "spread", true);
-      CUF(spread_gather<T>((T*)z->fp, false, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st, rec));
+      CUF(spread_slots<T>((T*)z->fp, false, xo, s->tf, s->tslots, a, s->st, rec));
       prof_mark(s, "spread", false);
     } else {
       CUF(cudaMemsetAsync(z->fp, 0, sizeof(T) * 3 * s->N, s->st));
@@ -689,19 +689,31 @@ template <typename T> static int fused_step_t(selm_sim* s) {
   if (s->M > 0) {
     WRec<T>* rec = static_cast<WRec<T>*>(s->wrec);
     prof_mark(s, "interp_update", true);
-    CUF(interp_update<T>((const T*)z->u, xo, xn, s->v, s->f, s->m, s->tf, nullptr, rec, a, s->err, s->st));
+    CUF(interp_update<T>((const T*)z->u, xo, xn, s->v, s->f, s->m, s->tf, nullptr, rec, a, s->err, s->st,
+                         &s->tslots));
     prof_mark(s, "interp_update", false);
-    prof_mark(s, "bin", true);
-    CUF(bin_particles(xo, s->M, s->tiles, s->tbb, s->st, wrec_bases(rec), wrec_stride<T>()));
-    prof_mark(s, "bin", false);
+    // The forces at x^{n+1} need only the positions just written: they run on
+    // the side stream while the spread and the fluid solve run here (device
+    // force field only; per-kernel timing keeps one stream).
+    if (s->have_topo && !s->cb && !s->prof) {
+      int rc0 = engine_side_stream(s);
+      if (rc0) return rc0;
+      CUF(cudaEventRecord(s->ev_fork, s->st));
+      CUF(cudaStreamWaitEvent(s->st2, s->ev_fork, 0));
+      rc0 = engine_forces_on(s, xn, s->st2);
+      if (rc0) return rc0;
+      CUF(cudaEventRecord(s->ev_join, s->st2));
+      *forces_done = true;
+    }
     prof_mark(s, "spread", true);
-    CUF(spread_gather<T>((T*)z->fp, false, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st, rec));
+    CUF(spread_slots<T>((T*)z->fp, false, xo, s->tf, s->tslots, a, s->st, rec));
     prof_mark(s, "spread", false);
   } else {
     CUF(cudaMemsetAsync(z->fp, 0, sizeof(T) * 3 * s->N, s->st));
   }
   int rc = fused_fluid_t<T>(s);
   if (rc) return rc;
+  if (*forces_done) CUF(cudaStreamWaitEvent(s->st, s->ev_join, 0));
   return SELM_OK;
 }
 
@@ -719,8 +731,9 @@ int fused_initial(selm_sim* s) {
 // x[parity ^ 1], then the conservative forces at the new positions.
 static int fused_body(selm_sim* s) {
   const bool f32 = s->fz->fp32;
-  int rc = f32 ? fused_step_t<float>(s) : fused_step_t<double>(s);
-  if (rc) return rc;
+  bool done = false;
+  int rc = f32 ? fused_step_t<float>(s, &done) : fused_step_t<double>(s, &done);
+  if (rc || done) return rc;
   if (s->M > 0) s->cx ^= 1;
   rc = engine_forces(s);
   if (s->M > 0) s->cx ^= 1;

@@ -234,6 +234,32 @@ static int alloc_bins(selm_sim* s, const BinSpec& bs, BinBuffers& bb, int M) {
   return SELM_OK;
 }
 
+// Spread-tile slots: a tile holds four times its expected candidate count
+// (plus 64) before its further candidates go to the overflow list, which has
+// room for every entry a monomer can make.
+static int alloc_slots(selm_sim* s, const BinSpec& bs, TileSlots& ts, int M) {
+  const long ntiles = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
+  double per = 1.0;  // expected tiles a union stencil (5 cells per axis) reaches
+  for (int a = 0; a < 3; a++) per *= (bs.nb[a] == 1) ? 1.0 : 1.0 + 4.0 / bs.tile[a];
+  const double avg = (double)M * per / (double)ntiles;
+  long cap = ((long)std::ceil(4.0 * avg) + 64 + 31) / 32 * 32;
+  cap = std::max(128L, std::min(65536L, cap));
+  ts = TileSlots{};
+  ts.bs = bs;
+  ts.cap = (int)cap;
+  ts.ovf_cap = (int)std::min<long>(2147483647L, (long)M * spread_entries_per_monomer(bs) + 1024);
+  int rc;
+  if ((rc = dalloc(s, &ts.count, ntiles))) return rc;
+  if ((rc = dalloc(s, &ts.slots, ntiles * cap))) return rc;
+  if ((rc = dalloc(s, &ts.ovf, (size_t)ts.ovf_cap))) return rc;
+  if ((rc = dalloc(s, &ts.ovf_count, 1))) return rc;
+  if ((rc = dalloc(s, &ts.done, 1))) return rc;
+  CU(cudaMemset(ts.count, 0, sizeof(int) * ntiles));
+  CU(cudaMemset(ts.ovf_count, 0, sizeof(int)));
+  CU(cudaMemset(ts.done, 0, sizeof(unsigned)));
+  return SELM_OK;
+}
+
 extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const double* v, const double* mass) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
   if (M < 0 || (M > 0 && (!x || !mass))) return selm_fail(SELM_ERR_INVALID, "bad particle arrays");
@@ -259,7 +285,7 @@ extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const dou
       if ((rc = dalloc(s, &w, rb * (size_t)M))) return rc;
       s->wrec = w;
     }
-    if ((rc = alloc_bins(s, s->tiles, s->tbb, M))) return rc;
+    if ((rc = alloc_slots(s, s->tiles, s->tslots, M))) return rc;
     CU(cudaMemsetAsync(s->f, 0, sizeof(double) * 3 * M, s->st));
     fused_invalidate_graphs(s);
   }
@@ -495,16 +521,29 @@ extern "C" int selm_set_force_callback(selm_sim* s, selm_force_fn fn, void* user
 }
 
 // ---------------------------------------------------------------- forces
+int engine_side_stream(selm_sim* s) {
+  if (s->st2) return SELM_OK;
+  CU(cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking));
+  CU(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+  CU(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+  return SELM_OK;
+}
+
+int engine_forces_on(selm_sim* s, double* x, cudaStream_t st) {
+  const bool pairs = s->nlist.cap > 0;
+  if (pairs) CU(neighbor_update(x, s->topo, s->fcells, s->fbb, s->nlist, s->err, st));
+  CU(compute_forces(x, s->f, s->topo, pairs ? &s->nlist : nullptr, s->err, st));
+  return SELM_OK;
+}
+
 int engine_forces(selm_sim* s) {
   if (s->M == 0) return SELM_OK;
   double* x = s->x[s->cx];
   if (s->have_topo) {
     prof_mark(s, "forces", true);
-    const bool pairs = s->nlist.cap > 0;
-    if (pairs) CU(neighbor_update(x, s->topo, s->fcells, s->fbb, s->nlist, s->err, s->st));
-    CU(compute_forces(x, s->f, s->topo, pairs ? &s->nlist : nullptr, s->err, s->st));
+    const int rc = engine_forces_on(s, x, s->st);
     prof_mark(s, "forces", false);
-    return SELM_OK;
+    return rc;
   }
   if (s->cb) {
     // host round trip, as Lagrangian_LAMMPS::compute_f (cuda/SELM_Lagrangian_LAMMPS.cu:107-130)
@@ -560,13 +599,11 @@ static int plain_step(selm_sim* s) {
   if (s->M > 0) {
     WRec<double>* rec = static_cast<WRec<double>*>(s->wrec);
     prof_mark(s, "interp_update", true);
-    CU(interp_update<double>(s->u64[s->cu], xo, xn, s->v, s->f, s->m, s->tf, nullptr, rec, a, s->err, s->st));
+    CU(interp_update<double>(s->u64[s->cu], xo, xn, s->v, s->f, s->m, s->tf, nullptr, rec, a, s->err, s->st,
+                             &s->tslots));
     prof_mark(s, "interp_update", false);
-    prof_mark(s, "bin", true);
-    CU(bin_particles(xo, s->M, s->tiles, s->tbb, s->st, wrec_bases(rec), wrec_stride<double>()));
-    prof_mark(s, "bin", false);
     prof_mark(s, "spread", true);
-    CU(spread_gather<double>(s->fg64, true, xo, s->tf, s->tiles, s->tbb.offsets, s->tbb.sorted, a, s->st, rec));
+    CU(spread_slots<double>(s->fg64, true, xo, s->tf, s->tslots, a, s->st, rec));
     prof_mark(s, "spread", false);
     s->cx ^= 1;
   }
@@ -618,9 +655,13 @@ extern "C" int selm_destroy(selm_sim* s) {
     cudaEventDestroy(ev.a);
     cudaEventDestroy(ev.b);
   }
+  if (s->st2) cudaStreamSynchronize(s->st2);
   fused_release(s);
   free_all(s->allocs);
   if (s->own_st && s->st) cudaStreamDestroy(s->st);
+  if (s->st2) cudaStreamDestroy(s->st2);
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_join) cudaEventDestroy(s->ev_join);
   delete s;
   return SELM_OK;
 }

@@ -26,6 +26,8 @@ struct selm_sim {
   double lo = 0, hi = 0, dx = 0;
   cudaStream_t st = nullptr;
   bool own_st = false;
+  cudaStream_t st2 = nullptr;  // side stream: the forces of a step beside its fluid solve
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::vector<void*> allocs;
   unsigned long long dev_bytes = 0;  // device bytes allocated for this simulation
   selm_batch* batch = nullptr;       // the batch this simulation steps in, if any
@@ -43,7 +45,8 @@ struct selm_sim {
   selm::FftTables<double> tb64{};
   selm::FftTables<float> tb32{};
   selm::BinSpec tiles{}, fcells{};
-  selm::BinBuffers tbb{}, fbb{};
+  selm::BinBuffers fbb{};
+  selm::TileSlots tslots{};  // spread-tile candidates, filed during the interpolation
   selm::NeighborList nlist{};  // Verlet list of the pair style
   bool have_topo = false;
   selm::ForceTopo topo{};
@@ -64,6 +67,9 @@ int selm_fail(int code, const std::string& msg);
 void prof_mark(selm_sim* s, const char* name, bool begin);
 int engine_allocate_grid(selm_sim* s);
 int engine_forces(selm_sim* s);
+// the conservative forces at positions x, issued on stream st (device force field only)
+int engine_forces_on(selm_sim* s, double* x, cudaStream_t st);
+int engine_side_stream(selm_sim* s);
 
 // case directory input (Model.SELM + LAMMPS script/data subset), selm_input.cpp
 int selm_case_create(const char* case_dir, selm_sim** out);

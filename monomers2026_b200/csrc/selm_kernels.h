@@ -67,6 +67,20 @@ cudaError_t bin_particles(const double* x, int M, const BinSpec& bs, const BinBu
 // ---- coupling and monomer update
 // Per-monomer stencil of one step: wrapped base cell of the 4-point stencil and
 // its weight factors, per axis, unshifted and shifted by half a cell.
+// Spread-tile slots filled during the interpolation (no counting sort): the
+// candidates of tile t sit at slots[t*cap .. t*cap + min(count[t], cap)), the
+// ones beyond a tile's capacity in the overflow list.  The spread clears
+// count[] and the overflow counter for the next step.
+struct TileSlots {
+  int* count = nullptr;       // [ntiles] appended so far
+  int* slots = nullptr;       // [ntiles][cap]
+  int cap = 0;
+  int2* ovf = nullptr;        // (tile, monomer) beyond a tile's capacity
+  int* ovf_count = nullptr;   // [1]
+  int ovf_cap = 0;
+  unsigned* done = nullptr;   // [1] spread blocks finished; the last one resets ovf_count
+  BinSpec bs{};               // the spread tiles (mode 2)
+};
 template <typename T> struct alignas(16) WRec {
   T w[3][2][4];  // weight factors [axis][unshifted, shifted][point] (16-byte aligned rows)
   int b[3][2];   // stencil bases wrapped into [0, n): [axis][unshifted, shifted]
@@ -90,7 +104,7 @@ struct CouplingArgs {
 template <typename T>
 cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double* v, double* f, const double* m,
                           double* tf, const int* order, WRec<T>* rec, const CouplingArgs& a, uint32_t* err,
-                          cudaStream_t st);
+                          cudaStream_t st, const TileSlots* ts = nullptr);
 template <typename T>
 cudaError_t interp_only(const T* u, const double* x, int M, int nx, int ny, int nz, double lo, double dx, double* out,
                         cudaStream_t st);
@@ -100,12 +114,16 @@ cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const 
                           const int* offsets, const int* sorted, const CouplingArgs& a, cudaStream_t st,
                           const WRec<T>* rec = nullptr);
 
+template <typename T>
+cudaError_t spread_slots(T* fgrid, bool accumulate, const double* x_old, const double* tf, const TileSlots& ts,
+                         const CouplingArgs& a, cudaStream_t st, const WRec<T>* rec);
+
 // ---- conservative forces (FP64)
 // quasi-steady form: stencil records at x and tf = -F inv_dv before the
 // spread; v = Gamma u (x_old), x_new = x_old + dt v after the fluid solve
 template <typename T>
 cudaError_t qs_prepare(const double* x, const double* f, double* tf, WRec<T>* rec, const CouplingArgs& a,
-                       double inv_dv, cudaStream_t st);
+                       double inv_dv, cudaStream_t st, const TileSlots* ts, uint32_t* err);
 template <typename T>
 cudaError_t qs_move(const T* u, const double* x_old, double* x_new, double* v, const CouplingArgs& a, uint32_t* err,
                     cudaStream_t st);

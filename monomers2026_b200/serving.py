@@ -41,9 +41,16 @@ def estimate_device_bytes(params, natoms: int, pairs: bool = True) -> int:
         grid = 8 * (3 * N * 4 + N * 3) + 16 * 3 * N2
     else:
         grid = 2 * 3 * N * s + 2 * 3 * N2 * 2 * s
-    tiles = (nx // 16 + 1) * (ny // 8 + 1) * (nz // 8 + 1)
+    tile = (16, 8, 8)
+    nb = [-(-n // t) for n, t in zip((nx, ny, nz), tile)]
+    tiles = nb[0] * nb[1] * nb[2]
     M = max(1, int(natoms))
-    mono = M * (2 * 24 + 3 * 24 + 8 + (128 if s == 4 else 224)) + 4 * (4 * tiles + 20 * M)
+    per = 1.0
+    for b, t in zip(nb, tile):
+        per *= 1.0 if b == 1 else 1.0 + 4.0 / t
+    cap = max(128, -(-(int(math.ceil(4.0 * M * per / tiles)) + 64) // 32) * 32)
+    slots = 4 * tiles * (cap + 1) + 8 * (27 * M + 1024)  # tile slots and the overflow list
+    mono = M * (2 * 24 + 3 * 24 + 8 + (128 if s == 4 else 224)) + slots
     nl = 0
     if pairs:
         nc3 = min(2 * M, N) + 1
