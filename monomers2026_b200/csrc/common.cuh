@@ -88,9 +88,11 @@ __device__ __forceinline__ void philox_normal2_f32(uint64_t seed, uint32_t c0, u
   philox4x32_10(c0, c1, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)seed, (uint32_t)(seed >> 32), o);
   const float u1 = ((float)(o[0] >> 8) + 0.5f) * (1.0f / 16777216.0f);
   const float u2 = ((float)(o[2] >> 8) + 0.5f) * (1.0f / 16777216.0f);
-  const float r = sqrtf(-2.0f * logf(u1));
+  // fast intrinsics: u1 in (0, 1] and the angle in [0, 2 pi) keep their
+  // errors near 1e-6, well inside what an FP32 noise field resolves
+  const float r = sqrtf(-2.0f * __logf(u1));
   float sn, cs;
-  sincospif(2.0f * u2, &sn, &cs);
+  __sincosf(6.283185307f * u2, &sn, &cs);
   z0 = r * cs;
   z1 = r * sn;
 }

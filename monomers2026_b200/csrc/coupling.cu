@@ -513,7 +513,9 @@ __device__ __forceinline__ void tile_append(const TileSlots& ts, int p, double g
 // bases and weights of axis d (unshifted) and axis d+1 (shifted) in the
 // monomer's record, so the three threads together fill it.
 template <typename T>
-__global__ void __launch_bounds__(384) k_interp_update(const T* __restrict__ u, const double* __restrict__ x_old,
+// 256 threads, at least four blocks per SM in FP32 (64 registers): more warps in flight
+// for the latency-bound stencil gathers
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_interp_update(const T* __restrict__ u, const double* __restrict__ x_old,
                                                        double* __restrict__ x_new, double* __restrict__ v,
                                                        double* __restrict__ f, const double* __restrict__ m,
                                                        double* __restrict__ tf_out, const int* __restrict__ order,
@@ -666,7 +668,7 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
                           cudaStream_t st, const TileSlots* ts) {
   if (a.M <= 0) return cudaSuccess;
   const long nt = 3L * a.M;
-  k_interp_update<T><<<(unsigned)((nt + 383) / 384), 384, 0, st>>>(u, x_old, x_new, v, f, m, tf, order, rec, a,
+  k_interp_update<T><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(u, x_old, x_new, v, f, m, tf, order, rec, a,
                                                                     err, ts ? *ts : TileSlots{});
   count_launches(1);
   return cudaGetLastError();

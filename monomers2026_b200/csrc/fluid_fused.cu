@@ -109,7 +109,7 @@ template <typename T>
 __global__ void __launch_bounds__(512) k_xy_inverse(const cpx<T>* __restrict__ in, T* __restrict__ out, FusedGeom g,
                                                     FftRadix Rx, FftRadix Ry, const cpx<T>* __restrict__ wx,
                                                     const cpx<T>* __restrict__ wy, int rows_per_chunk,
-                                                    int cols_per_chunk, int scr) {
+                                                    int cols_per_chunk, int scr, uint64_t* step) {
   using C = cpx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nx = g.nx, ny = g.ny, nxh = g.nxh;
@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(512) k_xy_inverse(const cpx<T>* __restrict__ i
   C* A = P + (long)ny * nxh;
   C* B = A + scr;
   C* W = B + scr;
+  if (step && blockIdx.x == 0 && threadIdx.x == 0) *step += 1;  // see k_xy_inverse_fast
   const long plane = blockIdx.x;
   const C* src = in + plane * (long)ny * nxh;
   T* dst = out + plane * (long)ny * nx;
@@ -331,8 +332,6 @@ __global__ void __launch_bounds__(256) k_z_update(cpx<T>* __restrict__ work, cpx
   }
 }
 
-__global__ void k_step_advance(uint64_t* step) { *step += 1; }
-
 // ---------------------------------------------------------------- host side
 struct FusedPlan {
   int rows_per_chunk, cols_per_chunk, scr, Wb;
@@ -420,7 +419,7 @@ static void fast_launch(const T* fp, cpx<T>* work, cpx<T>* uhat, T* u, const ZGe
   count_launches(1);
   prof_mark(s, "z_update", false);
   prof_mark(s, "xy_inverse", true);
-  k_xy_inverse_fast<T, N, RP><<<planes, 512, smem_xy_fast<T, N>(), st>>>(work, u, tb.wx_f);
+  k_xy_inverse_fast<T, N, RP><<<planes, 512, smem_xy_fast<T, N>(), st>>>(work, u, tb.wx_f, (uint64_t*)zg.step);
   count_launches(1);
   prof_mark(s, "xy_inverse", false);
 }
@@ -631,7 +630,7 @@ template <typename T> static int fused_fluid_t(selm_sim* s) {
   prof_mark(s, "xy_inverse", true);
   k_xy_inverse<T><<<planes, P.threads_xy, P.smem_xy, s->st>>>((const C*)z->work, (T*)z->u, g, tb.rx, tb.ry,
                                                                 tb.wx_b, tb.wy_b, P.rows_per_chunk,
-                                                                P.cols_per_chunk, P.scr);
+                                                                P.cols_per_chunk, P.scr, z->d_step);
   count_launches(1);
   prof_mark(s, "xy_inverse", false);
   CUF(cudaGetLastError());
@@ -658,9 +657,7 @@ template <typename T> static int fused_step_t(selm_sim* s, bool* forces_done) {
   a.step = 0;
   a.step_ptr = z->d_step;
   a.M = s->M;
-  // the step being taken is (*d_step + 1): advance first
-  k_step_advance<<<1, 1, 0, s->st>>>(z->d_step);
-  count_launches(1);
+  // *d_step is the step being taken; the inverse xy kernel advances it
   double* xo = s->x[s->cx];
   double* xn = s->x[s->cx ^ 1];
   if (s->prm.integrator == SELM_INTEGRATOR_QUASI_STEADY) {
@@ -723,7 +720,8 @@ int fused_initial(selm_sim* s) {
   const size_t es = z->fp32 ? sizeof(float) : sizeof(double);
   CUF(cudaMemsetAsync(z->u, 0, es * 3 * s->N, s->st));
   CUF(cudaMemsetAsync(z->uhat, 0, 2 * es * 3 * s->N2, s->st));
-  CUF(cudaMemsetAsync(z->d_step, 0, sizeof(uint64_t), s->st));
+  static const uint64_t kFirstStep = 1;
+  CUF(cudaMemcpyAsync(z->d_step, &kFirstStep, sizeof(uint64_t), cudaMemcpyHostToDevice, s->st));
   return SELM_OK;
 }
 

@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(512) k_xy_forward_fast(const T* __restrict__ i
 
 template <typename T, int N, int RP>
 __global__ void __launch_bounds__(512) k_xy_inverse_fast(const cpx<T>* __restrict__ in, T* __restrict__ out,
-                                                         const cpx<T>* __restrict__ twx) {
+                                                         const cpx<T>* __restrict__ twx, uint64_t* step) {
   using C = cpx<T>;
   constexpr int N1 = fftk::Split<N>::N1, N2 = fftk::Split<N>::N2;
   constexpr int NH = N / 2 + 1, NLP = NH + 1, RPP = RP + 1;
@@ -112,6 +112,9 @@ __global__ void __launch_bounds__(512) k_xy_inverse_fast(const cpx<T>* __restric
   const long plane = blockIdx.x;
   const C* src = in + plane * (long)N * NH;
   T* dst = out + plane * (long)N * N;
+  // the last kernel of the step's fluid solve advances the device step counter
+  // (the step's noise has been drawn; nothing later in the step reads it)
+  if (step && blockIdx.x == 0 && threadIdx.x == 0) *step += 1;
   for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twx[t];
   for (int idx = threadIdx.x; idx < N * NH; idx += blockDim.x) {
     const int ky = idx / NH, m = idx % NH;
