@@ -124,6 +124,7 @@ extern "C" int selm_batch_add(selm_batch* b, selm_sim* s) {
   s->st = b->st;
   s->own_st = false;
   s->batch = b;
+  fused_invalidate_graphs(s);  // a member's step is captured on one stream
   b->dirty = true;
   return SELM_OK;
 }
@@ -134,6 +135,7 @@ extern "C" int selm_batch_remove(selm_batch* b, selm_sim* s) {
   if (it == b->members.end()) return selm_fail(SELM_ERR_INVALID, "the simulation is not in this batch");
   const cudaError_t e = cudaStreamSynchronize(b->st);
   restore(*it);
+  fused_invalidate_graphs(s);  // alone again: the step with the side stream
   b->members.erase(it);
   b->dirty = true;
   if (e != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
@@ -172,7 +174,10 @@ extern "C" int selm_batch_synchronize(selm_batch* b) {
 extern "C" int selm_batch_destroy(selm_batch* b) {
   if (!b) return SELM_OK;
   cudaStreamSynchronize(b->st);
-  for (auto& m : b->members) restore(m);
+  for (auto& m : b->members) {
+    restore(m);
+    fused_invalidate_graphs(m.s);
+  }
   b->members.clear();
   drop_graphs(b);
   if (b->own_st) cudaStreamDestroy(b->st);

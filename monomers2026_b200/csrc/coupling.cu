@@ -16,6 +16,7 @@
 //                     floating-point atomics; results do not depend on
 //                     scheduling.
 #include <algorithm>
+#include <mutex>
 #include <type_traits>
 
 #include "common.cuh"
@@ -697,11 +698,13 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
 //          overflow for |v| < 2^(62 - 2k); a step of m 2^-(62-2k), 2^-44 of
 //          the tile's largest impulse for n <= 512.  Shared-memory 32-bit
 //          integer atomics are native; 64-bit ones are not.
-constexpr int kTX = 16, kTY = 8, kTZ = 8;
+constexpr int kTX = 16, kTY = 8, kTZ = 16;  // 16 cells in z: fewer candidates straddle two tiles
 constexpr int kSpreadThreads = 3 * kTY * kTZ;  // also the number of tile rows (component, y, z)
 constexpr int kSpreadCells = 3 * kTZ * kTY * kTX;
 constexpr int kSpreadPad = 32;  // per-lane dummy slots: points outside the tile add there (never read)
 constexpr int kAccWords = kSpreadCells + kSpreadPad;
+constexpr size_t kSpreadSmem = sizeof(unsigned long long) * kAccWords;
+constexpr int kMaxSpreadDevices = 64;
 static_assert(kTX == 16, "spread_rot assumes 16-cell rows");
 
 // Accumulator slot of cell (cx, cy, cz) of component d.  The x position is
@@ -839,7 +842,7 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
                                                                  const int* __restrict__ offsets,
                                                                  const int* __restrict__ entries, TileSlots ts,
                                                                  const WRec<T>* __restrict__ rec, CouplingArgs a) {
-  __shared__ unsigned long long acc[kAccWords];  // wide mode; split modes use it as lo[kAccWords], hi[kAccWords]
+  extern __shared__ unsigned long long acc[];  // [kAccWords]; the split modes use it as lo[kAccWords], hi[kAccWords]
   __shared__ double wmax[kSpreadThreads / 32];
   __shared__ int wbad[kSpreadThreads / 32];
   const unsigned* acc_lo = reinterpret_cast<const unsigned*>(acc);
@@ -985,8 +988,10 @@ cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const 
     return cudaMemsetAsync(fgrid, 0, sizeof(T) * 3L * a.nx * a.ny * a.nz, st);
   }
   if (bs.mode != 2 || bs.tile[0] != kTX || bs.tile[1] != kTY || bs.tile[2] != kTZ) return cudaErrorInvalidValue;
-  k_spread_tiles<T><<<ntiles, kSpreadThreads, 0, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets, sorted,
-                                                        TileSlots{}, rec, a);
+  cudaError_t e = spread_prepare_attributes();
+  if (e != cudaSuccess) return e;
+  k_spread_tiles<T><<<ntiles, kSpreadThreads, kSpreadSmem, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets,
+                                                                  sorted, TileSlots{}, rec, a);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -1001,8 +1006,10 @@ cudaError_t spread_slots(T* fgrid, bool accumulate, const double* x_old, const d
   }
   if (bs.mode != 2 || bs.tile[0] != kTX || bs.tile[1] != kTY || bs.tile[2] != kTZ || !ts.count)
     return cudaErrorInvalidValue;
-  k_spread_tiles<T><<<ntiles, kSpreadThreads, 0, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, nullptr, nullptr,
-                                                        ts, rec, a);
+  cudaError_t e = spread_prepare_attributes();
+  if (e != cudaSuccess) return e;
+  k_spread_tiles<T><<<ntiles, kSpreadThreads, kSpreadSmem, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, nullptr,
+                                                                  nullptr, ts, rec, a);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -1017,8 +1024,26 @@ template cudaError_t interp_update<double>(const double*, const double*, double*
 template cudaError_t interp_update<float>(const float*, const double*, double*, double*, double*, const double*,
                                           double*, const int*, WRec<float>*, const CouplingArgs&, uint32_t*,
                                           cudaStream_t, const TileSlots*);
-// the spread kernels use static shared memory only (kept for the engine's set-up order)
-cudaError_t spread_prepare_attributes() { return cudaSuccess; }
+// The tile accumulators (about 50 KB) exceed the default 48 KB of dynamic
+// shared memory: raise the limit once per device (the first call on a device
+// does it; make that call before any stream capture).
+cudaError_t spread_prepare_attributes() {
+  static std::mutex mu;
+  static bool done[kMaxSpreadDevices] = {false};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev >= 0 && dev < kMaxSpreadDevices && done[dev]) return cudaSuccess;
+  if ((e = cudaFuncSetAttribute((const void*)k_spread_tiles<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSpreadSmem)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute((const void*)k_spread_tiles<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSpreadSmem)) != cudaSuccess)
+    return e;
+  if (dev >= 0 && dev < kMaxSpreadDevices) done[dev] = true;
+  return cudaSuccess;
+}
 
 template cudaError_t spread_gather<double>(double*, bool, const double*, const double*, const BinSpec&, const int*,
                                            const int*, const CouplingArgs&, cudaStream_t, const WRec<double>*);

@@ -691,8 +691,10 @@ template <typename T> static int fused_step_t(selm_sim* s, bool* forces_done) {
     prof_mark(s, "interp_update", false);
     // The forces at x^{n+1} need only the positions just written: they run on
     // the side stream while the spread and the fluid solve run here (device
-    // force field only; per-kernel timing keeps one stream).
-    if (s->have_topo && !s->cb && !s->prof) {
+    // force field only; per-kernel timing keeps one stream).  A batch member
+    // keeps one stream: the batch's members already overlap, and the extra
+    // branches only add graph-scheduling work there.
+    if (s->have_topo && !s->cb && !s->prof && !s->batch) {
       int rc0 = engine_side_stream(s);
       if (rc0) return rc0;
       CUF(cudaEventRecord(s->ev_fork, s->st));

@@ -7,7 +7,7 @@
 // cudaFree synchronise the device, which a caller stepping in a tight loop
 // cannot afford.  selm_op_spread_noalloc serves them: the caller passes
 // device buffers for the inputs and the output, and the scratch the spread
-// needs (the counting sort of monomers into 16x8x8-cell spread tiles) lives in one
+// needs (the counting sort of monomers into 16x8x16-cell spread tiles) lives in one
 // file-scope __device__ array of fixed size that every GPU loading this
 // library holds until the process exits.
 //
