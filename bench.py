@@ -228,6 +228,14 @@ def run_ours(args, rank, world, local_rank):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
+    # ---- autotuner: FFT split and z-kernel occupancy for this shape (a throwaway copy)
+    tuned = None
+    if args.form != "plain64" and not args.no_autotune:
+        from monomers2026_b200.autotune import tune
+        wl.params.form = args.form
+        tuned = tune(wl)
+        log(f"autotune: {tuned['choice']}")
+
     # ---- headline form, timed with clocks sampled
     sim = make(args.form)
     log("timed steps")
@@ -351,6 +359,7 @@ def run_ours(args, rank, world, local_rank):
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "autotune": tuned,
             "batched": batched,
             "serving": serving,
             "gpu_launches": int(launches),
@@ -371,7 +380,13 @@ def batched_and_serving(args):
 
     log("batched ensemble: 256 replicas")
     ens = W.ensemble(256)
+    tuned = None
+    if not args.no_autotune:
+        from monomers2026_b200.autotune import tune_ensemble
+        tuned = tune_ensemble(ens)
+        log("autotune: " + ", ".join(f"{t['grid']}^3 {t['choice']}" for t in tuned))
     b = SV.run_ensemble(ens, steps=args.batch_steps, warmup=3)
+    b["autotune"] = tuned
     log(f"batched: {b['replica_steps_per_s']:.0f} replica-steps/s, step p50 {b['step_ms']['p50']:.2f} ms")
     seq = SV.run_sequential(ens, steps=2, form="plain64")
     b["sequential_plain64_replica_steps_per_s"] = seq["replica_steps_per_s"]
@@ -486,6 +501,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-ensemble and serving runs")
     ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--no-autotune", action="store_true", help="keep the built-in kernel choices")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -189,6 +189,20 @@ int selm_batch_destroy(selm_batch* b); /* members leave (not destroyed) */
  * the reference allocates per object in initial() (cuda/SELM_Eulerian_Period.cu:33-60) */
 int selm_device_bytes(selm_sim* s, unsigned long long* bytes);
 
+/* ---- tuning knobs of the fused forms (no counterpart in the reference) ----
+ * SELM_TUNE_FFT_SPLIT: 0 = four-step FFT split with the largest factor <= 16,
+ *   1 = the most balanced split (the same for sizes with one split);
+ * SELM_TUNE_Z_BLOCKS: blocks per SM of the z-pencil kernel, 0 = as many as fit.
+ * selm_tune_set changes one simulation (its step graph is recaptured);
+ * selm_tune_default sets the value that simulations created later with this
+ * cubic grid size and precision (32 or 64) start from.  monomers2026_b200's
+ * autotuner times the candidates and records its choices with it. */
+#define SELM_TUNE_FFT_SPLIT 1
+#define SELM_TUNE_Z_BLOCKS 2
+int selm_tune_set(selm_sim* s, int knob, int value);
+int selm_tune_get(selm_sim* s, int knob, int* value);
+int selm_tune_default(int grid, int precision, int knob, int value);
+
 /* kernels this library has launched since it was loaded (all simulations) */
 unsigned long long selm_kernel_launches(void);
 

@@ -21,6 +21,7 @@ EXPORTED = [
     "selm_last_error", "selm_version",
     "selm_batch_create", "selm_batch_add", "selm_batch_remove", "selm_batch_step", "selm_batch_size",
     "selm_batch_get_stream", "selm_batch_synchronize", "selm_batch_destroy", "selm_device_bytes",
+    "selm_tune_set", "selm_tune_get", "selm_tune_default",
 ]
 
 SELM_OK = 0
@@ -100,6 +101,9 @@ def load():
     L.selm_batch_synchronize.argtypes = [vp]
     L.selm_batch_destroy.argtypes = [vp]
     L.selm_device_bytes.argtypes = [vp, C.POINTER(C.c_ulonglong)]
+    L.selm_tune_set.argtypes = [vp, C.c_int, C.c_int]
+    L.selm_tune_get.argtypes = [vp, C.c_int, ip]
+    L.selm_tune_default.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
     L.selm_last_error.restype = C.c_char_p
     L.selm_version.restype = C.c_char_p
     _lib = L

@@ -173,7 +173,18 @@ template <int R, int S, typename C> struct Dft {
 
 template <int R, int S, typename C> __host__ __device__ __forceinline__ void dft(C* a) { Dft<R, S, C>::run(a); }
 
-// Four-step factorisation used for a line length N (both factors <= 16).
+// Four-step factorisations of a line length N (both factors <= 16): the
+// default takes the largest N1 <= 16; the alternative the most balanced one
+// (N1 >= N2), which an autotuner may prefer.
+template <int N> struct SplitBalanced {
+  static constexpr int pick() {
+    int best = 0;
+    for (int a = 1; a <= 16; a++)
+      if (N % a == 0 && N / a <= 16 && a >= N / a && (best == 0 || a < best)) best = a;
+    return best;
+  }
+  static constexpr int N1 = pick();
+};
 template <int N> struct Split {
   static constexpr int pick() {
     for (int a = 16; a >= 1; a--)

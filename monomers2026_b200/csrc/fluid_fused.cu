@@ -27,6 +27,9 @@
 // Positions stay FP64, the zero mode is set exactly, and the noise amplitude
 // sqrt(2 kB T dt mu / N) * N * sqrt(lambda_h) is formed in FP64 in both forms.
 #include <cmath>
+#include <tuple>
+#include <mutex>
+#include <map>
 
 #include "common.cuh"
 #include "fluid_fused_fast.cuh"
@@ -381,45 +384,59 @@ template <typename T, int N> constexpr int rows_per_chunk_fast() {
 }
 template <typename T, int N> constexpr size_t smem_xy_fast() { return smem_xy_for<T, N>(rows_per_chunk_fast<T, N>()); }
 template <typename T> constexpr int wb_fast() { return sizeof(T) == 8 ? 8 : 16; }
-// The request is raised to 60 KB so that at most three blocks share an SM:
-// with the 128^3 FP32 kernel, four resident blocks per SM measured slower
-// than three (the same kernel at 64 registers and 50 KB).
-template <typename T, int N> constexpr size_t smem_z_fast() {
-  constexpr size_t need = sizeof(cpx<T>) * ((size_t)N * 3 * wb_fast<T>() + N);
-  return need < 60 * 1024 ? 60 * 1024 : need;
+// Shared memory of the z kernel: what its lines need, or more when the
+// blocks per SM are capped (the request then leaves room for no more).  By
+// default at most three blocks share an SM: with the 128^3 FP32 kernel, four
+// resident blocks per SM measured slower than three.
+template <typename T, int N> constexpr size_t smem_z_need() {
+  return sizeof(cpx<T>) * ((size_t)N * 3 * wb_fast<T>() + N);
 }
+constexpr int kZDefaultBlocksPerSm = 3;
+static size_t smem_z_request(size_t need, int blocks_per_sm) {
+  if (blocks_per_sm <= 0) return need;
+  const size_t cap = 228 * 1024 / (size_t)(blocks_per_sm + 1) + 1024;  // blocks_per_sm + 1 do not fit
+  return need < cap ? cap : need;
+}
+constexpr size_t kZSmemMax = 228 * 1024 / 3 + 1024;  // the largest request (two blocks per SM)
 
-template <typename T, int N> static cudaError_t fast_attrs() {
+template <typename T, int N, int N1> static cudaError_t fast_attrs_split() {
   cudaError_t e;
   constexpr int RP = rows_per_chunk_fast<T, N>();
-  if ((e = cudaFuncSetAttribute((const void*)k_xy_forward_fast<T, N, RP>,
+  if ((e = cudaFuncSetAttribute((const void*)k_xy_forward_fast<T, N, N1, RP>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xy_fast<T, N>())))
     return e;
-  if ((e = cudaFuncSetAttribute((const void*)k_xy_inverse_fast<T, N, RP>,
+  if ((e = cudaFuncSetAttribute((const void*)k_xy_inverse_fast<T, N, N1, RP>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xy_fast<T, N>())))
     return e;
-  return cudaFuncSetAttribute((const void*)k_z_update_fast<T, N, wb_fast<T>()>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z_fast<T, N>());
+  const size_t zmax = smem_z_need<T, N>() > kZSmemMax ? smem_z_need<T, N>() : kZSmemMax;
+  return cudaFuncSetAttribute((const void*)k_z_update_fast<T, N, N1, wb_fast<T>()>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zmax);
+}
+template <typename T, int N> static cudaError_t fast_attrs() {
+  cudaError_t e = fast_attrs_split<T, N, fftk::Split<N>::N1>();
+  if (e != cudaSuccess) return e;
+  return fast_attrs_split<T, N, fftk::SplitBalanced<N>::N1>();
 }
 
-template <typename T, int N>
+template <typename T, int N, int N1>
 static void fast_launch(const T* fp, cpx<T>* work, cpx<T>* uhat, T* u, const ZGeom& zg, const FftTables<T>& tb,
                         const double* symx, const double* symy, const double* symz, int ny, int nz, cudaStream_t st,
-                        selm_sim* s) {
+                        selm_sim* s, int z_blocks_per_sm) {
   constexpr int RP = rows_per_chunk_fast<T, N>();
   constexpr int WB = wb_fast<T>();
   const unsigned planes = (unsigned)(3 * nz);
   prof_mark(s, "xy_forward", true);
-  k_xy_forward_fast<T, N, RP><<<planes, 512, smem_xy_fast<T, N>(), st>>>(fp, work, tb.wx_f);
+  k_xy_forward_fast<T, N, N1, RP><<<planes, 512, smem_xy_fast<T, N>(), st>>>(fp, work, tb.wx_f);
   count_launches(1);
   prof_mark(s, "xy_forward", false);
   prof_mark(s, "z_update", true);
-  k_z_update_fast<T, N, WB><<<(unsigned)z_blocks<WB>(zg.nxh, ny), 256, smem_z_fast<T, N>(), st>>>(
+  k_z_update_fast<T, N, N1, WB><<<(unsigned)z_blocks<WB>(zg.nxh, ny), 256,
+                                  smem_z_request(smem_z_need<T, N>(), z_blocks_per_sm), st>>>(
       work, uhat, zg, tb.wz_f, symx, symy, symz);
   count_launches(1);
   prof_mark(s, "z_update", false);
   prof_mark(s, "xy_inverse", true);
-  k_xy_inverse_fast<T, N, RP><<<planes, 512, smem_xy_fast<T, N>(), st>>>(work, u, tb.wx_f, (uint64_t*)zg.step);
+  k_xy_inverse_fast<T, N, N1, RP><<<planes, 512, smem_xy_fast<T, N>(), st>>>(work, u, tb.wx_f, (uint64_t*)zg.step);
   count_launches(1);
   prof_mark(s, "xy_inverse", false);
 }
@@ -449,14 +466,20 @@ template <typename T> static cudaError_t fast_attrs_for(int n) {
   }
 }
 
+// split 0: the default four-step split of N; 1: the most balanced one
 template <typename T>
-static void fast_dispatch(int n, const T* fp, cpx<T>* work, cpx<T>* uhat, T* u, const ZGeom& zg,
-                          const FftTables<T>& tb, const double* symx, const double* symy, const double* symz, int ny,
-                          int nz, cudaStream_t st, selm_sim* s) {
+static void fast_dispatch(int n, int split, int z_blocks_per_sm, const T* fp, cpx<T>* work, cpx<T>* uhat, T* u,
+                          const ZGeom& zg, const FftTables<T>& tb, const double* symx, const double* symy,
+                          const double* symz, int ny, int nz, cudaStream_t st, selm_sim* s) {
   switch (n) {
-#define SELM_CASE(N)                                                                    \
-  case N:                                                                               \
-    fast_launch<T, N>(fp, work, uhat, u, zg, tb, symx, symy, symz, ny, nz, st, s);      \
+#define SELM_CASE(N)                                                                                            \
+  case N:                                                                                                       \
+    if (split == 1)                                                                                             \
+      fast_launch<T, N, fftk::SplitBalanced<N>::N1>(fp, work, uhat, u, zg, tb, symx, symy, symz, ny, nz, st, s, \
+                                                    z_blocks_per_sm);                                          \
+    else                                                                                                        \
+      fast_launch<T, N, fftk::Split<N>::N1>(fp, work, uhat, u, zg, tb, symx, symy, symz, ny, nz, st, s,         \
+                                            z_blocks_per_sm);                                                  \
     break;
     SELM_FAST_SIZES(SELM_CASE)
 #undef SELM_CASE
@@ -483,6 +506,9 @@ struct FusedState {
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   unsigned long long graph_kernels[2] = {0, 0};
   bool fast = false;  // compile-time four-step kernels for this grid size
+  // tuning knobs (SELM_TUNE_*): four-step split, blocks per SM of the z kernel
+  int tune_split = 0;
+  int tune_z_blocks = kZDefaultBlocksPerSm;
 };
 
 #define CUF(x)                                                                                  \
@@ -490,6 +516,50 @@ struct FusedState {
     cudaError_t e_ = (x);                                                                       \
     if (e_ != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+
+// ---------------------------------------------------------------- tuning knobs
+// Process-wide defaults per (grid size, precision) for simulations created
+// later (an autotuner records its choices here), and per-simulation values.
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int>, int> g_tune_defaults;  // (grid, precision bits, knob) -> value
+
+static int tune_valid(int knob, int value) {
+  if (knob == SELM_TUNE_FFT_SPLIT) return value == 0 || value == 1;
+  if (knob == SELM_TUNE_Z_BLOCKS) return value >= 0 && value <= 8;
+  return 0;
+}
+
+extern "C" int selm_tune_default(int grid, int precision, int knob, int value) {
+  if ((precision != 32 && precision != 64) || grid < 4 || !tune_valid(knob, value))
+    return selm_fail(SELM_ERR_INVALID, "selm_tune_default: unknown knob, value, grid or precision");
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_defaults[std::make_tuple(grid, precision, knob)] = value;
+  return SELM_OK;
+}
+
+static int tune_default_of(int grid, int precision, int knob, int fallback) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune_defaults.find(std::make_tuple(grid, precision, knob));
+  return it == g_tune_defaults.end() ? fallback : it->second;
+}
+
+extern "C" int selm_tune_set(selm_sim* s, int knob, int value) {
+  if (!s || !tune_valid(knob, value)) return selm_fail(SELM_ERR_INVALID, "selm_tune_set: unknown knob or value");
+  if (!s->fz) return selm_fail(SELM_ERR_STATE, "the tuning knobs belong to the fused forms");
+  if (knob == SELM_TUNE_FFT_SPLIT) s->fz->tune_split = value;
+  else s->fz->tune_z_blocks = value;
+  fused_invalidate_graphs(s);
+  return SELM_OK;
+}
+
+extern "C" int selm_tune_get(selm_sim* s, int knob, int* value) {
+  if (!s || !value) return selm_fail(SELM_ERR_INVALID, "NULL argument");
+  if (!s->fz) return selm_fail(SELM_ERR_STATE, "the tuning knobs belong to the fused forms");
+  if (knob == SELM_TUNE_FFT_SPLIT) *value = s->fz->tune_split;
+  else if (knob == SELM_TUNE_Z_BLOCKS) *value = s->fz->tune_z_blocks;
+  else return selm_fail(SELM_ERR_INVALID, "selm_tune_get: unknown knob");
+  return SELM_OK;
+}
 
 template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
   using C = cpx<T>;
@@ -529,6 +599,9 @@ template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
   z->plan = plan_for<T>(s->nx, s->ny, s->nz);
   z->fast = fast_size(s->nx) && s->nx == s->ny && s->nx == s->nz;
   if (z->fast) CUF(fast_attrs_for<T>(s->nx));
+  const int prec = (int)(8 * sizeof(T));
+  z->tune_split = tune_default_of(s->nx, prec, SELM_TUNE_FFT_SPLIT, 0);
+  z->tune_z_blocks = tune_default_of(s->nx, prec, SELM_TUNE_Z_BLOCKS, kZDefaultBlocksPerSm);
   CUF(cudaFuncSetAttribute((const void*)k_xy_forward<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)z->plan.smem_xy));
   CUF(cudaFuncSetAttribute((const void*)k_xy_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -610,8 +683,8 @@ template <typename T> static int fused_fluid_t(selm_sim* s) {
     zg.noise_mode = g.noise_mode;
     zg.seed = g.seed;
     zg.step = g.step;
-    fast_dispatch<T>(s->nx, (const T*)z->fp, (C*)z->work, (C*)z->uhat, (T*)z->u, zg, tb, z->symx, z->symy, z->symz,
-                     s->ny, s->nz, s->st, s);
+    fast_dispatch<T>(s->nx, z->tune_split, z->tune_z_blocks, (const T*)z->fp, (C*)z->work, (C*)z->uhat, (T*)z->u,
+                     zg, tb, z->symx, z->symy, z->symz, s->ny, s->nz, s->st, s);
     CUF(cudaGetLastError());
     return SELM_OK;
   }

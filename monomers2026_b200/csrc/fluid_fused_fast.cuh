@@ -40,11 +40,12 @@ __device__ __forceinline__ void pass_a(C* s, int stride, int l, int n2, const C*
 template <int N1, int N2> __device__ __forceinline__ int dpos(int k) { return N2 * (k % N1) + k / N1; }
 
 // ---------------------------------------------------------------- x/y plane kernels
-template <typename T, int N, int RP>
+template <typename T, int N, int N1_, int RP>
 __global__ void __launch_bounds__(512) k_xy_forward_fast(const T* __restrict__ in, cpx<T>* __restrict__ out,
                                                          const cpx<T>* __restrict__ twx) {
   using C = cpx<T>;
-  constexpr int N1 = fftk::Split<N>::N1, N2 = fftk::Split<N>::N2;
+  constexpr int N1 = N1_, N2 = N / N1_;
+  static_assert(N1 * N2 == N && N1 <= 16 && N2 <= 16, "four-step split");
   constexpr int NH = N / 2 + 1, NLP = NH + 1, RPP = RP + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* P = reinterpret_cast<C*>(smem_raw);  // [N rows y][NLP] : element y of line m at y*NLP + m
@@ -99,11 +100,12 @@ __global__ void __launch_bounds__(512) k_xy_forward_fast(const T* __restrict__ i
   }
 }
 
-template <typename T, int N, int RP>
+template <typename T, int N, int N1_, int RP>
 __global__ void __launch_bounds__(512) k_xy_inverse_fast(const cpx<T>* __restrict__ in, T* __restrict__ out,
                                                          const cpx<T>* __restrict__ twx, uint64_t* step) {
   using C = cpx<T>;
-  constexpr int N1 = fftk::Split<N>::N1, N2 = fftk::Split<N>::N2;
+  constexpr int N1 = N1_, N2 = N / N1_;
+  static_assert(N1 * N2 == N && N1 <= 16 && N2 <= 16, "four-step split");
   constexpr int NH = N / 2 + 1, NLP = NH + 1, RPP = RP + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* P = reinterpret_cast<C*>(smem_raw);
@@ -231,14 +233,15 @@ template <int WB> __host__ __device__ __forceinline__ int z_blocks(int nxh, int 
   return ny * z_main_blocks<WB>(nxh) + (ny + WB - 1) / WB;
 }
 
-template <typename T, int N, int WB>
+template <typename T, int N, int N1_, int WB>
 __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work, cpx<T>* __restrict__ uhat, ZGeom g,
                                                        const cpx<T>* __restrict__ twz,
                                                        const double* __restrict__ symx,
                                                        const double* __restrict__ symy,
                                                        const double* __restrict__ symz) {
   using C = cpx<T>;
-  constexpr int N1 = fftk::Split<N>::N1, N2 = fftk::Split<N>::N2;
+  constexpr int N1 = N1_, N2 = N / N1_;
+  static_assert(N1 * N2 == N && N1 <= 16 && N2 <= 16, "four-step split");
   constexpr int NL = 3 * WB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* A = reinterpret_cast<C*>(smem_raw);  // element t of line (c, w) at t*NL + c*WB + w

@@ -171,6 +171,15 @@ class Selm:
             self._L.selm_destroy(self._h)  # leaves its batch first
             self._h = None
 
+    def tune(self, knob: int, value: int) -> None:
+        """Set a tuning knob of the fused forms (TUNE_FFT_SPLIT, TUNE_Z_BLOCKS)."""
+        check(self._L.selm_tune_set(self._h, int(knob), int(value)))
+
+    def tuned(self, knob: int) -> int:
+        v = C.c_int()
+        check(self._L.selm_tune_get(self._h, int(knob), C.byref(v)))
+        return int(v.value)
+
     def device_bytes(self) -> int:
         """Device memory this simulation holds (selm_device_bytes)."""
         n = C.c_ulonglong()
@@ -227,6 +236,16 @@ class Selm:
         n = C.c_long()
         check(self._L.selm_profile_read(self._h, name.encode(), C.byref(ms), C.byref(n)))
         return float(ms.value), int(n.value)
+
+
+TUNE_FFT_SPLIT = 1
+TUNE_Z_BLOCKS = 2
+
+
+def tune_default(grid: int, precision: int, knob: int, value: int) -> None:
+    """Value of a knob for fused-form simulations created later with this cubic
+    grid size and precision (selm_tune_default)."""
+    check(_lib.load().selm_tune_default(int(grid), int(precision), int(knob), int(value)))
 
 
 class Batch:
