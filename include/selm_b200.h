@@ -203,6 +203,23 @@ int selm_tune_set(selm_sim* s, int knob, int value);
 int selm_tune_get(selm_sim* s, int knob, int* value);
 int selm_tune_default(int grid, int precision, int knob, int value);
 
+/* ---- trajectory output: DCD as written by LAMMPS' "dump ... dcd" ----
+ * The reference's cases dump positions through LAMMPS
+ * (cuda/SELM_Lagrangian_LAMMPS.cu:125-127 runs LAMMPS' output; the case
+ * scripts hold "dump 1 all dcd N file").  Header, title, atom count, then per
+ * frame the unit cell and X, Y, Z as float32; the header's frame count and
+ * last step are kept current. */
+typedef struct selm_dcd selm_dcd;
+int selm_dcd_open(const char* path, int natoms, double dt, int first_step, int interval, const double box_len[3],
+                  selm_dcd** out);
+/* the same for a simulation: its monomer count, timestep, box, and its step as the first */
+int selm_dcd_open_sim(const char* path, selm_sim* s, int interval, selm_dcd** out);
+int selm_dcd_write(selm_dcd* d, const double* x /* host [natoms][3] */);
+int selm_dcd_write_sim(selm_dcd* d, selm_sim* s); /* the simulation's current positions */
+int selm_dcd_close(selm_dcd* d);
+/* the case directory's "dump ID group dcd N file": N (0 if none) and the file */
+int selm_case_dump(selm_sim* s, int* every, char* file, int len);
+
 /* kernels this library has launched since it was loaded (all simulations) */
 unsigned long long selm_kernel_launches(void);
 

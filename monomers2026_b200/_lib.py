@@ -22,6 +22,7 @@ EXPORTED = [
     "selm_batch_create", "selm_batch_add", "selm_batch_remove", "selm_batch_step", "selm_batch_size",
     "selm_batch_get_stream", "selm_batch_synchronize", "selm_batch_destroy", "selm_device_bytes",
     "selm_tune_set", "selm_tune_get", "selm_tune_default",
+    "selm_dcd_open", "selm_dcd_open_sim", "selm_dcd_write", "selm_dcd_write_sim", "selm_dcd_close", "selm_case_dump",
 ]
 
 SELM_OK = 0
@@ -104,6 +105,12 @@ def load():
     L.selm_tune_set.argtypes = [vp, C.c_int, C.c_int]
     L.selm_tune_get.argtypes = [vp, C.c_int, ip]
     L.selm_tune_default.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
+    L.selm_dcd_open.argtypes = [C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_int, dp, C.POINTER(vp)]
+    L.selm_dcd_open_sim.argtypes = [C.c_char_p, vp, C.c_int, C.POINTER(vp)]
+    L.selm_dcd_write.argtypes = [vp, dp]
+    L.selm_dcd_write_sim.argtypes = [vp, vp]
+    L.selm_dcd_close.argtypes = [vp]
+    L.selm_case_dump.argtypes = [vp, ip, C.c_char_p, C.c_int]
     L.selm_last_error.restype = C.c_char_p
     L.selm_version.restype = C.c_char_p
     _lib = L

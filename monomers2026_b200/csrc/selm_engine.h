@@ -55,6 +55,8 @@ struct selm_sim {
   std::vector<double> hx, hv, hf;
   uint64_t step = 0;
   int case_nsteps = 0;  // nsteps of Model.SELM when created from a case directory
+  int dump_every = 0;   // the case's "dump ... dcd N file" (0: none)
+  std::string dump_file;
   bool initialized = false;
   FusedState* fz = nullptr;
   // profiling

@@ -9,7 +9,8 @@
 // timestep, mass, bond_style/bond_coeff (harmonic, fene), angle_style/
 // angle_coeff (harmonic), pair_style/pair_coeff (lj/cut), special_bonds,
 // fix addforce.  Commands that do not change the step (units, boundary, log,
-// neighbor, neigh_modify, thermo*, dump, other fixes) are accepted and ignored.
+// neighbor, neigh_modify, thermo*, other dumps and fixes) are accepted and
+// ignored; a "dump ... dcd N file" is recorded for the selm_b200 executable.
 // Keys the reference does not know (form, integrator, noise_mode) select this
 // library's forms and are ignored by the reference.
 #include <cmath>
@@ -92,6 +93,8 @@ struct Model {
   double rc_global = 0;
   double special[3] = {0, 0, 0};
   double body[3] = {0, 0, 0};
+  int dump_every = 0;  // dump ID group dcd N file
+  std::string dump_file;
   void size_tables() {
     mass.resize(ntypes + 1, 0.0);
     bond_coeff.resize(4 * (size_t)(nbondtypes + 1), 0.0);
@@ -204,6 +207,10 @@ void read_script(Model& m, const std::string& dir, const std::string& path) {
       const std::string p = w.at(1);
       read_data(m, p.size() && p[0] == '/' ? p : dir + "/" + p);
     } else if (c == "timestep") m.dt = std::stod(w.at(1));
+    else if (c == "dump" && w.size() >= 6 && w[3] == "dcd") {
+      m.dump_every = std::stoi(w[4]);
+      m.dump_file = w[5];
+    }
     else if (c == "mass") {
       m.size_tables();
       m.mass.at(std::stoi(w.at(1))) = std::stod(w.at(2));
@@ -345,6 +352,8 @@ int selm_case_create(const char* case_dir, selm_sim** out) {
     return rc;
   }
   s->case_nsteps = nsteps;
+  s->dump_every = m.dump_every;
+  s->dump_file = m.dump_file.empty() ? std::string() : (m.dump_file[0] == '/' ? m.dump_file : dir + "/" + m.dump_file);
   *out = s;
   return SELM_OK;
 }

@@ -3,9 +3,11 @@
 // Model.SELM and Model.LAMMPS_script; runs nsteps and prints the timing.
 // Optional Model.SELM keys saveSkipSimulationData, writeParticalX/V/F append
 // the monomer state to particleX/V/F.dat every saveSkipSimulationData steps in
-// the reference's "%g %g %g" format (cuda/SELM_Lagrangian_LAMMPS.cu:147-175).
+// the reference's "%g %g %g" format (cuda/SELM_Lagrangian_LAMMPS.cu:147-175);
+// a "dump ID group dcd N file" in the LAMMPS script writes a DCD trajectory.
 // The elapsed time printed is the time of the loop (the reference prints the
 // absolute clock, cuda/SELM.cu:92).
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <fstream>
@@ -56,17 +58,33 @@ int main(int argc, char** argv) {
     return 1;
   }
   std::vector<double> x(3 * (size_t)M), v(3 * (size_t)M), f(3 * (size_t)M);
+  // the script's "dump ... dcd N file": a frame at step 0 and every N steps, as LAMMPS writes them
+  int dump_every = 0;
+  char dump_file[4096] = "";
+  selm_case_dump(s, &dump_every, dump_file, sizeof dump_file);
+  selm_dcd* dcd = nullptr;
+  if (dump_every > 0) {
+    if (selm_dcd_open_sim(dump_file, s, dump_every, &dcd) != SELM_OK || selm_dcd_write_sim(dcd, s) != SELM_OK) {
+      fprintf(stderr, "selm_b200: %s\n", selm_last_error());
+      return 1;
+    }
+  }
   selm_synchronize(s);
   const auto t0 = std::chrono::steady_clock::now();
   int done = 0;
   while (done < nsteps) {
     int chunk = nsteps - done;
     if (skip > 0) chunk = skip - (done % skip);
+    if (dump_every > 0) chunk = std::min(chunk, dump_every - (done % dump_every));
     if (selm_step(s, chunk) != SELM_OK) {
       fprintf(stderr, "selm_b200: %s\n", selm_last_error());
       return 1;
     }
     done += chunk;
+    if (dcd && done % dump_every == 0 && selm_dcd_write_sim(dcd, s) != SELM_OK) {
+      fprintf(stderr, "selm_b200: %s\n", selm_last_error());
+      return 1;
+    }
     if (skip > 0 && done % skip == 0 && (wx || wv || wf)) {
       selm_get_particles(s, x.data(), v.data(), f.data());
       if (wf) append("particleF.dat", f);
@@ -80,6 +98,7 @@ int main(int argc, char** argv) {
   selm_status(s, &w);
   printf("\nnGpu: 1\nsteps: %d\nTotal time: %fs\nTotal time average: %fs\nstatus: 0x%x\n", nsteps, el,
          nsteps ? el / nsteps : 0.0, w);
+  selm_dcd_close(dcd);
   selm_destroy(s);
   return 0;
 }
