@@ -220,6 +220,35 @@ int selm_dcd_close(selm_dcd* d);
 /* the case directory's "dump ID group dcd N file": N (0 if none) and the file */
 int selm_case_dump(selm_sim* s, int* every, char* file, int len);
 
+/* ---- on-device analysis: MSD, S(q), kinetic energy per direction ----
+ * Replaces the reference's post-processing of DCD trajectories
+ * (data/src/Diffusion Coefficient/MSD.py:14-91, fit of get_K.py) for runs
+ * that should not write trajectories.  Each selm_analysis_sample records the
+ * simulation's current positions as a float32 frame (what a DCD holds) and
+ * adds, on the simulation's stream and without a host sync:
+ *   MSD   lags l*lag_stride frames, l = 1..nlag: per direction the sum over
+ *         frame pairs (n, n + lag) and monomers of the displacement folded
+ *         once by the box (MSD.py:59-66), squared; MSD(l) = (sum of the three
+ *         directions) / pairs[l]
+ *   S(q)  |sum_j exp(i 2 pi n.x_j / L)|^2 / M for the nq integer triples n
+ *   K_d   sum_j m_j v_jd^2 (equipartition: mean K_d / M = kT per direction)
+ * Sums are deterministic (fixed reduction order).  An analysis belongs to
+ * its simulation; destroying the simulation releases the analysis' device
+ * memory (the handle must still be destroyed). */
+typedef struct selm_analysis selm_analysis;
+int selm_analysis_create(selm_sim* s, int nlag, int lag_stride, int nq, const int* qvec /* [nq][3] */,
+                         selm_analysis** out);
+int selm_analysis_sample(selm_analysis* a);
+/* sums [nlag][3]; pairs [nlag] = (frame pairs) x monomers */
+int selm_analysis_msd(selm_analysis* a, double* sums, long long* pairs);
+/* per wavevector: sum and sum of squares over samples of S(q) */
+int selm_analysis_structure(selm_analysis* a, double* sum, double* sumsq, long long* samples);
+/* per direction: sum and sum of squares over samples of K_d */
+int selm_analysis_kinetic(selm_analysis* a, double* sum, double* sumsq, long long* samples);
+int selm_analysis_reset(selm_analysis* a);
+int selm_analysis_device_bytes(selm_analysis* a, unsigned long long* bytes);
+int selm_analysis_destroy(selm_analysis* a);
+
 /* kernels this library has launched since it was loaded (all simulations) */
 unsigned long long selm_kernel_launches(void);
 

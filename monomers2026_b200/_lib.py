@@ -23,6 +23,8 @@ EXPORTED = [
     "selm_batch_get_stream", "selm_batch_synchronize", "selm_batch_destroy", "selm_device_bytes",
     "selm_tune_set", "selm_tune_get", "selm_tune_default",
     "selm_dcd_open", "selm_dcd_open_sim", "selm_dcd_write", "selm_dcd_write_sim", "selm_dcd_close", "selm_case_dump",
+    "selm_analysis_create", "selm_analysis_sample", "selm_analysis_msd", "selm_analysis_structure",
+    "selm_analysis_kinetic", "selm_analysis_reset", "selm_analysis_device_bytes", "selm_analysis_destroy",
 ]
 
 SELM_OK = 0
@@ -111,6 +113,15 @@ def load():
     L.selm_dcd_write_sim.argtypes = [vp, vp]
     L.selm_dcd_close.argtypes = [vp]
     L.selm_case_dump.argtypes = [vp, ip, C.c_char_p, C.c_int]
+    llp = C.POINTER(C.c_longlong)
+    L.selm_analysis_create.argtypes = [vp, C.c_int, C.c_int, C.c_int, ip, C.POINTER(vp)]
+    L.selm_analysis_sample.argtypes = [vp]
+    L.selm_analysis_msd.argtypes = [vp, dp, llp]
+    L.selm_analysis_structure.argtypes = [vp, dp, dp, llp]
+    L.selm_analysis_kinetic.argtypes = [vp, dp, dp, llp]
+    L.selm_analysis_reset.argtypes = [vp]
+    L.selm_analysis_device_bytes.argtypes = [vp, C.POINTER(C.c_ulonglong)]
+    L.selm_analysis_destroy.argtypes = [vp]
     L.selm_last_error.restype = C.c_char_p
     L.selm_version.restype = C.c_char_p
     _lib = L

@@ -656,6 +656,7 @@ extern "C" int selm_destroy(selm_sim* s) {
     cudaEventDestroy(ev.b);
   }
   if (s->st2) cudaStreamSynchronize(s->st2);
+  analysis_detach_all(s);
   fused_release(s);
   free_all(s->allocs);
   if (s->own_st && s->st) cudaStreamDestroy(s->st);

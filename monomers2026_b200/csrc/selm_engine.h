@@ -18,6 +18,7 @@ struct ProfEvent {
 
 struct FusedState;  // spectral-form buffers (fluid_fused.cu)
 struct selm_batch;  // batched stepping of several simulations (batch.cpp)
+struct selm_analysis;  // on-device statistics (analysis.cu)
 
 struct selm_sim {
   selm_params prm{};
@@ -31,6 +32,7 @@ struct selm_sim {
   std::vector<void*> allocs;
   unsigned long long dev_bytes = 0;  // device bytes allocated for this simulation
   selm_batch* batch = nullptr;       // the batch this simulation steps in, if any
+  std::vector<selm_analysis*> analyses;  // released with the simulation
   // monomers (Lagrangian::d_x/d_v/d_f/d_m, cuda/SELM_Lagrangian.cuh:22-25); x double-buffered
   int M = 0;
   double* x[2] = {nullptr, nullptr};
@@ -93,3 +95,6 @@ void fused_step_taken(selm_sim* s);
 // batches (batch.cpp)
 void batch_mark_dirty(selm_batch* b);
 int batch_detach(selm_sim* s);
+
+// analyses (analysis.cu): free their device memory when the simulation goes
+void analysis_detach_all(selm_sim* s);
