@@ -383,15 +383,43 @@ template <typename T, int N> constexpr int rows_per_chunk_fast() {
   return rp;
 }
 template <typename T, int N> constexpr size_t smem_xy_fast() { return smem_xy_for<T, N>(rows_per_chunk_fast<T, N>()); }
-template <typename T> constexpr int wb_fast() { return sizeof(T) == 8 ? 8 : 16; }
+// grid sizes with compile-time four-step kernels
+#define SELM_FAST_SIZES(X) X(16) X(24) X(30) X(32) X(48) X(64) X(96) X(128)
+
+// Shape of a z-kernel block: WB columns, TPB threads, at least MINB blocks
+// per SM (register bound), and the default cap on blocks per SM (0: none).
+// The 128^3 FP32 kernel takes 19 columns in blocks held to 80 registers:
+// its 438 blocks then all fit at once, three per SM, where 16 columns left a
+// second wave of 76 blocks (measured 64 us against 78; without the register
+// bound the 19-column block takes 96 registers, two per SM, and 81 us).
+template <typename T, int N> struct ZShape {
+  static constexpr bool kWide = sizeof(T) == 4 && N == 128;
+  static constexpr int WB = sizeof(T) == 8 ? 8 : (kWide ? 19 : 16);
+  static constexpr int TPB = 256;
+  static constexpr int MINB = kWide ? 3 : 1;
+  static constexpr int CAP = 3;
+};
+template <typename T, int N> constexpr int wb_fast() { return ZShape<T, N>::WB; }
 // Shared memory of the z kernel: what its lines need, or more when the
 // blocks per SM are capped (the request then leaves room for no more).  By
 // default at most three blocks share an SM: with the 128^3 FP32 kernel, four
 // resident blocks per SM measured slower than three.
 template <typename T, int N> constexpr size_t smem_z_need() {
-  return sizeof(cpx<T>) * ((size_t)N * 3 * wb_fast<T>() + N);
+  return sizeof(cpx<T>) * ((size_t)N * 3 * wb_fast<T, N>() + N);
 }
 constexpr int kZDefaultBlocksPerSm = 3;
+// the default cap of a size (ZShape<T, N>::CAP)
+static int z_default_blocks(int n, int precision) {
+  switch (n) {
+#define SELM_CASE(N) \
+  case N:            \
+    return precision == 32 ? ZShape<float, N>::CAP : ZShape<double, N>::CAP;
+    SELM_FAST_SIZES(SELM_CASE)
+#undef SELM_CASE
+    default:
+      return kZDefaultBlocksPerSm;
+  }
+}
 static size_t smem_z_request(size_t need, int blocks_per_sm) {
   if (blocks_per_sm <= 0) return need;
   const size_t cap = 228 * 1024 / (size_t)(blocks_per_sm + 1) + 1024;  // blocks_per_sm + 1 do not fit
@@ -409,7 +437,8 @@ template <typename T, int N, int N1> static cudaError_t fast_attrs_split() {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xy_fast<T, N>())))
     return e;
   const size_t zmax = smem_z_need<T, N>() > kZSmemMax ? smem_z_need<T, N>() : kZSmemMax;
-  return cudaFuncSetAttribute((const void*)k_z_update_fast<T, N, N1, wb_fast<T>()>,
+  using Z = ZShape<T, N>;
+  return cudaFuncSetAttribute((const void*)k_z_update_fast<T, N, N1, Z::WB, Z::TPB, Z::MINB>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zmax);
 }
 template <typename T, int N> static cudaError_t fast_attrs() {
@@ -423,14 +452,14 @@ static void fast_launch(const T* fp, cpx<T>* work, cpx<T>* uhat, T* u, const ZGe
                         const double* symx, const double* symy, const double* symz, int ny, int nz, cudaStream_t st,
                         selm_sim* s, int z_blocks_per_sm) {
   constexpr int RP = rows_per_chunk_fast<T, N>();
-  constexpr int WB = wb_fast<T>();
+  using Z = ZShape<T, N>;
   const unsigned planes = (unsigned)(3 * nz);
   prof_mark(s, "xy_forward", true);
   k_xy_forward_fast<T, N, N1, RP><<<planes, 512, smem_xy_fast<T, N>(), st>>>(fp, work, tb.wx_f);
   count_launches(1);
   prof_mark(s, "xy_forward", false);
   prof_mark(s, "z_update", true);
-  k_z_update_fast<T, N, N1, WB><<<(unsigned)z_blocks<WB>(zg.nxh, ny), 256,
+  k_z_update_fast<T, N, N1, Z::WB, Z::TPB, Z::MINB><<<(unsigned)z_blocks<Z::WB>(zg.nxh, ny), Z::TPB,
                                   smem_z_request(smem_z_need<T, N>(), z_blocks_per_sm), st>>>(
       work, uhat, zg, tb.wz_f, symx, symy, symz);
   count_launches(1);
@@ -440,8 +469,6 @@ static void fast_launch(const T* fp, cpx<T>* work, cpx<T>* uhat, T* u, const ZGe
   count_launches(1);
   prof_mark(s, "xy_inverse", false);
 }
-
-#define SELM_FAST_SIZES(X) X(16) X(24) X(30) X(32) X(48) X(64) X(96) X(128)
 
 static bool fast_size(int n) {
   switch (n) {
@@ -601,7 +628,7 @@ template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
   if (z->fast) CUF(fast_attrs_for<T>(s->nx));
   const int prec = (int)(8 * sizeof(T));
   z->tune_split = tune_default_of(s->nx, prec, SELM_TUNE_FFT_SPLIT, 0);
-  z->tune_z_blocks = tune_default_of(s->nx, prec, SELM_TUNE_Z_BLOCKS, kZDefaultBlocksPerSm);
+  z->tune_z_blocks = tune_default_of(s->nx, prec, SELM_TUNE_Z_BLOCKS, z_default_blocks(s->nx, prec));
   CUF(cudaFuncSetAttribute((const void*)k_xy_forward<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)z->plan.smem_xy));
   CUF(cudaFuncSetAttribute((const void*)k_xy_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -3,8 +3,8 @@
 // Same arithmetic contract as the generic kernels of fluid_fused.cu:
 //   k_xy_forward_fast : per (component, z) plane, x r2c (two rows per complex
 //                       line) and y FFT -> half spectrum [c][z][y][x];
-//   k_z_update_fast   : per block of Wb z-lines (Wb x modes of one y, or the
-//                       last x mode of Wb y rows): z FFT, the spectral update
+//   k_z_update_fast   : per block of Wb consecutive (x, y) columns of the
+//                       half spectrum, three components each: z FFT, the spectral update
 //                       (viscous factor, projection, Philox noise, zero mode)
 //                       with u_hat read and written in place, inverse z FFT
 //                       with the 1/N normalisation;
@@ -223,18 +223,15 @@ __device__ __forceinline__ void noise_draw_fast(const ZGeom& g, uint64_t step, i
   }
 }
 
-// Column blocks of the z kernel.  A "main" block takes WB consecutive
-// x-columns i0 .. i0+WB-1 (all below the last column nxh-1) of one y-row; a
-// "tail" block takes the last column i = nxh-1 of WB consecutive y-rows, so
-// that no block runs with a single line (for even nx that column is the
-// Nyquist plane).  Blocks 0 .. ny*nmb-1 are main blocks, the rest tail blocks.
-template <int WB> __host__ __device__ __forceinline__ int z_main_blocks(int nxh) { return (nxh - 1 + WB - 1) / WB; }
+// Column blocks of the z kernel: block b takes the WB consecutive columns
+// b*WB .. b*WB+WB-1 of the flattened (y, x) half-spectrum plane (column
+// index j*nxh + i, also its offset within a z plane), the last block fewer.
 template <int WB> __host__ __device__ __forceinline__ int z_blocks(int nxh, int ny) {
-  return ny * z_main_blocks<WB>(nxh) + (ny + WB - 1) / WB;
+  return (nxh * ny + WB - 1) / WB;
 }
 
-template <typename T, int N, int N1_, int WB>
-__global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work, cpx<T>* __restrict__ uhat, ZGeom g,
+template <typename T, int N, int N1_, int WB, int TPB, int MINB>
+__global__ void __launch_bounds__(TPB, MINB) k_z_update_fast(cpx<T>* __restrict__ work, cpx<T>* __restrict__ uhat, ZGeom g,
                                                        const cpx<T>* __restrict__ twz,
                                                        const double* __restrict__ symx,
                                                        const double* __restrict__ symy,
@@ -247,21 +244,9 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
   C* A = reinterpret_cast<C*>(smem_raw);  // element t of line (c, w) at t*NL + c*WB + w
   C* tw = A + N * NL;
   const int nxh = g.nxh, ny = g.ny;
-  const int nmb = z_main_blocks<WB>(nxh);
-  const bool tail = (int)blockIdx.x >= ny * nmb;
-  int i0, j0, wn;
-  if (!tail) {
-    j0 = blockIdx.x / nmb;
-    i0 = (blockIdx.x % nmb) * WB;
-    wn = min(WB, nxh - 1 - i0);
-  } else {
-    i0 = nxh - 1;
-    j0 = (blockIdx.x - ny * nmb) * WB;
-    wn = min(WB, ny - j0);
-  }
+  const long col0 = (long)blockIdx.x * WB;
+  const int wn = (int)min((long)WB, (long)nxh * ny - col0);
   const long plane = (long)ny * nxh;
-  const long cstep = tail ? nxh : 1;  // main lines step in x, tail lines in y
-  const long col0 = (long)j0 * nxh + i0;
   for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twz[t];
   __syncthreads();
   // pass A forward, loading straight from global: thread (line, n2)
@@ -269,7 +254,7 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
     const int l = u % NL, n2 = u / NL;
     const int c = l / WB, w = l % WB;
     const bool ok = w < wn;
-    const long cb = (long)c * N * plane + col0 + w * cstep;
+    const long cb = (long)c * N * plane + col0 + w;
     C v[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; n1++) v[n1] = ok ? work[cb + (N2 * n1 + n2) * plane] : fftk::mk<C>(T(0), T(0));
@@ -300,8 +285,9 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
   for (int u = threadIdx.x; u < WB * N; u += blockDim.x) {
     const int w = u % WB, k = u / WB;
     if (w >= wn) continue;
-    const int i = tail ? i0 : i0 + w, j = tail ? j0 + w : j0;
-    const long gk = (long)k * plane + col0 + w * cstep;
+    const int col = (int)col0 + w;
+    const int j = col / nxh, i = col - j * nxh;
+    const long gk = (long)k * plane + col;
     const int pa = dpos<N1, N2>(k) * NL + w;
     C X[3];
 #pragma unroll
@@ -401,7 +387,7 @@ __global__ void __launch_bounds__(256) k_z_update_fast(cpx<T>* __restrict__ work
     for (int k1 = 0; k1 < N1; k1++) v[k1] = A[(N2 * k1 + n2) * NL + l];
     fftk::dft<N1, +1>(v);
     if (w < wn) {
-      const long cb = (long)c * N * plane + col0 + w * cstep;
+      const long cb = (long)c * N * plane + col0 + w;
 #pragma unroll
       for (int n1 = 0; n1 < N1; n1++) work[cb + (N2 * n1 + n2) * plane] = v[n1];
     }

@@ -208,6 +208,14 @@ def test_fused_fene_wca_vs_oracle(oracle, form, tol):
     _compare_run(oracle, wl, 20, tol)
 
 
+@pytest.mark.parametrize("form,tol", [("fused64", 1e-11), ("fused32", 1e-4)])
+def test_fused_128_cubed_with_noise(oracle, form, tol):
+    """The 128^3 kernels (their own column blocks and block shapes) with the
+    thermal noise on: FENE chains against the FP64 oracle, step by step."""
+    wl = W.config(3, kT=1.0, nchains=8, length=25, grid=128, form=form)
+    _compare_run(oracle, wl, 3, tol)
+
+
 @pytest.mark.parametrize("grid", [30, 48])
 def test_fused64_nonpow2_grid_with_noise(oracle, grid):
     wl = W.config(3, kT=1.0, nchains=3, length=20, grid=grid, form="fused64")
