@@ -708,11 +708,12 @@ constexpr int kMaxSpreadDevices = 64;
 static_assert(kTX == 16, "spread_rot assumes 16-cell rows");
 
 // Accumulator slot of cell (cx, cy, cz) of component d.  The x position is
-// rotated by 4 cz within its 16-cell row, so that the four z-planes of one
-// candidate's component (consecutive cz, same cx and cy), which neighbouring
-// lanes add at the same time, fall on distinct banks.
+// rotated by 4 cz + d within its 16-cell row, so that the twelve (component,
+// z-plane) lanes of one candidate (consecutive cz, nearly the same cx and cy
+// in the three staggered frames), which add at the same time, fall on
+// distinct banks.
 __device__ __forceinline__ int spread_row(int d, int cy, int cz) { return ((d * kTZ + cz) * kTY + cy) * kTX; }
-__device__ __forceinline__ int spread_rot(int cx, int cz) { return (cx + 4 * cz) & (kTX - 1); }
+__device__ __forceinline__ int spread_rot(int cx, int cz, int d) { return (cx + 4 * cz + 1 * d) & (kTX - 1); }
 
 __device__ __forceinline__ long long to_fixed(float v) { return __float2ll_rn(v); }
 __device__ __forceinline__ long long to_fixed(double v) { return __double2ll_rn(v); }
@@ -787,7 +788,7 @@ __device__ __forceinline__ void spread_plane(int p, int d, int kz, const SpreadT
   for (int ix = 0; ix < 4; ix++) {
     int cx = cx0 + ix;
     if (cx >= nx) cx -= nx;
-    xo[ix] = (cx < tl.ex) ? spread_rot(cx, cz) : -1;
+    xo[ix] = (cx < tl.ex) ? spread_rot(cx, cz, d) : -1;
   }
   const int plane = spread_row(d, 0, cz);
 #pragma unroll
@@ -925,7 +926,7 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
     const int cy = row % kTY, cz = (row / kTY) % kTZ, d = row / (kTY * kTZ);
     if (cx < tl.ex && cy < tl.ey && cz < tl.ez) {
       T* dst = fgrid + d * N + ((long)(tl.t0z + cz) * ny + (tl.t0y + cy)) * nx + tl.t0x + cx;
-      const int slot = row * kTX + spread_rot(cx, cz);
+      const int slot = row * kTX + spread_rot(cx, cz, d);
       const long long sum = (tl.mode != kWide) ? (long long)(int)acc_hi[slot] * (1ll << tl.L) + (long long)acc_lo[slot]
                                                : (long long)acc[slot];
       const double add = (double)sum * inv_scale + nan_or_zero;

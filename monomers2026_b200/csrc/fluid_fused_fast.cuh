@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(512) k_xy_forward_fast(const T* __restrict__ i
   using C = cpx<T>;
   constexpr int N1 = N1_, N2 = N / N1_;
   static_assert(N1 * N2 == N && N1 <= 16 && N2 <= 16, "four-step split");
-  constexpr int NH = N / 2 + 1, NLP = NH + 1, RPP = RP + 1;
+  constexpr int NH = N / 2 + 1, NLP = NH, RPP = RP + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* P = reinterpret_cast<C*>(smem_raw);  // [N rows y][NLP] : element y of line m at y*NLP + m
   C* Ax = P + N * NLP;                    // [N][RPP]        : element x of row pair lr at x*RPP + lr
@@ -55,12 +55,12 @@ __global__ void __launch_bounds__(512) k_xy_forward_fast(const T* __restrict__ i
   const T* src = in + plane * (long)N * N;
   C* dst = out + plane * (long)N * NH;
   for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twx[t];
-  for (int y0 = 0; y0 < N; y0 += 2 * RP) {
+  for (int y0 = 0; y0 < N / 2; y0 += RP) {
     __syncthreads();
     for (int idx = threadIdx.x; idx < RP * N; idx += blockDim.x) {
       const int lr = idx / N, x = idx % N;
-      const int ya = y0 + 2 * lr;
-      Ax[x * RPP + lr] = fftk::mk<C>(src[(long)ya * N + x], src[(long)(ya + 1) * N + x]);
+      const int ya = y0 + lr;
+      Ax[x * RPP + lr] = fftk::mk<C>(src[(long)ya * N + x], src[(long)(ya + N / 2) * N + x]);
     }
     __syncthreads();
     for (int u = threadIdx.x; u < RP * N2; u += blockDim.x) pass_a<N1, N2>(Ax, RPP, u % RP, u / RP, tw, false);
@@ -75,15 +75,18 @@ __global__ void __launch_bounds__(512) k_xy_forward_fast(const T* __restrict__ i
       for (int k2 = 0; k2 < N2; k2++) Ax[(N2 * k1 + k2) * RPP + lr] = v[k2];
     }
     __syncthreads();
-    // unpack two real rows: A = (Z[m] + conj Z[-m])/2, B = (Z[m] - conj Z[-m])/(2i)
+    // unpack two real rows: A = (Z[m] + conj Z[-m])/2, B = (Z[m] - conj Z[-m])/(2i).
+    // The pair is rows y and y + N/2, so the lanes of a warp (consecutive
+    // pairs) store to consecutive rows of P, whose odd pitch NH spreads them
+    // over the banks (rows y, y + 1 put them two rows apart: 4-way conflicts)
     for (int u = threadIdx.x; u < RP * NH; u += blockDim.x) {
       const int lr = u % RP, m = u / RP;
       const C z = Ax[dpos<N1, N2>(m) * RPP + lr];
       const C zr = Ax[dpos<N1, N2>((N - m) % N) * RPP + lr];
       const T sx = z.x + zr.x, sy = z.y - zr.y, dx_ = z.x - zr.x, dy = z.y + zr.y;
-      const int ya = y0 + 2 * lr;
+      const int ya = y0 + lr;
       P[ya * NLP + m] = fftk::mk<C>(sx * T(0.5), sy * T(0.5));
-      P[(ya + 1) * NLP + m] = fftk::mk<C>(dy * T(0.5), -dx_ * T(0.5));
+      P[(ya + N / 2) * NLP + m] = fftk::mk<C>(dy * T(0.5), -dx_ * T(0.5));
     }
   }
   __syncthreads();
@@ -106,7 +109,7 @@ __global__ void __launch_bounds__(512) k_xy_inverse_fast(const cpx<T>* __restric
   using C = cpx<T>;
   constexpr int N1 = N1_, N2 = N / N1_;
   static_assert(N1 * N2 == N && N1 <= 16 && N2 <= 16, "four-step split");
-  constexpr int NH = N / 2 + 1, NLP = NH + 1, RPP = RP + 1;
+  constexpr int NH = N / 2 + 1, NLP = NH, RPP = RP + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* P = reinterpret_cast<C*>(smem_raw);
   C* Ax = P + N * NLP;
@@ -136,11 +139,14 @@ __global__ void __launch_bounds__(512) k_xy_inverse_fast(const cpx<T>* __restric
     for (int k2 = 0; k2 < N2; k2++) P[(N2 * k1 + k2) * NLP + m] = v[k2];
   }
   // x c2r, two rows per complex line; imaginary parts of m = 0 and m = N/2 drop out
-  for (int y0 = 0; y0 < N; y0 += 2 * RP) {
+  for (int y0 = 0; y0 < N / 2; y0 += RP) {
     __syncthreads();
+    // thread (m, row pair), m fastest: P is read along a row (consecutive
+    // words) and Ax written at the odd stride RPP (no bank conflicts); row
+    // pairs fastest would read rows 2 N2 apart, all on one bank
     for (int idx = threadIdx.x; idx < RP * N; idx += blockDim.x) {
-      const int lr = idx % RP, m = idx / RP;
-      const int pa = dpos<N1, N2>(y0 + 2 * lr), pb = dpos<N1, N2>(y0 + 2 * lr + 1);
+      const int m = idx % N, lr = idx / N;
+      const int pa = dpos<N1, N2>(y0 + lr), pb = dpos<N1, N2>(y0 + lr + N / 2);
       C a, b;
       if (m < NH) {
         a = P[pa * NLP + m];
@@ -165,12 +171,12 @@ __global__ void __launch_bounds__(512) k_xy_inverse_fast(const cpx<T>* __restric
 #pragma unroll
       for (int n2 = 0; n2 < N2; n2++) v[n2] = Ax[(N2 * k1 + n2) * RPP + lr];
       fftk::dft<N2, +1>(v);
-      const int ya = y0 + 2 * lr;
+      const int ya = y0 + lr;
 #pragma unroll
       for (int k2 = 0; k2 < N2; k2++) {
         const int xx = k1 + N1 * k2;
         dst[(long)ya * N + xx] = v[k2].x;
-        dst[(long)(ya + 1) * N + xx] = v[k2].y;
+        dst[(long)(ya + N / 2) * N + xx] = v[k2].y;
       }
     }
   }
