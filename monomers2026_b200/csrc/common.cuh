@@ -62,16 +62,54 @@ __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1,
   out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
+// The ten round keys of a Philox4x32-10 key (k0 + r W0, k1 + r W1, r = 0..9):
+// the same for every counter of a simulation, so kernels take them as
+// parameters instead of stepping the key in every draw.
+struct PhiloxKeys {
+  uint32_t k[20];
+};
+inline PhiloxKeys philox_keys(uint64_t seed) {
+  PhiloxKeys K{};
+  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  for (int r = 0; r < 10; r++) {
+    K.k[2 * r] = k0;
+    K.k[2 * r + 1] = k1;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return K;
+}
+// philox4x32_10 with the round keys given (the same output)
+__device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, const PhiloxKeys& K,
+                                              uint32_t out[4]) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    c0 = hi1 ^ c1 ^ K.k[2 * r];
+    c1 = lo1;
+    c2 = hi0 ^ c3 ^ K.k[2 * r + 1];
+    c3 = lo0;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
 __device__ __forceinline__ double u01_52(uint32_t a, uint32_t b) {
   const uint64_t x = ((((uint64_t)a) << 32) | b) >> 12;
   return ((double)x + 0.5) * (1.0 / 4503599627370496.0);
 }
 
 // Box-Muller pair from one Philox block
-__device__ __forceinline__ void philox_normal2(uint64_t seed, uint32_t c0, uint32_t c1, uint64_t step,
-                                               double& z0, double& z1) {
+template <typename Key>
+__device__ __forceinline__ void philox_normal2(const Key& key, uint32_t c0, uint32_t c1, uint64_t step, double& z0,
+                                               double& z1) {
   uint32_t o[4];
-  philox4x32_10(c0, c1, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)seed, (uint32_t)(seed >> 32), o);
+  if constexpr (sizeof(Key) == sizeof(PhiloxKeys))
+    philox4x32_10(c0, c1, (uint32_t)step, (uint32_t)(step >> 32), key, o);
+  else
+    philox4x32_10(c0, c1, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)key, (uint32_t)(key >> 32), o);
   const double u1 = u01_52(o[0], o[1]), u2 = u01_52(o[2], o[3]);
   const double r = sqrt(-2.0 * log(u1));
   double s, c;
@@ -82,10 +120,14 @@ __device__ __forceinline__ void philox_normal2(uint64_t seed, uint32_t c0, uint3
 
 // FP32 Box-Muller pair from the same Philox block (24-bit open-interval
 // uniforms); used by the FP32 form, whose noise needs no more than FP32
-__device__ __forceinline__ void philox_normal2_f32(uint64_t seed, uint32_t c0, uint32_t c1, uint64_t step, float& z0,
+template <typename Key>
+__device__ __forceinline__ void philox_normal2_f32(const Key& key, uint32_t c0, uint32_t c1, uint64_t step, float& z0,
                                                    float& z1) {
   uint32_t o[4];
-  philox4x32_10(c0, c1, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)seed, (uint32_t)(seed >> 32), o);
+  if constexpr (sizeof(Key) == sizeof(PhiloxKeys))
+    philox4x32_10(c0, c1, (uint32_t)step, (uint32_t)(step >> 32), key, o);
+  else
+    philox4x32_10(c0, c1, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)key, (uint32_t)(key >> 32), o);
   const float u1 = ((float)(o[0] >> 8) + 0.5f) * (1.0f / 16777216.0f);
   const float u2 = ((float)(o[2] >> 8) + 0.5f) * (1.0f / 16777216.0f);
   // fast intrinsics: u1 in (0, 1] and the angle in [0, 2 pi) keep their

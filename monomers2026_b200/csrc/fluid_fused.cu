@@ -396,7 +396,7 @@ template <typename T, int N> struct ZShape {
   static constexpr bool kWide = sizeof(T) == 4 && N == 128;
   static constexpr int WB = sizeof(T) == 8 ? 8 : (kWide ? 19 : 16);
   static constexpr int TPB = 256;
-  static constexpr int MINB = kWide ? 3 : 1;
+  static constexpr int MINB = kWide ? 3 : (sizeof(T) == 8 ? 2 : 1);
   static constexpr int CAP = 3;
 };
 template <typename T, int N> constexpr int wb_fast() { return ZShape<T, N>::WB; }
@@ -710,6 +710,7 @@ template <typename T> static int fused_fluid_t(selm_sim* s) {
     zg.noise_mode = g.noise_mode;
     zg.seed = g.seed;
     zg.step = g.step;
+    zg.rk = philox_keys(g.seed);
     fast_dispatch<T>(s->nx, z->tune_split, z->tune_z_blocks, (const T*)z->fp, (C*)z->work, (C*)z->uhat, (T*)z->u,
                      zg, tb, z->symx, z->symy, z->symz, s->ny, s->nz, s->st, s);
     CUF(cudaGetLastError());

@@ -191,6 +191,7 @@ struct ZGeom {
   int stochastic, noise_mode;
   uint64_t seed;
   const uint64_t* step;
+  PhiloxKeys rk;  // round keys of seed
 };
 
 // reference noise draw of a half-spectrum mode (cuda/SELM_Kernel.cu:56-79); the
@@ -212,7 +213,7 @@ __device__ __forceinline__ void noise_draw_fast(const ZGeom& g, uint64_t step, i
 #pragma unroll
     for (int d = 0; d < 3; d++) {
       double z0, z1;
-      philox_normal2(g.seed, q, (uint32_t)d, step, z0, z1);
+      philox_normal2(g.rk, q, (uint32_t)d, step, z0, z1);
       out[d] = make_double2(z0 * re, z1 * im);
     }
   } else {
@@ -223,7 +224,7 @@ __device__ __forceinline__ void noise_draw_fast(const ZGeom& g, uint64_t step, i
 #pragma unroll
     for (int d = 0; d < 3; d++) {
       float z0, z1;
-      philox_normal2_f32(g.seed, q, (uint32_t)d, step, z0, z1);
+      philox_normal2_f32(g.rk, q, (uint32_t)d, step, z0, z1);
       out[d] = make_float2(z0 * re, z1 * im);
     }
   }
@@ -253,7 +254,13 @@ __global__ void __launch_bounds__(TPB, MINB) k_z_update_fast(cpx<T>* __restrict_
   const long col0 = (long)blockIdx.x * WB;
   const int wn = (int)min((long)WB, (long)nxh * ny - col0);
   const long plane = (long)ny * nxh;
+  __shared__ int coli[WB], colj[WB];  // (i, j) of the block's columns
   for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twz[t];
+  if (threadIdx.x < wn) {
+    const int col = (int)col0 + threadIdx.x;
+    colj[threadIdx.x] = col / nxh;
+    coli[threadIdx.x] = col - colj[threadIdx.x] * nxh;
+  }
   __syncthreads();
   // pass A forward, loading straight from global: thread (line, n2)
   for (int u = threadIdx.x; u < NL * N2; u += blockDim.x) {
@@ -291,9 +298,8 @@ __global__ void __launch_bounds__(TPB, MINB) k_z_update_fast(cpx<T>* __restrict_
   for (int u = threadIdx.x; u < WB * N; u += blockDim.x) {
     const int w = u % WB, k = u / WB;
     if (w >= wn) continue;
-    const int col = (int)col0 + w;
-    const int j = col / nxh, i = col - j * nxh;
-    const long gk = (long)k * plane + col;
+    const int i = coli[w], j = colj[w];
+    const long gk = (long)k * plane + col0 + w;
     const int pa = dpos<N1, N2>(k) * NL + w;
     C X[3];
 #pragma unroll

@@ -265,11 +265,15 @@ extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const dou
   if (M < 0 || (M > 0 && (!x || !mass))) return selm_fail(SELM_ERR_INVALID, "bad particle arrays");
   if (s->M != 0 && M != s->M) return selm_fail(SELM_ERR_STATE, "monomer count is fixed once set");
   const double L = s->hi - s->lo;
-  for (long i = 0; i < 3L * M; i++)
-    if (!std::isfinite(x[i]) || std::fabs(x[i] - s->lo) > 1e6 * L)
-      return selm_fail(SELM_ERR_INVALID, "non-finite or far out-of-box position");
-  for (int i = 0; i < M; i++)
-    if (!(mass[i] > 0)) return selm_fail(SELM_ERR_INVALID, "masses must be positive");
+  // branch-free reductions (vectorised): this runs on every call of a host round trip
+  {
+    const double lo = s->lo, lim = 1e6 * L;
+    bool bad = false;
+    for (long i = 0; i < 3L * M; i++) bad |= !(std::fabs(x[i] - lo) <= lim);  // NaN and infinities fail too
+    if (bad) return selm_fail(SELM_ERR_INVALID, "non-finite or far out-of-box position");
+    for (int i = 0; i < M; i++) bad |= !(mass[i] > 0);
+    if (bad) return selm_fail(SELM_ERR_INVALID, "masses must be positive");
+  }
   int rc;
   if (s->M == 0 && M > 0) {
     s->M = M;
@@ -293,9 +297,12 @@ extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const dou
   // periodic remap as LAMMPS' Domain::pbc at setup (whole box lengths until x is in [lo, hi));
   // positions already in the box are passed through untouched
   const double* xs = x;
-  bool inside = true;
-  for (long i = 0; i < 3L * M && inside; i++) inside = (x[i] >= s->lo && x[i] < s->hi);
-  if (!inside) {
+  bool outside = false;
+  {
+    const double lo = s->lo, hi = s->hi;
+    for (long i = 0; i < 3L * M; i++) outside |= (x[i] < lo) | (x[i] >= hi);
+  }
+  if (outside) {
     s->hx.assign(x, x + 3L * M);
     for (double& q : s->hx) {
       while (q < s->lo) q += L;
