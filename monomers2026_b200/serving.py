@@ -27,6 +27,7 @@ import numpy as np
 from .selm import Batch, Selm
 
 _FP = {"fused32": 4, "fused64": 8, "plain64": 8}
+SPREAD_TILE = (16, 8, 16)  # cells of a spread tile (kTX, kTY, kTZ of the engine)
 
 
 def estimate_device_bytes(params, natoms: int, pairs: bool = True) -> int:
@@ -41,7 +42,7 @@ def estimate_device_bytes(params, natoms: int, pairs: bool = True) -> int:
         grid = 8 * (3 * N * 4 + N * 3) + 16 * 3 * N2
     else:
         grid = 2 * 3 * N * s + 2 * 3 * N2 * 2 * s
-    tile = (16, 8, 8)
+    tile = SPREAD_TILE
     nb = [-(-n // t) for n, t in zip((nx, ny, nz), tile)]
     tiles = nb[0] * nb[1] * nb[2]
     M = max(1, int(natoms))
