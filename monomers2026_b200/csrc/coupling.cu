@@ -690,8 +690,12 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
 // Each contribution carries the impulse pre-scaled by 2^S, chosen per tile
 // from its largest impulse m and its candidate count n, and is rounded to an
 // integer v:
-//   wide   (FP64 grids, or n > 2^16): one 64-bit accumulator per cell,
-//          n m 2^S < 2^61, a step of about n m 2^-61;
+//   split3 (FP64 grids, n <= 2048): three 32-bit accumulators per cell,
+//          v = hi 2^42 + mid 2^21 + lo with 0 <= lo, mid < 2^21, |v| < 2^(61-k):
+//          the step of the wide form, with native 32-bit atomics (64-bit
+//          shared-memory atomics measured 2.6x slower for the whole spread);
+//   wide   (FP64 grids beyond 2048 candidates, or FP32 beyond 2^16): one
+//          64-bit accumulator per cell, n m 2^S < 2^61, a step of about n m 2^-61;
 //   split  (FP32 grids): two 32-bit accumulators per cell, v = hi 2^L + lo
 //          with 0 <= lo < 2^L, L = 32 - k and k = ceil(log2 n), so that
 //          neither the sum of the lo parts nor that of the hi parts can
@@ -703,7 +707,8 @@ constexpr int kSpreadThreads = 3 * kTY * kTZ;  // also the number of tile rows (
 constexpr int kSpreadCells = 3 * kTZ * kTY * kTX;
 constexpr int kSpreadPad = 32;  // per-lane dummy slots: points outside the tile add there (never read)
 constexpr int kAccWords = kSpreadCells + kSpreadPad;
-constexpr size_t kSpreadSmem = sizeof(unsigned long long) * kAccWords;
+// accumulator words per cell: two 32-bit words (FP32 grids) or three (FP64)
+template <typename T> constexpr size_t spread_smem() { return sizeof(unsigned) * (sizeof(T) == 4 ? 2 : 3) * kAccWords; }
 constexpr int kMaxSpreadDevices = 64;
 static_assert(kTX == 16, "spread_rot assumes 16-cell rows");
 
@@ -730,10 +735,12 @@ struct SpreadTile {
 // Fixed-point modes (v = rounded contribution, n candidates, k = ceil(log2 n)):
 //   kSplit20 (FP32, n <= 4096): lo = v mod 2^20, hi = v >> 20, |v| < 2^(50-k);
 //   kSplitK  (FP32, n <= 65536): lo = v mod 2^(32-k), hi = v >> (32-k), |v| < 2^(62-2k);
-//   kWide    (FP64, or more candidates): one 64-bit word, n |v| < 2^61.
+//   kSplit3  (FP64, n <= 2048): lo = v mod 2^21, mid = (v >> 21) mod 2^21, hi = v >> 42,
+//            |v| < 2^(61-k), so that n 2^21 <= 2^32 and n |hi| <= 2^19;
+//   kWide    (more candidates): one 64-bit word, n |v| < 2^61.
 // In the split modes neither the lo sums (< n 2^L <= 2^32) nor the hi sums
 // (< 2^30 in magnitude) can overflow their 32-bit words.
-enum { kSplit20 = 0, kSplitK = 1, kWide = 2 };
+enum { kSplit20 = 0, kSplitK = 1, kWide = 2, kSplit3 = 3 };
 
 // Add the 16 points of z-plane kz of candidate p's component d (points
 // outside the tile go to the lane's dummy slot, so every lane does the same work).
@@ -743,6 +750,7 @@ __device__ __forceinline__ void spread_plane(int p, int d, int kz, const SpreadT
                                              const WRec<T>* __restrict__ rec, const CouplingArgs& a) {
   unsigned* acc_lo = reinterpret_cast<unsigned*>(acc);
   unsigned* acc_hi = acc_lo + kAccWords;
+  unsigned* acc_top = acc_lo + 2 * kAccWords;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int sx = (d != 0), sy = (d != 1), sz = (d != 2);
   int bx, by, bz;
@@ -808,6 +816,10 @@ __device__ __forceinline__ void spread_plane(int p, int d, int kz, const SpreadT
       } else if (MODE == kSplitK) {
         atomicAdd(acc_lo + slot, (unsigned)v & (0xffffffffu >> tl.k));
         atomicAdd(acc_hi + slot, (unsigned)(v >> tl.L));
+      } else if (MODE == kSplit3) {
+        atomicAdd(acc_lo + slot, (unsigned)v & 0x1fffffu);
+        atomicAdd(acc_hi + slot, (unsigned)(v >> 21) & 0x1fffffu);
+        atomicAdd(acc_top + slot, (unsigned)(v >> 42));
       } else {
         atomicAdd(acc + slot, (unsigned long long)v);
       }
@@ -843,11 +855,12 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
                                                                  const int* __restrict__ offsets,
                                                                  const int* __restrict__ entries, TileSlots ts,
                                                                  const WRec<T>* __restrict__ rec, CouplingArgs a) {
-  extern __shared__ unsigned long long acc[];  // [kAccWords]; the split modes use it as lo[kAccWords], hi[kAccWords]
+  extern __shared__ unsigned long long acc[];  // u64[kAccWords] (wide), or u32 lo[kAccWords], hi[kAccWords] (, top[kAccWords])
   __shared__ double wmax[kSpreadThreads / 32];
   __shared__ int wbad[kSpreadThreads / 32];
   const unsigned* acc_lo = reinterpret_cast<const unsigned*>(acc);
   const unsigned* acc_hi = acc_lo + kAccWords;
+  const unsigned* acc_top = acc_lo + 2 * kAccWords;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int tb = blockIdx.x;
   const int tbx = tb % bs.nb[0], tby = (tb / bs.nb[0]) % bs.nb[1], tbz = tb / (bs.nb[0] * bs.nb[1]);
@@ -873,7 +886,10 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
     ids = entries + s0;
   }
   const int n_ovf = (n > n_prim) ? min(*ts.ovf_count, ts.ovf_cap) : 0;  // only a tile beyond its capacity scans it
-  for (int i = tid; i < kAccWords; i += kSpreadThreads) acc[i] = 0ull;
+  {
+    unsigned* w = reinterpret_cast<unsigned*>(acc);
+    for (int i = tid; i < (sizeof(T) == 4 ? 2 : 3) * kAccWords; i += kSpreadThreads) w[i] = 0u;
+  }
   // fixed-point scale of this tile from its largest impulse component
   double m = 0.0;
   int bad = 0;
@@ -904,17 +920,22 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
     bad |= wbad[w];
   }
   tl.k = (n > 1) ? 32 - __clz(n - 1) : 1;  // ceil(log2 n)
-  tl.mode = (sizeof(T) != 4 || tl.k > 16) ? kWide : (tl.k <= 12) ? kSplit20 : kSplitK;
+  if (sizeof(T) == 4) tl.mode = (tl.k > 16) ? kWide : (tl.k <= 12) ? kSplit20 : kSplitK;
+  else tl.mode = (tl.k <= 11) ? kSplit3 : kWide;
   tl.L = (tl.mode == kSplit20) ? 20 : 32 - tl.k;
   int em = 0;
   if (m > 0.0 && !bad) frexp(tl.mode == kWide ? m * (double)n : m, &em);  // m (or n m) < 2^em
-  const int bits = (tl.mode == kSplit20) ? 50 - tl.k : (tl.mode == kSplitK) ? 62 - 2 * tl.k : 61;
+  const int bits = (tl.mode == kSplit20) ? 50 - tl.k
+                   : (tl.mode == kSplitK) ? 62 - 2 * tl.k
+                   : (tl.mode == kSplit3) ? 61 - tl.k
+                                          : 61;
   const int S = max(-1000, min(1000, bits - em));
   tl.scale = ldexp(1.0, S);
   const double inv_scale = ldexp(1.0, -S);
   if (!bad) {
     if (tl.mode == kSplit20) spread_candidates<kSplit20, T>(ids, n_prim, n_ovf, ts, tb, tl, acc, x_old, tf, rec, a);
     else if (tl.mode == kSplitK) spread_candidates<kSplitK, T>(ids, n_prim, n_ovf, ts, tb, tl, acc, x_old, tf, rec, a);
+    else if (tl.mode == kSplit3) spread_candidates<kSplit3, T>(ids, n_prim, n_ovf, ts, tb, tl, acc, x_old, tf, rec, a);
     else spread_candidates<kWide, T>(ids, n_prim, n_ovf, ts, tb, tl, acc, x_old, tf, rec, a);
   }
   __syncthreads();
@@ -927,8 +948,11 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
     if (cx < tl.ex && cy < tl.ey && cz < tl.ez) {
       T* dst = fgrid + d * N + ((long)(tl.t0z + cz) * ny + (tl.t0y + cy)) * nx + tl.t0x + cx;
       const int slot = row * kTX + spread_rot(cx, cz, d);
-      const long long sum = (tl.mode != kWide) ? (long long)(int)acc_hi[slot] * (1ll << tl.L) + (long long)acc_lo[slot]
-                                               : (long long)acc[slot];
+      const long long sum =
+          (tl.mode == kSplit3) ? (long long)(int)acc_top[slot] * (1ll << 42) + (long long)acc_hi[slot] * (1ll << 21) +
+                                     (long long)acc_lo[slot]
+          : (tl.mode != kWide) ? (long long)(int)acc_hi[slot] * (1ll << tl.L) + (long long)acc_lo[slot]
+                               : (long long)acc[slot];
       const double add = (double)sum * inv_scale + nan_or_zero;
       *dst = accumulate ? (T)((double)*dst + add) : (T)add;
     }
@@ -991,7 +1015,7 @@ cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const 
   if (bs.mode != 2 || bs.tile[0] != kTX || bs.tile[1] != kTY || bs.tile[2] != kTZ) return cudaErrorInvalidValue;
   cudaError_t e = spread_prepare_attributes();
   if (e != cudaSuccess) return e;
-  k_spread_tiles<T><<<ntiles, kSpreadThreads, kSpreadSmem, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets,
+  k_spread_tiles<T><<<ntiles, kSpreadThreads, spread_smem<T>(), st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, offsets,
                                                                   sorted, TileSlots{}, rec, a);
   count_launches(1);
   return cudaGetLastError();
@@ -1009,7 +1033,7 @@ cudaError_t spread_slots(T* fgrid, bool accumulate, const double* x_old, const d
     return cudaErrorInvalidValue;
   cudaError_t e = spread_prepare_attributes();
   if (e != cudaSuccess) return e;
-  k_spread_tiles<T><<<ntiles, kSpreadThreads, kSpreadSmem, st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, nullptr,
+  k_spread_tiles<T><<<ntiles, kSpreadThreads, spread_smem<T>(), st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, nullptr,
                                                                   nullptr, ts, rec, a);
   count_launches(1);
   return cudaGetLastError();
@@ -1025,7 +1049,7 @@ template cudaError_t interp_update<double>(const double*, const double*, double*
 template cudaError_t interp_update<float>(const float*, const double*, double*, double*, double*, const double*,
                                           double*, const int*, WRec<float>*, const CouplingArgs&, uint32_t*,
                                           cudaStream_t, const TileSlots*);
-// The tile accumulators (about 50 KB) exceed the default 48 KB of dynamic
+// The tile accumulators (49 KB in FP32, 74 KB in FP64) exceed the default 48 KB of dynamic
 // shared memory: raise the limit once per device (the first call on a device
 // does it; make that call before any stream capture).
 cudaError_t spread_prepare_attributes() {
@@ -1037,10 +1061,10 @@ cudaError_t spread_prepare_attributes() {
   std::lock_guard<std::mutex> lk(mu);
   if (dev >= 0 && dev < kMaxSpreadDevices && done[dev]) return cudaSuccess;
   if ((e = cudaFuncSetAttribute((const void*)k_spread_tiles<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kSpreadSmem)) != cudaSuccess)
+                                (int)spread_smem<float>())) != cudaSuccess)
     return e;
   if ((e = cudaFuncSetAttribute((const void*)k_spread_tiles<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kSpreadSmem)) != cudaSuccess)
+                                (int)spread_smem<double>())) != cudaSuccess)
     return e;
   if (dev >= 0 && dev < kMaxSpreadDevices) done[dev] = true;
   return cudaSuccess;
