@@ -1,14 +1,19 @@
-// batch.cpp - many independent simulations stepped by one graph launch.
+// batch.cpp - many independent simulations stepped together by graph launches.
 //
 // A batch holds simulations of the fused forms (any grid size and monomer
 // count, each with its own parameters and Philox seed).  Each simulation's
-// step is already captured as a CUDA graph (one per parity of its
-// double-buffered positions); the batch adds those graphs as independent
-// child nodes of one graph, so one cudaGraphLaunch per step runs every
-// member's kernels, and the graph executor overlaps the members on the GPU.
-// Every launch flips every member's parity, so the batch alternates between
-// two instantiated graphs; both are rebuilt when a member joins or leaves, or
-// when a member's own graphs are invalidated (new topology, new callback).
+// step is captured once as a CUDA graph (one per parity of its
+// double-buffered positions).  The members are spread over up to kGroups
+// groups; a group adds its members' graphs as independent child nodes of one
+// graph, so a step is one cudaGraphLaunch per group, forked from the batch's
+// stream onto the group streams and joined back, and the graph executor
+// overlaps the members on the GPU.  Every launch flips its members' parity,
+// so a group alternates between two instantiated graphs; a group's graphs
+// are rebuilt when one of its members joins or leaves, or when a member's
+// own graphs are invalidated (new topology, new callback).  Rebuilding one
+// group instead of the whole batch keeps the host work of an admission to
+// about 1/kGroups of the batch: the steps right after an admission are the
+// slow ones of a serving loop.
 //
 // Members run on the batch's stream while they belong to it (their own
 // stream is restored when they leave), so reads of a member (selm_get_particles,
@@ -23,60 +28,85 @@
 #include "../../include/selm_b200.h"
 #include "selm_engine.h"
 
+namespace {
+constexpr int kGroups = 8;
+}
+
 struct selm_batch {
   struct Member {
     selm_sim* s;
     cudaStream_t st;  // the member's own stream, restored when it leaves
     bool own_st;
+    int group;
+  };
+  struct Group {
+    cudaStream_t st = nullptr;
+    cudaEvent_t join = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};  // phase 0: members at their current parity; 1: flipped
+    unsigned long long kernels[2] = {0, 0};
+    bool dirty = true;
+    int phase = 0;
+    int size = 0;
   };
   std::vector<Member> members;
+  Group groups[kGroups];
   cudaStream_t st = nullptr;
   bool own_st = false;
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};  // phase 0: members at their current parity; 1: flipped
-  unsigned long long kernels[2] = {0, 0};
-  bool dirty = true;
-  int phase = 0;
+  cudaEvent_t fork = nullptr;
 };
 
-void batch_mark_dirty(selm_batch* b) { b->dirty = true; }
+// the graphs of member s changed: rebuild its group
+void batch_mark_dirty(selm_batch* b, selm_sim* s) {
+  for (auto& m : b->members)
+    if (m.s == s) b->groups[m.group].dirty = true;
+}
 
-static void drop_graphs(selm_batch* b) {
+static void drop_graphs(selm_batch::Group& g) {
   for (int q = 0; q < 2; q++) {
-    if (b->exec[q]) cudaGraphExecDestroy(b->exec[q]);
-    b->exec[q] = nullptr;
-    b->kernels[q] = 0;
+    if (g.exec[q]) cudaGraphExecDestroy(g.exec[q]);
+    g.exec[q] = nullptr;
+    g.kernels[q] = 0;
   }
 }
 
-static int rebuild(selm_batch* b) {
-  drop_graphs(b);
+static int rebuild(selm_batch* b, int gi) {
+  selm_batch::Group& G = b->groups[gi];
+  drop_graphs(G);
+  G.phase = 0;
+  G.dirty = false;
+  if (G.size == 0) return SELM_OK;
   for (int q = 0; q < 2; q++) {
     cudaGraph_t g = nullptr;
     if (cudaGraphCreate(&g, 0) != cudaSuccess) return selm_fail(SELM_ERR_CUDA, "cudaGraphCreate");
     unsigned long long k = 0;
     for (auto& m : b->members) {
+      if (m.group != gi) continue;
       cudaGraph_t child = nullptr;
       unsigned long long kc = 0;
       const int rc = fused_step_graph(m.s, m.s->cx ^ q, &child, &kc);
       if (rc) {
         cudaGraphDestroy(g);
+        G.dirty = true;
         return rc;
       }
       cudaGraphNode_t node;
       const cudaError_t e = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, child);
       if (e != cudaSuccess) {
         cudaGraphDestroy(g);
+        G.dirty = true;
         return selm_fail(SELM_ERR_CUDA, std::string("cudaGraphAddChildGraphNode: ") + cudaGetErrorString(e));
       }
       k += kc;
     }
-    const cudaError_t ei = cudaGraphInstantiate(&b->exec[q], g, 0);
+    const cudaError_t ei = cudaGraphInstantiate(&G.exec[q], g, 0);
     cudaGraphDestroy(g);
-    if (ei != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(ei));
-    b->kernels[q] = k;
+    if (ei != cudaSuccess) {
+      G.exec[q] = nullptr;
+      G.dirty = true;
+      return selm_fail(SELM_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(ei));
+    }
+    G.kernels[q] = k;
   }
-  b->phase = 0;
-  b->dirty = false;
   return SELM_OK;
 }
 
@@ -93,19 +123,36 @@ int batch_detach(selm_sim* s) {
   return selm_batch_remove(b, s);
 }
 
+static void release(selm_batch* b) {
+  for (auto& g : b->groups) {
+    drop_graphs(g);
+    if (g.join) cudaEventDestroy(g.join);
+    if (g.st) cudaStreamDestroy(g.st);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->own_st && b->st) cudaStreamDestroy(b->st);
+  delete b;
+}
+
 extern "C" int selm_batch_create(void* stream, selm_batch** out) {
   if (!out) return selm_fail(SELM_ERR_INVALID, "out is NULL");
   *out = nullptr;
   selm_batch* b = new selm_batch();
+  cudaError_t e = cudaSuccess;
   if (stream) {
     b->st = static_cast<cudaStream_t>(stream);
   } else {
-    const cudaError_t e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-      delete b;
-      return selm_fail(SELM_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
-    }
-    b->own_st = true;
+    e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+    b->own_st = (e == cudaSuccess);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  for (auto& g : b->groups) {
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming);
+  }
+  if (e != cudaSuccess) {
+    release(b);
+    return selm_fail(SELM_ERR_CUDA, std::string("selm_batch_create: ") + cudaGetErrorString(e));
   }
   *out = b;
   return SELM_OK;
@@ -120,12 +167,17 @@ extern "C" int selm_batch_add(selm_batch* b, selm_sim* s) {
   if (s->prof) return selm_fail(SELM_ERR_STATE, "profiling needs single steps");
   cudaError_t e = cudaStreamSynchronize(s->st);
   if (e != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
-  b->members.push_back({s, s->st, s->own_st});
+  // the group with the fewest members (the lowest index among equals)
+  int gi = 0;
+  for (int i = 1; i < kGroups; i++)
+    if (b->groups[i].size < b->groups[gi].size) gi = i;
+  b->members.push_back({s, s->st, s->own_st, gi});
+  b->groups[gi].size++;
+  b->groups[gi].dirty = true;
   s->st = b->st;
   s->own_st = false;
   s->batch = b;
   fused_invalidate_graphs(s);  // a member's step is captured on one stream
-  b->dirty = true;
   return SELM_OK;
 }
 
@@ -134,10 +186,12 @@ extern "C" int selm_batch_remove(selm_batch* b, selm_sim* s) {
   auto it = std::find_if(b->members.begin(), b->members.end(), [&](const selm_batch::Member& m) { return m.s == s; });
   if (it == b->members.end()) return selm_fail(SELM_ERR_INVALID, "the simulation is not in this batch");
   const cudaError_t e = cudaStreamSynchronize(b->st);
+  const int gi = it->group;
   restore(*it);
-  fused_invalidate_graphs(s);  // alone again: the step with the side stream
   b->members.erase(it);
-  b->dirty = true;
+  b->groups[gi].size--;
+  b->groups[gi].dirty = true;
+  fused_invalidate_graphs(s);  // alone again: the step with the side stream
   if (e != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
   return SELM_OK;
 }
@@ -147,15 +201,32 @@ extern "C" int selm_batch_step(selm_batch* b, int nsteps) {
   if (nsteps < 0) return selm_fail(SELM_ERR_INVALID, "nsteps < 0");
   if (b->members.empty() || nsteps == 0) return SELM_OK;
   for (int i = 0; i < nsteps; i++) {
-    if (b->dirty) {
-      const int rc = rebuild(b);
-      if (rc) return rc;
+    int active = 0;
+    for (int gi = 0; gi < kGroups; gi++) {
+      selm_batch::Group& G = b->groups[gi];
+      if (G.dirty) {
+        const int rc = rebuild(b, gi);
+        if (rc) return rc;
+      }
+      active += (G.size > 0);
     }
-    const cudaError_t e = cudaGraphLaunch(b->exec[b->phase], b->st);
+    cudaError_t e = cudaEventRecord(b->fork, b->st);
+    unsigned long long k = 0;
+    for (auto& G : b->groups) {
+      if (G.size == 0 || e != cudaSuccess) continue;
+      // one active group runs on the batch's stream itself
+      cudaStream_t gs = (active == 1) ? b->st : G.st;
+      if (gs != b->st) e = cudaStreamWaitEvent(gs, b->fork, 0);
+      if (e == cudaSuccess) e = cudaGraphLaunch(G.exec[G.phase], gs);
+      if (e == cudaSuccess && gs != b->st) e = cudaEventRecord(G.join, gs);
+      if (e == cudaSuccess && gs != b->st) e = cudaStreamWaitEvent(b->st, G.join, 0);
+      k += G.kernels[G.phase];
+    }
     if (e != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
-    selm::count_launches((unsigned)b->kernels[b->phase]);
+    selm::count_launches((unsigned)k);
     for (auto& m : b->members) fused_step_taken(m.s);
-    b->phase ^= 1;
+    for (auto& G : b->groups)
+      if (G.size > 0) G.phase ^= 1;
   }
   return SELM_OK;
 }
@@ -179,9 +250,7 @@ extern "C" int selm_batch_destroy(selm_batch* b) {
     fused_invalidate_graphs(m.s);
   }
   b->members.clear();
-  drop_graphs(b);
-  if (b->own_st) cudaStreamDestroy(b->st);
-  delete b;
+  release(b);
   return SELM_OK;
 }
 

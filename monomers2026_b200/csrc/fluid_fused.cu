@@ -849,14 +849,16 @@ void fused_invalidate_graphs(selm_sim* s) {
     s->fz->gexec[q] = nullptr;
     s->fz->graph[q] = nullptr;
   }
-  if (s->batch) batch_mark_dirty(s->batch);
+  if (s->batch) batch_mark_dirty(s->batch, s);
 }
 
-// Capture the step of parity par (x[par] -> x[par ^ 1]) once: the graph is
-// kept (a batch adds it as a child graph) and instantiated for single steps.
+// Capture the step of parity par (x[par] -> x[par ^ 1]) once; the graph is
+// kept (a batch adds it as a child graph).  It is instantiated only when the
+// simulation steps alone (fused_instantiate): a batch member needs the graph
+// only, which keeps a member's admission to a capture.
 static int fused_capture(selm_sim* s, int par) {
   FusedState* z = s->fz;
-  if (z->gexec[par]) return SELM_OK;
+  if (z->graph[par]) return SELM_OK;
   const int saved = s->cx;
   if (s->M > 0) s->cx = par;
   const unsigned long long l0 = launches_total();
@@ -876,13 +878,21 @@ static int fused_capture(selm_sim* s, int par) {
     return rc;
   }
   if (ec != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
-  const cudaError_t ei = cudaGraphInstantiate(&z->gexec[par], g, 0);
-  if (ei != cudaSuccess) {
-    cudaGraphDestroy(g);
-    return selm_fail(SELM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
-  }
   z->graph[par] = g;
   z->graph_kernels[par] = k;
+  return SELM_OK;
+}
+
+static int fused_instantiate(selm_sim* s, int par) {
+  FusedState* z = s->fz;
+  if (z->gexec[par]) return SELM_OK;
+  const int rc = fused_capture(s, par);
+  if (rc) return rc;
+  const cudaError_t ei = cudaGraphInstantiate(&z->gexec[par], z->graph[par], 0);
+  if (ei != cudaSuccess) {
+    z->gexec[par] = nullptr;
+    return selm_fail(SELM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+  }
   return SELM_OK;
 }
 
@@ -908,7 +918,7 @@ int fused_step(selm_sim* s) {
   const bool graph = !s->cb && !s->prof;
   const int par = (s->M > 0) ? s->cx : 0;
   if (graph) {
-    const int rc = fused_capture(s, par);
+    const int rc = fused_instantiate(s, par);
     if (rc) return rc;
     count_launches((unsigned)z->graph_kernels[par]);
     CUF(cudaGraphLaunch(z->gexec[par], s->st));

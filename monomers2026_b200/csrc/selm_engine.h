@@ -93,7 +93,7 @@ int fused_step_graph(selm_sim* s, int par, cudaGraph_t* graph, unsigned long lon
 void fused_step_taken(selm_sim* s);
 
 // batches (batch.cpp)
-void batch_mark_dirty(selm_batch* b);
+void batch_mark_dirty(selm_batch* b, selm_sim* s);  // member s has new graphs
 int batch_detach(selm_sim* s);
 
 // analyses (analysis.cu): free their device memory when the simulation goes
