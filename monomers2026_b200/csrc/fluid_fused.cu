@@ -371,7 +371,8 @@ template <typename T> static FusedPlan plan_for(int nx, int ny, int nz) {
 // N/2 (halving from N/2) at which two blocks share an SM, else the largest
 // at which one block fits.
 template <typename T, int N> constexpr size_t smem_xy_for(int rp) {
-  return sizeof(cpx<T>) * ((size_t)N * (N / 2 + 1) + (size_t)N * (rp + 1) + N);
+  // plane P, x-pass rows Ax (padded by up to 16 slots in the inverse), twiddles
+  return sizeof(cpx<T>) * ((size_t)N * (N / 2 + 1) + (size_t)N * (rp + 1) + 16 + N);
 }
 template <typename T, int N> constexpr int rows_per_chunk_fast() {
   constexpr size_t kSm = 227 * 1024;

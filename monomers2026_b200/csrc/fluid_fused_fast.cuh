@@ -19,11 +19,13 @@ namespace selm {
 
 // ---------------------------------------------------------------- helpers
 template <int N1, int N2, typename C>
-__device__ __forceinline__ void pass_a(C* s, int stride, int l, int n2, const C* tw, bool inverse_twiddle) {
-  // in place: reads x[N2 n1 + n2], writes Y at N2 k1 + n2
+__device__ __forceinline__ void pass_a(C* s, int stride, int l, int n2, const C* tw, bool inverse_twiddle,
+                                       int gpad = 0) {
+  // in place: reads x[N2 n1 + n2], writes Y at N2 k1 + n2; element x of line l
+  // at x stride + (x / N2) gpad + l
   C v[N1];
 #pragma unroll
-  for (int n1 = 0; n1 < N1; n1++) v[n1] = s[(N2 * n1 + n2) * stride + l];
+  for (int n1 = 0; n1 < N1; n1++) v[n1] = s[(N2 * n1 + n2) * stride + n1 * gpad + l];
   if (!inverse_twiddle) fftk::dft<N1, -1>(v);
   else fftk::dft<N1, +1>(v);
 #pragma unroll
@@ -33,7 +35,7 @@ __device__ __forceinline__ void pass_a(C* s, int stride, int l, int n2, const C*
     v[k1] = cmul(v[k1], w);
   }
 #pragma unroll
-  for (int k1 = 0; k1 < N1; k1++) s[(N2 * k1 + n2) * stride + l] = v[k1];
+  for (int k1 = 0; k1 < N1; k1++) s[(N2 * k1 + n2) * stride + k1 * gpad + l] = v[k1];
 }
 
 // position of natural index k after pass A + pass B (in place): N2 (k mod N1) + k / N1
@@ -113,7 +115,10 @@ __global__ void __launch_bounds__(512) k_xy_inverse_fast(const cpx<T>* __restric
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* P = reinterpret_cast<C*>(smem_raw);
   C* Ax = P + N * NLP;
-  C* tw = Ax + N * RPP;
+  // Ax: element x of row pair lr at x RPP + x / N2 + lr.  The slot added every
+  // N2 rows makes the x pass B, whose lanes read rows N2 apart, hit distinct
+  // banks (N2 RPP alone is a multiple of 8 words)
+  C* tw = Ax + N * RPP + N1;
   const long plane = blockIdx.x;
   const C* src = in + plane * (long)N * NH;
   T* dst = out + plane * (long)N * N;
@@ -160,16 +165,16 @@ __global__ void __launch_bounds__(512) k_xy_inverse_fast(const cpx<T>* __restric
         a.y = T(0);
         b.y = T(0);
       }
-      Ax[m * RPP + lr] = fftk::mk<C>(a.x - b.y, a.y + b.x);
+      Ax[m * RPP + m / N2 + lr] = fftk::mk<C>(a.x - b.y, a.y + b.x);
     }
     __syncthreads();
-    for (int u = threadIdx.x; u < RP * N2; u += blockDim.x) pass_a<N1, N2>(Ax, RPP, u % RP, u / RP, tw, true);
+    for (int u = threadIdx.x; u < RP * N2; u += blockDim.x) pass_a<N1, N2>(Ax, RPP, u % RP, u / RP, tw, true, 1);
     __syncthreads();
     for (int u = threadIdx.x; u < RP * N1; u += blockDim.x) {
       const int k1 = u % N1, lr = u / N1;
       C v[N2];
 #pragma unroll
-      for (int n2 = 0; n2 < N2; n2++) v[n2] = Ax[(N2 * k1 + n2) * RPP + lr];
+      for (int n2 = 0; n2 < N2; n2++) v[n2] = Ax[(N2 * k1 + n2) * RPP + k1 + lr];
       fftk::dft<N2, +1>(v);
       const int ya = y0 + lr;
 #pragma unroll
