@@ -713,12 +713,13 @@ constexpr int kMaxSpreadDevices = 64;
 static_assert(kTX == 16, "spread_rot assumes 16-cell rows");
 
 // Accumulator slot of cell (cx, cy, cz) of component d.  The x position is
-// rotated by 4 cz + d within its 16-cell row, so that the twelve (component,
-// z-plane) lanes of one candidate (consecutive cz, nearly the same cx and cy
-// in the three staggered frames), which add at the same time, fall on
-// distinct banks.
+// rotated by 4 cz + 3 d within its 16-cell row, so that the twelve
+// (component, z-plane) lanes of one candidate, which add at the same time,
+// fall on twelve distinct banks whatever the half-cell shifts between the
+// three staggered frames (x and y bases differing by 0 or 1; a rotation of
+// 4 cz + d collides for a quarter of the shift patterns).
 __device__ __forceinline__ int spread_row(int d, int cy, int cz) { return ((d * kTZ + cz) * kTY + cy) * kTX; }
-__device__ __forceinline__ int spread_rot(int cx, int cz, int d) { return (cx + 4 * cz + 1 * d) & (kTX - 1); }
+__device__ __forceinline__ int spread_rot(int cx, int cz, int d) { return (cx + 4 * cz + 3 * d) & (kTX - 1); }
 
 __device__ __forceinline__ long long to_fixed(float v) { return __float2ll_rn(v); }
 __device__ __forceinline__ long long to_fixed(double v) { return __double2ll_rn(v); }
