@@ -192,8 +192,9 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
-    def make(form):
+    def make(form, integrator="inertial"):
         wl.params.form = form
+        wl.params.integrator = integrator
         sim = Selm(wl.params, wl.x, wl.mass, topology=wl.topology)
         sim.set_stream(stream.cuda_stream)
         sim.initial()
@@ -309,6 +310,14 @@ def run_ours(args, rank, world, local_rank):
             forms[form] = world * N * k2 / (reduce_max(sum(per2)) / 1e3)
             log(f"form {form}: {sum(per2) / k2:.3f} ms/step")
             s2.final()
+        # the overdamped (quasi-steady) integrator on the same workload and form
+        s2 = make(args.form, "quasi_steady")
+        k2 = max(5, args.steps // 2)
+        per2, _ = timed(s2, k2, max(3, args.warmup // 2))
+        forms[f"{args.form}_quasi_steady"] = world * N * k2 / (reduce_max(sum(per2)) / 1e3)
+        log(f"form {args.form} quasi-steady: {sum(per2) / k2:.3f} ms/step")
+        s2.final()
+        wl.params.integrator = "inertial"
     forms[args.form] = value
 
     # ---- roofline of the dominant kernel
