@@ -388,7 +388,9 @@ __device__ __forceinline__ T stencil_gather(const T* __restrict__ ud, const int 
         const T* row = ud + (zoff + wrapi(base[1] + j, a.ny)) * a.nx;
 #pragma unroll
         for (int m = 0; m < NV; m++) {
-          const Vec q = __ldg(reinterpret_cast<const Vec*>(row + vs[m]));
+          // the last chunk holds stencil points only when the window is not chunk-aligned
+          Vec q{};
+          if (m < NV - 1 || off > 0) q = __ldg(reinterpret_cast<const Vec*>(row + vs[m]));
           const T* e = reinterpret_cast<const T*>(&q);
 #pragma unroll
           for (int t = 0; t < V; t++) val += e[t] * (dj * wsel[m * V + t]);
