@@ -68,10 +68,18 @@ __global__ void k_nl_scatter(const int* __restrict__ cellof, int M, const int* _
 }
 
 // thread per member slot q (so a warp covers neighbouring cells): partners of
-// i = members[q] within rl from the 27 cells, inserted in index order
-__global__ void k_nl_build(const double* __restrict__ x, ForceTopo t, int nc, const int* __restrict__ offsets,
-                           const int* __restrict__ members, NeighborList nl, uint32_t* err,
-                           const int* __restrict__ flag) {
+// i = members[q] within rl from the 27 cells, inserted in index order.  With
+// a list capacity up to kNlSmemCap the sorted list is built in shared memory
+// (entry k of thread t at k * blockDim + t) and written out once: an insertion
+// shifts entries, and in global memory (stride M) every shift was a dependent
+// round trip.
+constexpr int kNlBuildThreads = 128;
+constexpr int kNlSmemCap = 64;
+__global__ void __launch_bounds__(kNlBuildThreads) k_nl_build(const double* __restrict__ x, ForceTopo t, int nc,
+                                                              const int* __restrict__ offsets,
+                                                              const int* __restrict__ members, NeighborList nl,
+                                                              uint32_t* err, const int* __restrict__ flag) {
+  extern __shared__ int nl_sbuf[];
   if (*flag == 0) return;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= t.M) return;
@@ -79,7 +87,10 @@ __global__ void k_nl_build(const double* __restrict__ x, ForceTopo t, int nc, co
   const int i = members[q];
   const double L = t.hi - t.lo;
   const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
-  int* out = nl.idx + i;  // entry k at out[k * M]
+  const bool in_smem = nl.cap <= kNlSmemCap;
+  // entry k at out[k * stride]
+  int* out = in_smem ? nl_sbuf + threadIdx.x : nl.idx + i;
+  const long stride = in_smem ? (long)blockDim.x : (long)M;
   int n = 0;
   bool over = false;
   auto scan = [&](int q0, int q1) {
@@ -96,18 +107,19 @@ __global__ void k_nl_build(const double* __restrict__ x, ForceTopo t, int nc, co
           cls = (w == nl.wtab[1]) ? 1 : (w == nl.wtab[2]) ? 2 : 3;
           break;
         }
-      if (nl.wtab[cls] == 0.0) continue;
+      const double wc = (cls == 0) ? nl.wtab[0] : (cls == 1) ? nl.wtab[1] : (cls == 2) ? nl.wtab[2] : nl.wtab[3];
+      if (wc == 0.0) continue;
       if (n == nl.cap) {
         over = true;
         continue;
       }
       // insertion by partner index
       int k = n;
-      while (k > 0 && (out[(long)(k - 1) * M] & 0x3fffffff) > j) {
-        out[(long)k * M] = out[(long)(k - 1) * M];
+      while (k > 0 && (out[(k - 1) * stride] & 0x3fffffff) > j) {
+        out[k * stride] = out[(k - 1) * stride];
         k--;
       }
-      out[(long)k * M] = (int)((unsigned)j | ((unsigned)cls << 30));
+      out[k * stride] = (int)((unsigned)j | ((unsigned)cls << 30));
       n++;
     }
   };
@@ -133,6 +145,8 @@ __global__ void k_nl_build(const double* __restrict__ x, ForceTopo t, int nc, co
       }
     }
   }
+  if (in_smem)
+    for (int k = 0; k < n; k++) nl.idx[i + (long)k * M] = out[k * stride];
   nl.cnt[i] = n;
   nl.xb[3 * i] = xi;
   nl.xb[3 * i + 1] = yi;
@@ -156,7 +170,9 @@ cudaError_t neighbor_update(const double* x, const ForceTopo& t, const BinSpec& 
   if (e != cudaSuccess) return e;
   k_nl_scatter<<<g, 256, 0, st>>>(bb.bucket_of, M, bb.offsets, bb.counts, bb.sorted, nl.flag);
   count_launches(1);
-  k_nl_build<<<(unsigned)((M + 127) / 128), 128, 0, st>>>(x, t, nc, bb.offsets, bb.sorted, nl, err, nl.flag);
+  const size_t smem = (nl.cap <= kNlSmemCap) ? sizeof(int) * kNlBuildThreads * nl.cap : 0;
+  k_nl_build<<<(unsigned)((M + kNlBuildThreads - 1) / kNlBuildThreads), kNlBuildThreads, smem, st>>>(
+      x, t, nc, bb.offsets, bb.sorted, nl, err, nl.flag);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -241,7 +257,8 @@ __global__ void __launch_bounds__(128) k_forces(const double* __restrict__ x, do
       const double* pc = t.pair_coeff + 3 * (ti * nt1 + t.type[j]);
       if (rsq >= pc[2] * pc[2] || rsq <= 0.0) continue;
       const double r2i = 1.0 / rsq, s2 = pc[1] * pc[1] * r2i, s6 = s2 * s2 * s2;
-      const double fp = nl.wtab[cls] * 24.0 * pc[0] * s6 * (2.0 * s6 - 1.0) * r2i;
+      const double wc = (cls == 0) ? nl.wtab[0] : (cls == 1) ? nl.wtab[1] : (cls == 2) ? nl.wtab[2] : nl.wtab[3];
+      const double fp = wc * 24.0 * pc[0] * s6 * (2.0 * s6 - 1.0) * r2i;
       px += dx * fp;
       py += dy * fp;
       pz += dz * fp;
