@@ -1,7 +1,7 @@
 """Batched stepping (selm_batch_*) on a B200.
 
-A member of a batch runs its own captured step graph as a child of the
-batch's graph, with its own buffers and Philox counters, so its state after
+A member of a batch runs its own captured step graph as a child of its
+group's graph, with its own buffers and Philox counters, so its state after
 any number of batch steps must equal, bit for bit, the state of the same
 simulation stepped alone; members joining and leaving between steps
 (continuous batching) must not change that.
@@ -72,6 +72,37 @@ def test_continuous_batching_join_and_leave():
     sim["a"].run(2)
     ref["a"].run(2)
     assert _same(_state(ref["a"]), _state(sim["a"]))
+    b.final()
+
+
+def test_groups_shared_by_several_members():
+    """More members than groups (eight): groups hold two members each; a
+    member leaving a shared group and members joining at odd steps (other
+    position parities) rebuild only their groups, and every member still
+    equals its solo run bit for bit."""
+    mk = lambda seed: _sim(W.replica(16 if seed % 2 else 24, 1 + seed % 3, 10, 1.0, seed))
+    seeds = list(range(60, 73))  # 13 members
+    ref = {k: mk(k) for k in seeds}
+    sim = {k: mk(k) for k in seeds}
+    b = Batch()
+    for k in seeds[:10]:
+        b.add(sim[k])
+    b.run(3)
+    b.remove(sim[seeds[8]])  # shares a group with seeds[0]
+    b.add(sim[seeds[10]])
+    b.run(2)
+    b.add(sim[seeds[11]])
+    b.add(sim[seeds[12]])
+    b.run(4)
+    assert len(b) == 12
+    done = {k: 9 for k in seeds[:10]}
+    done[seeds[8]] = 3
+    done[seeds[10]] = 6
+    done[seeds[11]] = done[seeds[12]] = 4
+    for k in seeds:
+        ref[k].run(done[k])
+        assert sim[k].nstep == done[k]
+        assert _same(_state(ref[k]), _state(sim[k])), k
     b.final()
 
 
