@@ -6,6 +6,7 @@
 // calls those files make are provided.  FFTs and forces come from the
 // oracle's restatement (selm_oracle.c); RanMars restates the published
 // Marsaglia-Zaman RANMAR generator with a polar Box-Muller normal.
+#include <algorithm>
 #include <sys/time.h>
 
 #include <cmath>
@@ -124,14 +125,19 @@ void fftw_execute(const fftw_plan p) {
         }
     return;
   }
-  for (int d = 0; d < H; d++) {
+  // the reference runs these in place (input and output share the buffer):
+  // every field's input is gathered before any output is written
+  std::vector<double> tca(2 * nc * H);
+  for (int d = 0; d < H; d++)
     for (int k = 0; k < n0; k++)
       for (int j = 0; j < n1; j++)
         for (int i = 0; i < nh; i++) {
           const size_t t = ((size_t)k * n1 + j) * nh + i, s = (((size_t)j * n0 + k) * nh + i) * H + d;
-          tc[2 * t] = p->cbuf[2 * s];
-          tc[2 * t + 1] = p->cbuf[2 * s + 1];
+          tca[2 * (d * nc + t)] = p->cbuf[2 * s];
+          tca[2 * (d * nc + t) + 1] = p->cbuf[2 * s + 1];
         }
+  for (int d = 0; d < H; d++) {
+    std::copy(tca.begin() + 2 * d * nc, tca.begin() + 2 * (d + 1) * nc, tc.begin());
     orc_fft3_c2r(n2, n1, n0, tc.data(), tr.data());
     for (int k = 0; k < n0; k++)
       for (int j = 0; j < n1; j++)

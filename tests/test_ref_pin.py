@@ -4,7 +4,8 @@ oracle/_ref/libselm_ref.so is the reference's mpi/SELM.cpp,
 SELM_Eulerian_Period.cpp and SELM_Lagrangian_LAMMPS.cpp compiled unchanged
 (oracle/ref.mk) against single-rank MPI / FFTW-MPI / LAMMPS shims.  At kT = 0
 the oracle restatement must reproduce it bit for bit, step by step, on inputs
-written as a reference case directory (Model.SELM, LAMMPS script and data).
+written as a reference case directory (Model.SELM, LAMMPS script and data);
+at kT > 0 (different random streams) their statistics must agree.
 """
 import numpy as np
 import pytest
@@ -45,14 +46,31 @@ def test_oracle_is_bit_exact_with_reference_cpu_code(oracle, case):
         assert np.array_equal(f, o.f) and np.array_equal(u, o.u)
 
 
-def test_reference_kT_positive_runs_with_its_own_rng(oracle):
-    # kT > 0 draws from RanMars (reference) vs Philox (oracle): only statistics compare.
+def test_reference_noise_matches_oracle_statistically(oracle):
+    """kT > 0: the reference draws RanMars normals and the oracle Philox ones,
+    so only statistics compare.  From rest, after six steps, the RMS of each
+    fluid-velocity component (32^3 cells) agrees within 3% (measured: 1.008,
+    1.014, 0.998), and the monomers' velocity RMS within 25% (20 monomers,
+    60 samples; measured 0.90).  An error in the
+    thermal forcing's amplitude or in its three-field inverse transform shows
+    up here as a factor, not a few percent."""
     from monomers2026_b200 import workloads as W
-    wl = W.config(1, kT=1.0, grid=16)
-    r = refdriver.ReferenceRun(wl, nsteps=5)
-    r.step(5)
-    x, v, f, u = r.state()
-    assert np.isfinite(u).all() and np.abs(u).max() > 0
+    wl = W.config(1, kT=1.0, grid=32)
+    p = wl.params
+    r = refdriver.ReferenceRun(wl, nsteps=6)
+    r.step(6)
+    _, v_ref, _, u_ref = r.state()
+    ff = oracle.ForceField(wl.topology.as_dict(), p.box_lo, p.box_hi)
+    o = oracle.Sim(p.numMeshPtsPerDir, p.box_lo, p.box_hi, p.dt, p.mu, p.rho, p.KB, p.T, wl.x, wl.mass,
+                   stochastic=1, seed=p.SELM_Seed, ff=ff)
+    o.initial()
+    o.step(6)
+    u_o = o.u.reshape(u_ref.shape)
+    assert np.isfinite(u_ref).all()
+    for d in range(3):
+        a, b = u_ref[d].std(), u_o[d].std()
+        assert abs(a / b - 1) < 0.03, (d, a, b)
+    assert abs(v_ref.std() / o.v.std() - 1) < 0.25
 
 
 def _nucleotide_like(nmol=10, seed=4):
