@@ -56,15 +56,21 @@ __global__ void k_nl_count(const double* __restrict__ x, int M, double lo, doubl
   atomicAdd(&counts[c], 1);
 }
 
-// members[] grouped by cell (in no particular order within a cell); counts
-// return to zero, ready for the next rebuild
-__global__ void k_nl_scatter(const int* __restrict__ cellof, int M, const int* __restrict__ offsets,
-                             int* __restrict__ counts, int* __restrict__ members, const int* __restrict__ flag) {
+// members[] grouped by cell (in no particular order within a cell), with
+// their positions beside them (xs, same slots); counts return to zero, ready
+// for the next rebuild
+__global__ void k_nl_scatter(const double* __restrict__ x, const int* __restrict__ cellof, int M,
+                             const int* __restrict__ offsets, int* __restrict__ counts, int* __restrict__ members,
+                             double* __restrict__ xs, const int* __restrict__ flag) {
   if (*flag == 0) return;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= M) return;
   const int c = cellof[p];
-  members[offsets[c] + atomicSub(&counts[c], 1) - 1] = p;
+  const int slot = offsets[c] + atomicSub(&counts[c], 1) - 1;
+  members[slot] = p;
+  xs[3L * slot] = x[3L * p];
+  xs[3L * slot + 1] = x[3L * p + 1];
+  xs[3L * slot + 2] = x[3L * p + 2];
 }
 
 // thread per member slot q (so a warp covers neighbouring cells): partners of
@@ -87,6 +93,16 @@ __global__ void __launch_bounds__(kNlBuildThreads) k_nl_build(const double* __re
   const int i = members[q];
   const double L = t.hi - t.lo;
   const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
+  // i's special partners (bonded neighbours) in registers when there are few
+  constexpr int kSp = 8;
+  const int sp0 = t.sp_off[i], nsp = t.sp_off[i + 1] - sp0;
+  int spj[kSp];
+  double spw[kSp];
+#pragma unroll
+  for (int s = 0; s < kSp; s++) {
+    spj[s] = (s < nsp) ? t.sp_nbr[sp0 + s] : -1;
+    spw[s] = (s < nsp) ? t.sp_w[sp0 + s] : 0.0;
+  }
   const bool in_smem = nl.cap <= kNlSmemCap;
   // entry k at out[k * stride]
   int* out = in_smem ? nl_sbuf + threadIdx.x : nl.idx + i;
@@ -95,18 +111,31 @@ __global__ void __launch_bounds__(kNlBuildThreads) k_nl_build(const double* __re
   bool over = false;
   auto scan = [&](int q0, int q1) {
     for (int r = q0; r < q1; r++) {
+      // index and position come from the same slot: no load waits on another
       const int j = members[r];
+      const double dx = min_img(xi - nl.xs[3L * r], L), dy = min_img(yi - nl.xs[3L * r + 1], L),
+                   dz = min_img(zi - nl.xs[3L * r + 2], L);
       if (j == i) continue;
-      const double dx = min_img(xi - x[3 * j], L), dy = min_img(yi - x[3 * j + 1], L),
-                   dz = min_img(zi - x[3 * j + 2], L);
       if (!(dx * dx + dy * dy + dz * dz < nl.rl2)) continue;
       int cls = 0;
-      for (int s = t.sp_off[i]; s < t.sp_off[i + 1]; s++)
-        if (t.sp_nbr[s] == j) {
-          const double w = t.sp_w[s];
-          cls = (w == nl.wtab[1]) ? 1 : (w == nl.wtab[2]) ? 2 : 3;
-          break;
-        }
+      if (nsp <= kSp) {
+        double w = 0.0;
+        bool hit = false;
+#pragma unroll
+        for (int s = 0; s < kSp; s++)
+          if (!hit && spj[s] == j) {
+            w = spw[s];
+            hit = true;
+          }
+        if (hit) cls = (w == nl.wtab[1]) ? 1 : (w == nl.wtab[2]) ? 2 : 3;
+      } else {
+        for (int s = sp0; s < sp0 + nsp; s++)
+          if (t.sp_nbr[s] == j) {
+            const double w = t.sp_w[s];
+            cls = (w == nl.wtab[1]) ? 1 : (w == nl.wtab[2]) ? 2 : 3;
+            break;
+          }
+      }
       const double wc = (cls == 0) ? nl.wtab[0] : (cls == 1) ? nl.wtab[1] : (cls == 2) ? nl.wtab[2] : nl.wtab[3];
       if (wc == 0.0) continue;
       if (n == nl.cap) {
@@ -168,7 +197,7 @@ cudaError_t neighbor_update(const double* x, const ForceTopo& t, const BinSpec& 
   count_launches(1);
   cudaError_t e = exclusive_scan(bb.counts, bb.offsets, nbk + 1, bb.scan_tmp, st, nl.flag);
   if (e != cudaSuccess) return e;
-  k_nl_scatter<<<g, 256, 0, st>>>(bb.bucket_of, M, bb.offsets, bb.counts, bb.sorted, nl.flag);
+  k_nl_scatter<<<g, 256, 0, st>>>(x, bb.bucket_of, M, bb.offsets, bb.counts, bb.sorted, nl.xs, nl.flag);
   count_launches(1);
   const size_t smem = (nl.cap <= kNlSmemCap) ? sizeof(int) * kNlBuildThreads * nl.cap : 0;
   k_nl_build<<<(unsigned)((M + kNlBuildThreads - 1) / kNlBuildThreads), kNlBuildThreads, smem, st>>>(

@@ -513,6 +513,7 @@ extern "C" int selm_set_topology(selm_sim* s, const selm_topology* tp) {
     if ((rc = dalloc(s, &NL.idx, (size_t)cap * M))) return rc;
     if ((rc = dalloc(s, &NL.cnt, M))) return rc;
     if ((rc = dalloc(s, &NL.xb, 3L * M))) return rc;
+    if ((rc = dalloc(s, &NL.xs, 3L * M))) return rc;
     if ((rc = dalloc(s, &NL.flag, 1))) return rc;
     const int one = 1;  // first build at the next force evaluation
     CU(cudaMemcpy(NL.flag, &one, sizeof(int), cudaMemcpyHostToDevice));

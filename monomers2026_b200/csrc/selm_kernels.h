@@ -159,6 +159,7 @@ struct NeighborList {
   int* idx = nullptr;      // [cap][M]: partner j | weight class << 30
   int* cnt = nullptr;      // [M]
   double* xb = nullptr;    // [3M] positions at the last build
+  double* xs = nullptr;    // [3M] positions in cell order (slot of the cell sort), for the build
   int* flag = nullptr;     // rebuild requested: set by the check, cleared by the forces kernel
   double rl2 = 0.0;        // list radius squared
   double half_skin2 = 0.0; // (skin / 2)^2
