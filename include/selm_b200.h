@@ -112,7 +112,10 @@ int selm_create(const selm_params* params, selm_sim** out);
 /* replaces Selm::Selm() reading Model.SELM + LAMMPS script/data from a case
  * directory (cuda/SELM.cu:20, cuda/SELM_Lagrangian_LAMMPS.cu:21-28) */
 int selm_create_from_files(const char* case_dir, selm_sim** out);
-/* monomer state: replaces Lagrangian_LAMMPS::initial uploads (cuda/SELM_Lagrangian_LAMMPS.cu:71-93) */
+/* monomer state: replaces Lagrangian_LAMMPS::initial uploads (cuda/SELM_Lagrangian_LAMMPS.cu:71-93).
+ * v NULL: zero velocities.  mass NULL: keep the masses of an earlier call (the
+ * first call must give them), as the per-step round trip of a host force
+ * provider moves positions and velocities only. */
 int selm_set_particles(selm_sim* s, int natoms, const double* x, const double* v, const double* mass);
 /* device force field (replaces the per-step LAMMPS round trip) */
 int selm_set_topology(selm_sim* s, const selm_topology* topo);

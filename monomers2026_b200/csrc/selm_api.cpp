@@ -262,8 +262,10 @@ static int alloc_slots(selm_sim* s, const BinSpec& bs, TileSlots& ts, int M) {
 
 extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const double* v, const double* mass) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
-  if (M < 0 || (M > 0 && (!x || !mass))) return selm_fail(SELM_ERR_INVALID, "bad particle arrays");
+  if (M < 0 || (M > 0 && !x)) return selm_fail(SELM_ERR_INVALID, "bad particle arrays");
   if (s->M != 0 && M != s->M) return selm_fail(SELM_ERR_STATE, "monomer count is fixed once set");
+  // masses may be left out once set: a per-step host round trip moves positions and velocities only
+  if (M > 0 && !mass && s->M == 0) return selm_fail(SELM_ERR_INVALID, "the first call must give the masses");
   const double L = s->hi - s->lo;
   // branch-free reductions (vectorised): this runs on every call of a host round trip
   {
@@ -271,7 +273,8 @@ extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const dou
     bool bad = false;
     for (long i = 0; i < 3L * M; i++) bad |= !(std::fabs(x[i] - lo) <= lim);  // NaN and infinities fail too
     if (bad) return selm_fail(SELM_ERR_INVALID, "non-finite or far out-of-box position");
-    for (int i = 0; i < M; i++) bad |= !(mass[i] > 0);
+    if (mass)
+      for (int i = 0; i < M; i++) bad |= !(mass[i] > 0);
     if (bad) return selm_fail(SELM_ERR_INVALID, "masses must be positive");
   }
   int rc;
@@ -317,7 +320,7 @@ extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const dou
   }
   if (v) CU(cudaMemcpyAsync(s->v, v, sizeof(double) * 3 * M, cudaMemcpyHostToDevice, s->st));
   else CU(cudaMemsetAsync(s->v, 0, sizeof(double) * 3 * M, s->st));
-  CU(cudaMemcpyAsync(s->m, mass, sizeof(double) * M, cudaMemcpyHostToDevice, s->st));
+  if (mass) CU(cudaMemcpyAsync(s->m, mass, sizeof(double) * M, cudaMemcpyHostToDevice, s->st));
   CU(cudaStreamSynchronize(s->st));
   return SELM_OK;
 }

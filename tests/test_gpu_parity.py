@@ -270,3 +270,33 @@ def test_graph_replay_equals_direct_launches(form):
     (xa, va, fa), ua = out[0]
     (xb, vb, fb), ub = out[1]
     assert np.array_equal(xa, xb) and np.array_equal(va, vb) and np.array_equal(fa, fb) and np.array_equal(ua, ub)
+
+
+def test_set_particles_keeps_masses_when_left_out():
+    """The per-step host round trip sends positions and velocities only: a
+    call with mass = NULL keeps the masses (the run equals one that never
+    made the call, bit for bit); a first call without masses is refused."""
+    import ctypes as C
+
+    from monomers2026_b200 import _lib
+    L = _lib.load()
+    dp = C.POINTER(C.c_double)
+    wl = W.config(1, kT=1.0, grid=16, form="fused32")
+    wl.mass = np.linspace(0.5, 2.0, len(wl.mass))
+    a = _gpu_sim(wl)
+    b = _gpu_sim(wl)
+    a.run(3)
+    b.run(3)
+    x, v, _ = a.particles()
+    x, v = np.ascontiguousarray(x), np.ascontiguousarray(v)
+    _lib.check(L.selm_set_particles(a._h, a.M, x.ctypes.data_as(dp), v.ctypes.data_as(dp), None))
+    a.run(4)
+    b.run(4)
+    for p, q in zip(a.particles(), b.particles()):
+        assert np.array_equal(p, q)
+    h = C.c_void_p()
+    _lib.check(L.selm_create(C.byref(wl.params.to_c()), C.byref(h)))
+    try:
+        assert L.selm_set_particles(h, a.M, x.ctypes.data_as(dp), v.ctypes.data_as(dp), None) != 0
+    finally:
+        L.selm_destroy(h)
