@@ -831,6 +831,15 @@ void orc_qs_velocity(const double *x, const double *F, int M, int nx, int ny, in
   free(Fh);
 }
 
+/* The conservative forces at the current positions: the force field's, or
+ * zero without one (LAMMPS recomputes f every step in the reference,
+ * cuda/SELM_Lagrangian_LAMMPS.cu:107-130, so with no interactions it is zero;
+ * it must not keep the coupling force the update stored there). */
+static void sim_forces(orc_sim *s) {
+  if (s->ff) orc_forces(s->ff, s->x, s->f);
+  else memset(s->f, 0, sizeof(double) * 3 * (size_t)s->M);
+}
+
 static void sim_step_qs(orc_sim *s) {
   const uint64_t n = ++s->step;
   const double L = s->hi - s->lo;
@@ -843,7 +852,7 @@ static void sim_step_qs(orc_sim *s) {
     else if (tx < s->lo) tx += L;
     s->x[q] = tx;
   }
-  if (s->ff) orc_forces(s->ff, s->x, s->f);
+  sim_forces(s);
 }
 
 void orc_sim_initial(orc_sim *s) {
@@ -851,7 +860,7 @@ void orc_sim_initial(orc_sim *s) {
   s->step = 0;
   remap_initial(s);
   memset(s->u, 0, sizeof(double) * 3 * N);
-  if (s->ff) orc_forces(s->ff, s->x, s->f);
+  sim_forces(s);
   sim_compute_f(s, 1);
 }
 
@@ -875,5 +884,5 @@ void orc_sim_step(orc_sim *s) {
   orc_fluid_run(s->u, s->scratch, s->fgrid, s->nx, s->ny, s->nz, s->dx, s->mu, s->rho, s->dt);
   memcpy(s->u, s->scratch, sizeof(double) * 3 * N);
   sim_compute_f(s, n + 1);
-  if (s->ff) orc_forces(s->ff, s->x, s->f);
+  sim_forces(s);
 }

@@ -300,3 +300,36 @@ def test_set_particles_keeps_masses_when_left_out():
         assert L.selm_set_particles(h, a.M, x.ctypes.data_as(dp), v.ctypes.data_as(dp), None) != 0
     finally:
         L.selm_destroy(h)
+
+
+@pytest.mark.parametrize("form,tol", [("plain64", 1e-11), ("fused64", 1e-11), ("fused32", 1e-4)])
+@pytest.mark.parametrize("M", [0, 1])
+def test_fluid_alone_and_one_monomer_with_noise(oracle, form, tol, M):
+    """Edge cases of the monomer side: no monomers at all (the fluid alone,
+    thermal forcing on) and a single monomer (no pair partners), against the
+    oracle on the same Philox stream."""
+    wl = W.config(1, kT=1.0, grid=16, form=form)
+    p = wl.params
+    x, m = wl.x[:M].copy(), wl.mass[:M].copy()
+    o = oracle.Sim(p.numMeshPtsPerDir, p.box_lo, p.box_hi, p.dt, p.mu, p.rho, p.KB, p.T, x, m, stochastic=1,
+                   seed=p.SELM_Seed)
+    o.initial()
+    g = Selm(p, x, m)
+    g.initial()
+    for _ in range(4):
+        o.step(2)
+        g.run(2)
+        assert rel(g.get_field(0), o.u) < tol
+        if M:
+            xg, vg, _ = g.particles()
+            assert rel(xg, o.x) < tol and rel(vg, o.v) < tol
+    assert g.status() == 0
+
+
+def test_monomer_on_the_upper_box_face(oracle):
+    """A monomer exactly at box_hi is the periodic image of box_lo: the
+    interpolation, spreading and the step give the oracle's results."""
+    wl = _moving(W.config(1, kT=0.0, grid=16, form="fused64"))
+    wl.params.flagStochasticDriving = 0
+    wl.x[0] = [wl.params.box_hi, wl.params.box_lo + 3.0, wl.params.box_hi]
+    _compare_run(oracle, wl, 6, 1e-12)
