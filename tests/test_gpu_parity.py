@@ -333,3 +333,26 @@ def test_monomer_on_the_upper_box_face(oracle):
     wl.params.flagStochasticDriving = 0
     wl.x[0] = [wl.params.box_hi, wl.params.box_lo + 3.0, wl.params.box_hi]
     _compare_run(oracle, wl, 6, 1e-12)
+
+
+def test_neighbour_list_overflow_is_flagged():
+    """More pair partners within reach than a monomer's list holds: the list
+    keeps what fits and the status word reports it (0x20), as the force
+    kernels then miss pairs."""
+    n = 16
+    # a 4x4x4 block at spacing 0.45 sigma: the inner monomers have about 50
+    # partners within cutoff + skin (1.62 sigma), the list holds 40; the
+    # closest pairs stay 0.45 apart, so the forces remain finite
+    g1 = np.arange(4) * 0.45
+    x = 8.0 + np.stack(np.meshgrid(g1, g1, g1, indexing="ij"), -1).reshape(-1, 3)
+    M = len(x)
+    pc = np.zeros((4, 3))
+    pc[3] = (1.0, 1.0, 2 ** (1 / 6))  # type 1 with itself: WCA
+    topo = Topology(types=np.ones(M, np.int32), ntypes=1, pair_style="lj/cut", pair_coeff=pc,
+                    special_lj=(0.0, 0.0, 0.0))
+    p = Params(numMeshPtsPerDir=(n, n, n), box_lo=0.0, box_hi=float(n), rho=1.0, mu=1.0, KB=1.0, T=0.0, dt=1e-6,
+               flagStochasticDriving=0, SELM_Seed=1, form="fused64")
+    g = Selm(p, x, np.ones(M), topology=topo)
+    g.initial()
+    g.run(1)
+    assert g.status() & 0x20

@@ -73,3 +73,25 @@ def test_qs_plain_form_is_refused():
     wl.params.integrator = "quasi_steady"
     with pytest.raises(Exception):
         Selm(wl.params, wl.x, wl.mass, topology=wl.topology)
+
+
+@pytest.mark.parametrize("M", [0, 1])
+def test_qs_fluid_alone_and_one_monomer(oracle, M):
+    """The quasi-steady form with no monomers (the thermal forcing alone) and
+    with one free monomer, against the oracle on the same Philox stream."""
+    wl = W.config(1, kT=1.0, grid=16, form="fused64")
+    p = wl.params
+    p.integrator = "quasi_steady"
+    x, m = wl.x[:M].copy(), wl.mass[:M].copy()
+    o = oracle.Sim(p.numMeshPtsPerDir, p.box_lo, p.box_hi, p.dt, p.mu, p.rho, p.KB, p.T, x, m, stochastic=1,
+                   seed=p.SELM_Seed, integrator=1)
+    o.initial()
+    g = Selm(p, x, m)
+    g.initial()
+    for _ in range(3):
+        o.step(2)
+        g.run(2)
+        assert rel(g.get_field(0), o.u) < 1e-11
+        if M:
+            assert rel(g.particles()[0], o.x) < 1e-11
+    assert g.status() == 0
