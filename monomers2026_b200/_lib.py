@@ -25,6 +25,7 @@ EXPORTED = [
     "selm_dcd_open", "selm_dcd_open_sim", "selm_dcd_write", "selm_dcd_write_sim", "selm_dcd_close", "selm_case_dump",
     "selm_analysis_create", "selm_analysis_sample", "selm_analysis_msd", "selm_analysis_structure",
     "selm_analysis_kinetic", "selm_analysis_reset", "selm_analysis_device_bytes", "selm_analysis_destroy",
+    "selm_get_coupling_impulse",
 ]
 
 SELM_OK = 0
@@ -112,6 +113,7 @@ def load():
     L.selm_dcd_write.argtypes = [vp, dp]
     L.selm_dcd_write_sim.argtypes = [vp, vp]
     L.selm_dcd_close.argtypes = [vp]
+    L.selm_get_coupling_impulse.argtypes = [vp, dp, dp]
     L.selm_case_dump.argtypes = [vp, ip, C.c_char_p, C.c_int]
     llp = C.POINTER(C.c_longlong)
     L.selm_analysis_create.argtypes = [vp, C.c_int, C.c_int, C.c_int, ip, C.POINTER(vp)]

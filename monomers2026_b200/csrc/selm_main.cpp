@@ -2,8 +2,9 @@
 // selm_cuda (cuda/main.cu:5-12).  Run from a case directory holding
 // Model.SELM and Model.LAMMPS_script; runs nsteps and prints the timing.
 // Optional Model.SELM keys saveSkipSimulationData, writeParticalX/V/F append
-// the monomer state to particleX/V/F.dat every saveSkipSimulationData steps in
-// the reference's "%g %g %g" format (cuda/SELM_Lagrangian_LAMMPS.cu:147-175);
+// the monomer state to particleX/V/F.dat every saveSkipSimulationData steps
+// in the reference's "%g %g %g" format
+// (cuda/SELM_Lagrangian_LAMMPS.cu:147-175);
 // a "dump ID group dcd N file" in the LAMMPS script writes a DCD trajectory.
 // The elapsed time printed is the time of the loop (the reference prints the
 // absolute clock, cuda/SELM.cu:92).
@@ -69,15 +70,42 @@ int main(int argc, char** argv) {
       return 1;
     }
   }
+  // particle files as the reference writes them (mpi/SELM_Lagrangian_LAMMPS.cpp:79-82,280-300):
+  // after every saveSkipSimulationData-th step (not at step 0: Selm::initial
+  // writes nothing); F is the force array as the update leaves it,
+  // (t_f + dt f_before) / dt, not the recomputed force
+  const bool files = skip > 0 && (wx || wv || wf);
+  std::vector<double> f_before(3 * (size_t)M), tf(3 * (size_t)M);
+  auto write_files = [&]() {
+    selm_get_particles(s, x.data(), v.data(), f.data());
+    double dt = 0.0;
+    if (wf && selm_get_coupling_impulse(s, tf.data(), &dt) == SELM_OK)
+      for (size_t q = 0; q < f.size(); q++) f[q] = (tf[q] + dt * f_before[q]) / dt;
+    if (wf) append("particleF.dat", f);
+    if (wv) append("particleV.dat", v);
+    if (wx) append("particleX.dat", x);
+  };
+  auto step = [&](int n) {
+    if (n > 0 && selm_step(s, n) != SELM_OK) {
+      fprintf(stderr, "selm_b200: %s\n", selm_last_error());
+      return false;
+    }
+    return true;
+  };
   selm_synchronize(s);
   const auto t0 = std::chrono::steady_clock::now();
   int done = 0;
   while (done < nsteps) {
     int chunk = nsteps - done;
-    if (skip > 0) chunk = skip - (done % skip);
+    if (skip > 0) chunk = std::min(chunk, skip - (done % skip));
     if (dump_every > 0) chunk = std::min(chunk, dump_every - (done % dump_every));
-    if (selm_step(s, chunk) != SELM_OK) {
-      fprintf(stderr, "selm_b200: %s\n", selm_last_error());
+    const bool write = files && (done + chunk) % skip == 0;
+    if (write && wf) {
+      // the force before the last step of the chunk enters the written F
+      if (!step(chunk - 1)) return 1;
+      selm_get_particles(s, nullptr, nullptr, f_before.data());
+      if (!step(1)) return 1;
+    } else if (!step(chunk)) {
       return 1;
     }
     done += chunk;
@@ -85,12 +113,7 @@ int main(int argc, char** argv) {
       fprintf(stderr, "selm_b200: %s\n", selm_last_error());
       return 1;
     }
-    if (skip > 0 && done % skip == 0 && (wx || wv || wf)) {
-      selm_get_particles(s, x.data(), v.data(), f.data());
-      if (wf) append("particleF.dat", f);
-      if (wv) append("particleV.dat", v);
-      if (wx) append("particleX.dat", x);
-    }
+    if (write) write_files();
   }
   selm_synchronize(s);
   const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
