@@ -119,8 +119,11 @@ int main(int argc, char** argv) {
   const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   unsigned int w = 0;
   selm_status(s, &w);
-  printf("\nnGpu: 1\nsteps: %d\nTotal time: %fs\nTotal time average: %fs\nstatus: 0x%x\n", nsteps, el,
-         nsteps ? el / nsteps : 0.0, w);
+  // the reference's lines (cuda/SELM.cu:92-96), then the step count and the status word
+  double dt = 0.0;
+  selm_get_coupling_impulse(s, nullptr, &dt);
+  printf("\ndt: %f\nnGpu: 1\nTotal time: %fs\nTotal time average: %fs\nsteps: %d\nstatus: 0x%x\n", dt, el,
+         nsteps ? el / nsteps : 0.0, nsteps, w);
   selm_dcd_close(dcd);
   selm_destroy(s);
   return 0;
