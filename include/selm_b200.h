@@ -135,8 +135,9 @@ int selm_get_particles(selm_sim* s, double* x, double* v, double* f); /* any may
  * conservative force is added (cuda/SELM_Kernel.cu:302-373).  The reference
  * writes (t_f + dt f_before) / dt to particleF.dat, the force array as the
  * update leaves it, before LAMMPS recomputes it
- * (mpi/SELM_Lagrangian_LAMMPS.cpp:79-82,280-300).  dt may be NULL.  The
- * quasi-steady form has no such impulse (SELM_ERR_STATE). */
+ * (mpi/SELM_Lagrangian_LAMMPS.cpp:79-82,280-300).  dt (the timestep) may be
+ * NULL.  The quasi-steady form has no such impulse (SELM_ERR_STATE, dt still
+ * set). */
 int selm_get_coupling_impulse(selm_sim* s, double* tf, double* dt);
 #define SELM_FIELD_U 0 /* Eulerian::d_u[cur_u] */
 #define SELM_FIELD_F 1 /* Eulerian::d_f (forcing for the next fluid update) */

@@ -700,9 +700,9 @@ extern "C" int selm_get_particles(selm_sim* s, double* x, double* v, double* f) 
 
 extern "C" int selm_get_coupling_impulse(selm_sim* s, double* tf, double* dt) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  if (dt) *dt = s->prm.dt;
   if (s->prm.integrator == SELM_INTEGRATOR_QUASI_STEADY)
     return selm_fail(SELM_ERR_STATE, "the quasi-steady form has no coupling impulse");
-  if (dt) *dt = s->prm.dt;
   if (s->M == 0 || !tf) return SELM_OK;
   CU(cudaMemcpyAsync(tf, s->tf, sizeof(double) * 3 * s->M, cudaMemcpyDeviceToHost, s->st));
   CU(cudaStreamSynchronize(s->st));
