@@ -9,8 +9,9 @@
 // stream onto the group streams and joined back, and the graph executor
 // overlaps the members on the GPU.  Every launch flips its members' parity,
 // so a group alternates between two instantiated graphs; a group's graphs
-// are rebuilt when one of its members joins or leaves, or when a member's
-// own graphs are invalidated (new topology, new callback).  Rebuilding one
+// are rebuilt, one per step as they come due, when one of its members joins
+// or leaves, or when a member's own graphs are invalidated (new topology,
+// new callback).  Rebuilding one
 // group instead of the whole batch keeps the host work of an admission to
 // about 1/kGroups of the batch: the steps right after an admission are the
 // slow ones of a serving loop.
@@ -69,44 +70,39 @@ static void drop_graphs(selm_batch::Group& g) {
   }
 }
 
-static int rebuild(selm_batch* b, int gi) {
+// The graph of phase q of group gi, built when it is about to be launched:
+// each member's step graph at its current parity.  An admission or a
+// retirement drops both phases; they are rebuilt over the next two steps, so
+// no single step pays for both.
+static int build_phase(selm_batch* b, int gi, int q) {
   selm_batch::Group& G = b->groups[gi];
-  drop_graphs(G);
-  G.phase = 0;
-  G.dirty = false;
-  if (G.size == 0) return SELM_OK;
-  for (int q = 0; q < 2; q++) {
-    cudaGraph_t g = nullptr;
-    if (cudaGraphCreate(&g, 0) != cudaSuccess) return selm_fail(SELM_ERR_CUDA, "cudaGraphCreate");
-    unsigned long long k = 0;
-    for (auto& m : b->members) {
-      if (m.group != gi) continue;
-      cudaGraph_t child = nullptr;
-      unsigned long long kc = 0;
-      const int rc = fused_step_graph(m.s, m.s->cx ^ q, &child, &kc);
-      if (rc) {
-        cudaGraphDestroy(g);
-        G.dirty = true;
-        return rc;
-      }
-      cudaGraphNode_t node;
-      const cudaError_t e = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, child);
-      if (e != cudaSuccess) {
-        cudaGraphDestroy(g);
-        G.dirty = true;
-        return selm_fail(SELM_ERR_CUDA, std::string("cudaGraphAddChildGraphNode: ") + cudaGetErrorString(e));
-      }
-      k += kc;
+  cudaGraph_t g = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) return selm_fail(SELM_ERR_CUDA, "cudaGraphCreate");
+  unsigned long long k = 0;
+  for (auto& m : b->members) {
+    if (m.group != gi) continue;
+    cudaGraph_t child = nullptr;
+    unsigned long long kc = 0;
+    const int rc = fused_step_graph(m.s, m.s->cx, &child, &kc);
+    if (rc) {
+      cudaGraphDestroy(g);
+      return rc;
     }
-    const cudaError_t ei = cudaGraphInstantiate(&G.exec[q], g, 0);
-    cudaGraphDestroy(g);
-    if (ei != cudaSuccess) {
-      G.exec[q] = nullptr;
-      G.dirty = true;
-      return selm_fail(SELM_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(ei));
+    cudaGraphNode_t node;
+    const cudaError_t e = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, child);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return selm_fail(SELM_ERR_CUDA, std::string("cudaGraphAddChildGraphNode: ") + cudaGetErrorString(e));
     }
-    G.kernels[q] = k;
+    k += kc;
   }
+  const cudaError_t ei = cudaGraphInstantiate(&G.exec[q], g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    G.exec[q] = nullptr;
+    return selm_fail(SELM_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(ei));
+  }
+  G.kernels[q] = k;
   return SELM_OK;
 }
 
@@ -205,8 +201,16 @@ extern "C" int selm_batch_step(selm_batch* b, int nsteps) {
     for (int gi = 0; gi < kGroups; gi++) {
       selm_batch::Group& G = b->groups[gi];
       if (G.dirty) {
-        const int rc = rebuild(b, gi);
-        if (rc) return rc;
+        drop_graphs(G);
+        G.phase = 0;
+        G.dirty = false;
+      }
+      if (G.size > 0 && !G.exec[G.phase]) {
+        const int rc = build_phase(b, gi, G.phase);
+        if (rc) {
+          G.dirty = true;
+          return rc;
+        }
       }
       active += (G.size > 0);
     }
