@@ -260,6 +260,26 @@ static int alloc_slots(selm_sim* s, const BinSpec& bs, TileSlots& ts, int M) {
   return SELM_OK;
 }
 
+// The checks of every selm_set_particles call, written so that the compiler
+// vectorises them (restrict pointers, integer counts, no early exit): on a
+// per-step host round trip they ran at one element per nanosecond, 0.6 ms
+// for 1e5 monomers, as long as the transfers.
+static void check_positions(const double* __restrict__ x, long n, double lo, double hi, double lim, long* bad,
+                            long* outside) {
+  long b = 0, o = 0;
+  for (long i = 0; i < n; i++) {
+    b += (long)(!(std::fabs(x[i] - lo) <= lim));  // NaN and infinities fail too
+    o += (long)((x[i] < lo) | (x[i] >= hi));
+  }
+  *bad = b;
+  *outside = o;
+}
+static long count_nonpositive(const double* __restrict__ m, long n) {
+  long b = 0;
+  for (long i = 0; i < n; i++) b += (long)(!(m[i] > 0));
+  return b;
+}
+
 extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const double* v, const double* mass) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
   if (M < 0 || (M > 0 && !x)) return selm_fail(SELM_ERR_INVALID, "bad particle arrays");
@@ -267,15 +287,12 @@ extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const dou
   // masses may be left out once set: a per-step host round trip moves positions and velocities only
   if (M > 0 && !mass && s->M == 0) return selm_fail(SELM_ERR_INVALID, "the first call must give the masses");
   const double L = s->hi - s->lo;
-  // branch-free reductions (vectorised): this runs on every call of a host round trip
+  long outside_count = 0;
   {
-    const double lo = s->lo, lim = 1e6 * L;
-    bool bad = false;
-    for (long i = 0; i < 3L * M; i++) bad |= !(std::fabs(x[i] - lo) <= lim);  // NaN and infinities fail too
+    long bad = 0;
+    check_positions(x, 3L * M, s->lo, s->hi, 1e6 * L, &bad, &outside_count);
     if (bad) return selm_fail(SELM_ERR_INVALID, "non-finite or far out-of-box position");
-    if (mass)
-      for (int i = 0; i < M; i++) bad |= !(mass[i] > 0);
-    if (bad) return selm_fail(SELM_ERR_INVALID, "masses must be positive");
+    if (mass && count_nonpositive(mass, M)) return selm_fail(SELM_ERR_INVALID, "masses must be positive");
   }
   int rc;
   if (s->M == 0 && M > 0) {
@@ -300,12 +317,7 @@ extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const dou
   // periodic remap as LAMMPS' Domain::pbc at setup (whole box lengths until x is in [lo, hi));
   // positions already in the box are passed through untouched
   const double* xs = x;
-  bool outside = false;
-  {
-    const double lo = s->lo, hi = s->hi;
-    for (long i = 0; i < 3L * M; i++) outside |= (x[i] < lo) | (x[i] >= hi);
-  }
-  if (outside) {
+  if (outside_count) {
     s->hx.assign(x, x + 3L * M);
     for (double& q : s->hx) {
       while (q < s->lo) q += L;

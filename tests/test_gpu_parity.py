@@ -356,3 +356,32 @@ def test_neighbour_list_overflow_is_flagged():
     g.initial()
     g.run(1)
     assert g.status() & 0x20
+
+
+def test_set_particles_checks_and_remaps():
+    """Non-finite or far positions and non-positive masses are refused before
+    anything reaches the device; positions outside the box are moved by whole
+    box lengths into [lo, hi), as LAMMPS does at setup."""
+    import ctypes as C
+
+    from monomers2026_b200 import _lib
+    L = _lib.load()
+    dp = C.POINTER(C.c_double)
+    wl = W.config(1, kT=0.0, grid=16, form="fused32")
+    g = _gpu_sim(wl)
+    M = g.M
+    x0, v0, _ = g.particles()
+    for bad in (np.nan, np.inf, -np.inf, 1e12):
+        x = np.ascontiguousarray(x0.copy())
+        x[M // 2, 1] = bad
+        assert L.selm_set_particles(g._h, M, x.ctypes.data_as(dp), None, None) == 1  # SELM_ERR_INVALID
+    m = np.ones(M)
+    m[3] = 0.0
+    x = np.ascontiguousarray(x0.copy())
+    assert L.selm_set_particles(g._h, M, x.ctypes.data_as(dp), None, m.ctypes.data_as(dp)) == 1
+    box = wl.params.box_hi - wl.params.box_lo
+    x[0] = [wl.params.box_hi + 0.25, wl.params.box_lo - 0.5, wl.params.box_lo + 3 * box + 0.125]
+    _lib.check(L.selm_set_particles(g._h, M, x.ctypes.data_as(dp), None, None))
+    got = g.particles()[0]
+    assert np.allclose(got[0], [wl.params.box_lo + 0.25, wl.params.box_hi - 0.5, wl.params.box_lo + 0.125])
+    assert np.array_equal(got[1:], x0[1:])
