@@ -295,6 +295,8 @@ def run_ours(args, rank, world, local_rank):
            "d2h_bytes_per_step": M * 72, "steps": ke}
     log(f"e2e: {e2e['value']:.3e} cell-steps/s")
     U = stencil_union(xp, n, p.box_lo, (p.box_hi - p.box_lo) / n)
+    extras = outputs_and_analysis(sim, lib, stream, p.dt)
+    log(f"analysis and output: {extras}")
     sim.final()
     del sim
 
@@ -368,6 +370,7 @@ def run_ours(args, rank, world, local_rank):
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "analysis_and_output": extras,
             "autotune": tuned,
             "batched": batched,
             "serving": serving,
@@ -425,6 +428,43 @@ def batched_and_serving(args):
                     "budget_bytes": 150 * 10**9, "form": "fused32"}
     log(f"serving: {sv['jobs']} jobs, step p99 {sv['step_ms']['p99']:.2f} ms")
     return b, sv
+
+
+def outputs_and_analysis(sim, lib, stream, dt, samples=20, frames=10):
+    """Cost of the on-device analysis (one sample: MSD over 40 lags, S(q) at
+    the 16 shortest wavevectors, K_d) on the device, and of writing DCD frames
+    (read-back plus file write), on the headline simulation."""
+    import ctypes as C
+    import tempfile
+
+    import torch
+
+    from monomers2026_b200 import _lib
+    from monomers2026_b200.analysis import Analysis, wavevectors
+    q = wavevectors(2)[:16]
+    an = Analysis(sim, nlag=40, lag_stride=1, qvec=q)
+    for _ in range(3):
+        an.sample()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(samples):
+        an.sample()
+    b.record(stream)
+    b.synchronize()
+    sample_us = 1000.0 * a.elapsed_time(b) / samples
+    an.close()
+    with tempfile.TemporaryDirectory() as tmp:
+        h = C.c_void_p()
+        _lib.check(lib.selm_dcd_open_sim(os.path.join(tmp, "t.dcd").encode(), sim._h, 1, C.byref(h)))
+        t0 = time.perf_counter()
+        for _ in range(frames):
+            _lib.check(lib.selm_dcd_write_sim(h, sim._h))
+        frame_ms = 1e3 * (time.perf_counter() - t0) / frames
+        _lib.check(lib.selm_dcd_close(h))
+    return {"analysis_sample_us": round(sample_us, 2), "analysis": "MSD 40 lags (ring of 41 float32 frames), "
+            "S(q) at 16 wavevectors, K_d; device time per sample", "dcd_frame_ms": round(frame_ms, 3),
+            "dcd": "one frame of 1e5 monomers: device read-back plus the file write (host)"}
 
 
 def cpu_baseline(wl, budget_s=20.0):
