@@ -162,3 +162,26 @@ def test_reset_and_lags_without_pairs():
     assert np.all(sums == 0) and np.all(pairs == 0)
     a.close()
     s.final()
+
+
+def test_analysis_without_monomers():
+    """A fluid-only simulation: sampling counts, and every sum stays zero."""
+    from monomers2026_b200 import workloads as W
+    from monomers2026_b200.analysis import Analysis, wavevectors
+    from monomers2026_b200.selm import Selm
+    wl = W.config(1, kT=1.0, grid=16, form="fused32")
+    s = Selm(wl.params, wl.x[:0].copy(), wl.mass[:0].copy())
+    s.initial()
+    a = Analysis(s, 3, 1, wavevectors(1))
+    for _ in range(4):
+        s.run(1)
+        a.sample()
+    sums, pairs = a.msd_sums()
+    assert np.all(sums == 0) and np.all(pairs == 0)
+    sq, _, k = a.structure()
+    assert k == 4 and np.all(sq == 0)
+    kd, _, k = a.kinetic()
+    assert k == 4 and np.all(kd == 0)
+    assert s.status() == 0
+    a.close()
+    s.final()
