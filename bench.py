@@ -17,7 +17,9 @@ from pinned host memory, step, read the monomer state back, every step.
 
 ``--impl reference`` times the reference's CPU step (the reference's own
 source built against single-rank shims when available, else the FP64 port in
-oracle/) on the host cores, one rank only.
+oracle/) on all the host's hardware threads: one single-rank instance of the
+same workload per thread, run concurrently, their cell-steps summed over the
+common window (torchrun rank 0 only).
 """
 from __future__ import annotations
 
@@ -490,6 +492,109 @@ def cpu_baseline(wl, budget_s=20.0):
 
 
 # --------------------------------------------------------------------------- reference arm
+# Resident memory of one single-rank reference instance of the 128^3 workload
+# with 1e5 monomers (measured 0.37 GB) plus its interpreter, rounded up.
+REF_INSTANCE_BYTES = 0.75e9
+
+
+def _host_memory_available() -> float:
+    """Bytes this process may still allocate: the smaller of the host's
+    available memory and what its memory cgroup (v2 or v1) leaves."""
+    import psutil
+    avail = float(psutil.virtual_memory().available)
+    for lim, use in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
+                     ("/sys/fs/cgroup/memory/memory.limit_in_bytes", "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
+        try:
+            with open(lim) as f:
+                t = f.read().strip()
+            if t == "max":
+                continue
+            with open(use) as f:
+                avail = min(avail, float(t) - float(f.read().strip()))
+        except (OSError, ValueError):
+            continue
+    return avail
+
+
+def reference_workers(limit: int | None = None) -> int:
+    """Concurrent single-rank instances the host runs: one per usable hardware
+    thread, no more than half the available memory holds."""
+    cpus = len(os.sched_getaffinity(0))
+    by_mem = int(0.5 * _host_memory_available() // REF_INSTANCE_BYTES)
+    n = max(1, min(cpus, by_mem))
+    return min(n, limit) if limit else n
+
+
+def _reference_instance(wl, kind):
+    p = wl.params
+    if kind == "reference":
+        from oracle import refdriver
+        return refdriver.ReferenceRun(wl)
+    from oracle import pyoracle as O
+    ff = O.ForceField(wl.topology.as_dict(), p.box_lo, p.box_hi)
+    run = O.Sim(p.numMeshPtsPerDir, p.box_lo, p.box_hi, p.dt, p.mu, p.rho, p.KB, p.T, wl.x, wl.mass,
+                stochastic=p.flagStochasticDriving, seed=p.SELM_Seed, ff=ff)
+    run.initial()
+    return run
+
+
+def _reference_worker(wl, kind, warmup, steps, barrier, results, i):
+    """One instance in its own process: warm up, wait for all, time `steps`
+    full steps.  Its stdout goes to /dev/null (one JSON line from the parent)."""
+    try:
+        fd = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(fd, 1)
+        run = _reference_instance(wl, kind)
+        for _ in range(warmup):
+            run.step(1)
+        barrier.wait()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            run.step(1)
+        results.put((i, t0, time.perf_counter(), ""))
+    except Exception as e:  # reported by the parent
+        barrier.abort()
+        results.put((i, 0.0, 0.0, f"{type(e).__name__}: {e}"))
+
+
+def time_reference(wl, kind, warmup, steps, workers, timeout_s=1800.0):
+    """Aggregate rate of `workers` concurrent instances of the same workload:
+    (instances x steps x cells) / (last end - first start).  CLOCK_MONOTONIC
+    (perf_counter) is one clock for all processes of the host."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(workers, timeout=timeout_s)
+    results = ctx.Queue()
+    procs = [ctx.Process(target=_reference_worker, args=(wl, kind, warmup, steps, barrier, results, i), daemon=True)
+             for i in range(workers)]
+    for q in procs:
+        q.start()
+    got, err, done = [], [], set()
+    deadline = time.time() + timeout_s
+    while len(done) < workers and not err:
+        try:
+            i, t0, t1, e = results.get(timeout=2.0)
+            done.add(i)
+            (err if e else got).append(e if e else (t0, t1))
+        except Exception:
+            dead = [k for k, q in enumerate(procs) if k not in done and q.exitcode not in (None, 0)]
+            if dead:
+                err.append(f"instance {dead[0]} exited with code {procs[dead[0]].exitcode}")
+            elif time.time() > deadline:
+                err.append("no result before the deadline")
+    if err:
+        barrier.abort()
+    for q in procs:
+        q.join(timeout=30)
+        if q.is_alive():
+            q.kill()
+    if err:
+        raise RuntimeError("reference instance failed: " + err[0])
+    window = max(t1 for _, t1 in got) - min(t0 for t0, _ in got)
+    N = int(np.prod(wl.params.numMeshPtsPerDir))
+    return N * workers * steps / window, window
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -497,42 +602,27 @@ def run_reference(args, rank, world):
     wl = W.config(3)
     p = wl.params
     N = int(np.prod(p.numMeshPtsPerDir))
-    ref = None
     try:
         from oracle import refdriver  # the reference's own CPU source, built under oracle/_ref
-        ref = refdriver.available()
+        kind = "reference" if refdriver.available() else "port"
     except Exception:
-        ref = None
-    if ref:
-        from oracle import refdriver
-        run = refdriver.ReferenceRun(wl)
-        kind = "reference"
-        sample = "full steps of the same workload through the reference's own CPU code (single rank)"
-    else:
-        from oracle import pyoracle as O
-        ff = O.ForceField(wl.topology.as_dict(), p.box_lo, p.box_hi)
-        run = O.Sim(p.numMeshPtsPerDir, p.box_lo, p.box_hi, p.dt, p.mu, p.rho, p.KB, p.T, wl.x, wl.mass,
-                    stochastic=p.flagStochasticDriving, seed=p.SELM_Seed, ff=ff)
-        run.initial()
         kind = "port"
-        sample = "full steps of the same workload (FP64 oracle port, single thread)"
-    for _ in range(args.warmup):
-        run.step(1)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        run.step(1)
-    dt = time.perf_counter() - t0
-    value = N * args.steps / dt
+    what = ("the reference's own CPU code (mpi/ sources, single rank each)" if kind == "reference"
+            else "the FP64 oracle port (single thread each)")
+    workers = reference_workers(args.ref_workers)
+    value, window = time_reference(wl, kind, args.warmup, args.steps, workers)
     out = {
         "impl": "reference",
         "metric": "fluid-cell-steps/s @128^3, 1e5 monomers (FP32 fused form; plain FP64 form beside it)",
         "value": value, "unit": "fluid-cell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": N / value * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded random-walk FENE chains)",
         "config": {"workload": "large single instance: 1000 FENE chains x 100 monomers, L=128, 128^3 grid, "
                                "kT=1, dt=0.005", "grid": p.numMeshPtsPerDir[0], "monomers": len(wl.mass)},
-        "cpu_baseline": {"value": value, "unit": "fluid-cell-steps/s", "cores": 1, "kind": kind,
-                         "sample": f"{args.steps} " + sample},
+        "cpu_baseline": {"value": value, "unit": "fluid-cell-steps/s", "cores": workers, "kind": kind,
+                         "sample": f"{workers} concurrent instances x {args.steps} full steps of the same workload "
+                                   f"through {what}, one per host thread; value = all their cell-steps over "
+                                   f"the {window:.1f} s from the first start to the last end"},
         "e2e": {"value": value, "unit": "fluid-cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -548,6 +638,8 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other forms")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-workers", type=int, default=None,
+                    help="reference arm: cap on concurrent instances (default: one per host thread)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-ensemble and serving runs")
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--no-autotune", action="store_true", help="keep the built-in kernel choices")
