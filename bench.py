@@ -341,7 +341,7 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_batched:
         batched, serving = batched_and_serving(args)
 
-    # ---- CPU baseline (rank 0 at N=1): the FP64 oracle port on a bounded sample
+    # ---- CPU baseline (rank 0 at N=1): the reference's CPU code on every host thread, a bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         log("CPU baseline")
@@ -469,26 +469,20 @@ def outputs_and_analysis(sim, lib, stream, dt, samples=20, frames=10):
             "dcd": "one frame of 1e5 monomers: device read-back plus the file write (host)"}
 
 
-def cpu_baseline(wl, budget_s=20.0):
-    """FP64 oracle port (or the reference's own CPU code when built) on this host, single thread."""
-    from oracle import pyoracle as O
-    p = wl.params
-    ff = O.ForceField(wl.topology.as_dict(), p.box_lo, p.box_hi)
-    sim = O.Sim(p.numMeshPtsPerDir, p.box_lo, p.box_hi, p.dt, p.mu, p.rho, p.KB, p.T, wl.x, wl.mass,
-                stochastic=p.flagStochasticDriving, seed=p.SELM_Seed, ff=ff)
-    sim.initial()
-    sim.step(1)
-    t0 = time.perf_counter()
-    k = 0
-    while True:
-        sim.step(1)
-        k += 1
-        if time.perf_counter() - t0 > budget_s or k >= 50:
-            break
-    dt = time.perf_counter() - t0
-    N = int(np.prod(p.numMeshPtsPerDir))
-    return {"value": N * k / dt, "unit": "fluid-cell-steps/s", "cores": 1, "kind": "port",
-            "sample": f"{k} full steps of the same workload (FP64 oracle port, single thread)"}
+def cpu_baseline(wl, budget_s=15.0):
+    """The reference's own CPU code (oracle/_ref; else the FP64 oracle port)
+    on all the host's hardware threads, one single-rank instance of the same
+    workload per thread, as the reference arm runs it: a bounded sample of
+    about `budget_s` seconds (a step takes about 1 s per instance at 128^3
+    with 1e5 monomers)."""
+    kind = reference_kind()
+    workers = reference_workers()
+    steps = max(2, int(budget_s))
+    value, window = time_reference(wl, kind, 1, steps, workers)
+    what = "the reference's own CPU code" if kind == "reference" else "FP64 oracle port"
+    return {"value": value, "unit": "fluid-cell-steps/s", "cores": workers, "kind": kind,
+            "sample": f"{workers} concurrent single-rank instances x {steps} full steps of the same workload "
+                      f"({what}), {window:.1f} s from the first start to the last end"}
 
 
 # --------------------------------------------------------------------------- reference arm
@@ -523,6 +517,16 @@ def reference_workers(limit: int | None = None) -> int:
     by_mem = int(0.5 * _host_memory_available() // REF_INSTANCE_BYTES)
     n = max(1, min(cpus, by_mem))
     return min(n, limit) if limit else n
+
+
+def reference_kind() -> str:
+    """"reference" when the reference's own CPU source is built under
+    oracle/_ref, else "port" (the FP64 oracle restatement)."""
+    try:
+        from oracle import refdriver
+        return "reference" if refdriver.available() else "port"
+    except Exception:
+        return "port"
 
 
 def _reference_instance(wl, kind):
@@ -602,11 +606,7 @@ def run_reference(args, rank, world):
     wl = W.config(3)
     p = wl.params
     N = int(np.prod(p.numMeshPtsPerDir))
-    try:
-        from oracle import refdriver  # the reference's own CPU source, built under oracle/_ref
-        kind = "reference" if refdriver.available() else "port"
-    except Exception:
-        kind = "port"
+    kind = reference_kind()
     what = ("the reference's own CPU code (mpi/ sources, single rank each)" if kind == "reference"
             else "the FP64 oracle port (single thread each)")
     workers = reference_workers(args.ref_workers)
