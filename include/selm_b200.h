@@ -115,7 +115,12 @@ int selm_create_from_files(const char* case_dir, selm_sim** out);
 /* monomer state: replaces Lagrangian_LAMMPS::initial uploads (cuda/SELM_Lagrangian_LAMMPS.cu:71-93).
  * v NULL: zero velocities.  mass NULL: keep the masses of an earlier call (the
  * first call must give them), as the per-step round trip of a host force
- * provider moves positions and velocities only. */
+ * provider moves positions and velocities only.  A non-finite position, or
+ * one more than 1e6 box lengths away, or a non-positive mass returns
+ * SELM_ERR_INVALID and leaves the monomers as they were; positions outside
+ * the box are moved by whole box lengths into [lo, hi).  After the first call
+ * the positions are checked on the device (staging buffers, 48 bytes per
+ * monomer, allocated by the second call). */
 int selm_set_particles(selm_sim* s, int natoms, const double* x, const double* v, const double* mass);
 /* device force field (replaces the per-step LAMMPS round trip) */
 int selm_set_topology(selm_sim* s, const selm_topology* topo);

@@ -1073,6 +1073,68 @@ cudaError_t spread_prepare_attributes() {
   return cudaSuccess;
 }
 
+// ---------------------------------------------------------------- staged monomer upload
+// Positions staged in device memory are checked there: cnt[0] counts the
+// entries that are non-finite or more than `lim` from lo, cnt[1] those
+// outside [lo, hi).  The commit copies the staged positions (and velocities;
+// zeros without them) into the simulation only when both counts are zero, so
+// a refused upload leaves the state as it was.
+constexpr int kStageThreads = 256;
+constexpr long kStageBlocks = 4 * 148;  // four blocks on each of the B200's 148 SMs
+
+__global__ void __launch_bounds__(kStageThreads) k_stage_check(const double* __restrict__ x, long n, double lo,
+                                                               double hi, double lim,
+                                                               unsigned long long* __restrict__ cnt) {
+  unsigned b = 0, o = 0;
+  for (long i = blockIdx.x * (long)kStageThreads + threadIdx.x; i < n; i += (long)gridDim.x * kStageThreads) {
+    const double q = x[i];
+    b += !(fabs(q - lo) <= lim);  // NaN and infinities fail too
+    o += (q < lo) | (q >= hi);
+  }
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+    b += __shfl_xor_sync(0xffffffffu, b, w);
+    o += __shfl_xor_sync(0xffffffffu, o, w);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (b) atomicAdd(cnt, (unsigned long long)b);
+    if (o) atomicAdd(cnt + 1, (unsigned long long)o);
+  }
+}
+
+__global__ void __launch_bounds__(kStageThreads) k_stage_commit(const double* __restrict__ xin,
+                                                                const double* __restrict__ vin, double* __restrict__ x,
+                                                                double* __restrict__ v, long n,
+                                                                const unsigned long long* __restrict__ cnt) {
+  if (cnt[0] != 0ull || cnt[1] != 0ull) return;
+  for (long i = blockIdx.x * (long)kStageThreads + threadIdx.x; i < n; i += (long)gridDim.x * kStageThreads) {
+    x[i] = xin[i];
+    v[i] = vin ? vin[i] : 0.0;
+  }
+}
+
+static unsigned stage_blocks(long n) {
+  return (unsigned)std::max(1L, std::min(kStageBlocks, (n + kStageThreads - 1) / kStageThreads));
+}
+
+cudaError_t stage_check(const double* xin, long n, double lo, double hi, double lim, unsigned long long* cnt,
+                        cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  if (n == 0) return cudaSuccess;
+  k_stage_check<<<stage_blocks(n), kStageThreads, 0, st>>>(xin, n, lo, hi, lim, cnt);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t stage_commit(const double* xin, const double* vin, double* x, double* v, long n,
+                         const unsigned long long* cnt, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_stage_commit<<<stage_blocks(n), kStageThreads, 0, st>>>(xin, vin, x, v, n, cnt);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 template cudaError_t spread_gather<double>(double*, bool, const double*, const double*, const BinSpec&, const int*,
                                            const int*, const CouplingArgs&, cudaStream_t, const WRec<double>*);
 template cudaError_t spread_gather<float>(float*, bool, const double*, const double*, const BinSpec&, const int*,

@@ -280,19 +280,60 @@ static long count_nonpositive(const double* __restrict__ m, long n) {
   return b;
 }
 
+static int set_particles_host(selm_sim* s, int M, const double* x, const double* v, const double* mass);
+
+// Upload of a simulation that already holds its monomers (the per-step round
+// trip): the positions and velocities go to device staging buffers, checked
+// and committed there (no host pass over them); the rare upload with
+// positions outside the box is redone by the host path, which remaps them.
+static int set_particles_staged(selm_sim* s, int M, const double* x, const double* v, const double* mass) {
+  int rc;
+  const long n = 3L * M;
+  if (!s->xin) {
+    if ((rc = dalloc(s, &s->xin, n)) || (rc = dalloc(s, &s->vin, n)) || (rc = dalloc(s, &s->stage_cnt, 2)))
+      return rc;
+    if (cudaMallocHost((void**)&s->hstage_cnt, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaGetLastError();
+      s->hstage_cnt = nullptr;
+      return selm_fail(SELM_ERR_NOMEM, "cudaMallocHost failed");
+    }
+  }
+  const double L = s->hi - s->lo;
+  CU(cudaMemcpyAsync(s->xin, x, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
+  if (v) CU(cudaMemcpyAsync(s->vin, v, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
+  CU(selm::stage_check(s->xin, n, s->lo, s->hi, 1e6 * L, s->stage_cnt, s->st));
+  CU(selm::stage_commit(s->xin, v ? s->vin : nullptr, s->x[s->cx], s->v, n, s->stage_cnt, s->st));
+  CU(cudaMemcpyAsync(s->hstage_cnt, s->stage_cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  if (s->hstage_cnt[0]) return selm_fail(SELM_ERR_INVALID, "non-finite or far out-of-box position");
+  if (s->hstage_cnt[1]) return set_particles_host(s, M, x, v, mass);
+  if (mass) {
+    CU(cudaMemcpyAsync(s->m, mass, sizeof(double) * M, cudaMemcpyHostToDevice, s->st));
+    CU(cudaStreamSynchronize(s->st));
+  }
+  return SELM_OK;
+}
+
 extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const double* v, const double* mass) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
   if (M < 0 || (M > 0 && !x)) return selm_fail(SELM_ERR_INVALID, "bad particle arrays");
   if (s->M != 0 && M != s->M) return selm_fail(SELM_ERR_STATE, "monomer count is fixed once set");
   // masses may be left out once set: a per-step host round trip moves positions and velocities only
   if (M > 0 && !mass && s->M == 0) return selm_fail(SELM_ERR_INVALID, "the first call must give the masses");
+  if (mass && count_nonpositive(mass, M)) return selm_fail(SELM_ERR_INVALID, "masses must be positive");
+  if (M > 0 && s->M == M) return set_particles_staged(s, M, x, v, mass);
+  return set_particles_host(s, M, x, v, mass);
+}
+
+// First upload (allocates the monomer buffers), or positions outside the box:
+// checked and remapped on the host.
+static int set_particles_host(selm_sim* s, int M, const double* x, const double* v, const double* mass) {
   const double L = s->hi - s->lo;
   long outside_count = 0;
   {
     long bad = 0;
     check_positions(x, 3L * M, s->lo, s->hi, 1e6 * L, &bad, &outside_count);
     if (bad) return selm_fail(SELM_ERR_INVALID, "non-finite or far out-of-box position");
-    if (mass && count_nonpositive(mass, M)) return selm_fail(SELM_ERR_INVALID, "masses must be positive");
   }
   int rc;
   if (s->M == 0 && M > 0) {
@@ -690,6 +731,7 @@ extern "C" int selm_destroy(selm_sim* s) {
   analysis_detach_all(s);
   fused_release(s);
   free_all(s->allocs);
+  if (s->hstage_cnt) cudaFreeHost(s->hstage_cnt);
   if (s->own_st && s->st) cudaStreamDestroy(s->st);
   if (s->st2) cudaStreamDestroy(s->st2);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);

@@ -39,6 +39,10 @@ struct selm_sim {
   double *v = nullptr, *f = nullptr, *m = nullptr, *tf = nullptr;
   void* wrec = nullptr;  // per-monomer stencil records (WRec<T> of the grid precision)
   int cx = 0;
+  // staged upload of a per-step round trip (allocated on the first upload after the first)
+  double *xin = nullptr, *vin = nullptr;
+  unsigned long long* stage_cnt = nullptr;   // device: bad, outside
+  unsigned long long* hstage_cnt = nullptr;  // pinned host copy
   // plain-form grid (Eulerian::d_u[2], d_f, d_p, cuda/SELM_Eulerian.cuh:12-20)
   double* u64[2] = {nullptr, nullptr};
   double *fg64 = nullptr, *p64 = nullptr, *work64 = nullptr, *partial = nullptr, *sum = nullptr;

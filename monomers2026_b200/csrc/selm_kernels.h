@@ -109,6 +109,12 @@ template <typename T>
 cudaError_t interp_only(const T* u, const double* x, int M, int nx, int ny, int nz, double lo, double dx, double* out,
                         cudaStream_t st);
 cudaError_t spread_prepare_attributes();
+// staged monomer upload: check the staged positions (cnt[2] on the device),
+// then commit positions and velocities (vin NULL: zeros) if both counts are 0
+cudaError_t stage_check(const double* xin, long n, double lo, double hi, double lim, unsigned long long* cnt,
+                        cudaStream_t st);
+cudaError_t stage_commit(const double* xin, const double* vin, double* x, double* v, long n,
+                         const unsigned long long* cnt, cudaStream_t st);
 template <typename T>
 cudaError_t spread_gather(T* fgrid, bool accumulate, const double* x_old, const double* tf, const BinSpec& bs,
                           const int* offsets, const int* sorted, const CouplingArgs& a, cudaStream_t st,

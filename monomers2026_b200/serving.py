@@ -32,8 +32,9 @@ SPREAD_TILE = (16, 8, 16)  # cells of a spread tile (kTX, kTY, kTZ of the engine
 
 def estimate_device_bytes(params, natoms: int, pairs: bool = True) -> int:
     """Upper estimate of the device memory of one simulation (for admission
-    before it is created): fields, spectra, monomer arrays, stencil records,
-    tile and force-cell buckets and the neighbour list."""
+    before it is created): fields, spectra, monomer arrays (with the staging
+    buffers of a per-step upload), stencil records, tile and force-cell
+    buckets and the neighbour list."""
     nx, ny, nz = (int(v) for v in params.numMeshPtsPerDir)
     N = nx * ny * nz
     N2 = (nx // 2 + 1) * ny * nz
@@ -51,7 +52,8 @@ def estimate_device_bytes(params, natoms: int, pairs: bool = True) -> int:
         per *= 1.0 if b == 1 else 1.0 + 4.0 / t
     cap = max(128, -(-(int(math.ceil(4.0 * M * per / tiles)) + 64) // 32) * 32)
     slots = 4 * tiles * (cap + 1) + 8 * (27 * M + 1024)  # tile slots and the overflow list
-    mono = M * (2 * 24 + 3 * 24 + 8 + (128 if s == 4 else 224)) + slots
+    # x (two buffers), v, f, tf, m, the staged upload of a per-step round trip, stencil records
+    mono = M * (2 * 24 + 3 * 24 + 8 + 2 * 24 + (128 if s == 4 else 224)) + slots
     nl = 0
     if pairs:
         nc3 = min(2 * M, N) + 1

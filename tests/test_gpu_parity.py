@@ -359,9 +359,11 @@ def test_neighbour_list_overflow_is_flagged():
 
 
 def test_set_particles_checks_and_remaps():
-    """Non-finite or far positions and non-positive masses are refused before
-    anything reaches the device; positions outside the box are moved by whole
-    box lengths into [lo, hi), as LAMMPS does at setup."""
+    """Non-finite or far positions and non-positive masses are refused and
+    leave the simulation's monomers as they were (the positions are checked in
+    device staging buffers before they are committed); positions outside the
+    box are moved by whole box lengths into [lo, hi), as LAMMPS does at
+    setup."""
     import ctypes as C
 
     from monomers2026_b200 import _lib
@@ -374,7 +376,11 @@ def test_set_particles_checks_and_remaps():
     for bad in (np.nan, np.inf, -np.inf, 1e12):
         x = np.ascontiguousarray(x0.copy())
         x[M // 2, 1] = bad
-        assert L.selm_set_particles(g._h, M, x.ctypes.data_as(dp), None, None) == 1  # SELM_ERR_INVALID
+        x[0] += 0.125
+        v = np.full((M, 3), 0.5)
+        assert L.selm_set_particles(g._h, M, x.ctypes.data_as(dp), v.ctypes.data_as(dp), None) == 1  # INVALID
+        xg, vg, _ = g.particles()
+        assert np.array_equal(xg, x0) and np.array_equal(vg, v0)
     m = np.ones(M)
     m[3] = 0.0
     x = np.ascontiguousarray(x0.copy())
@@ -385,3 +391,12 @@ def test_set_particles_checks_and_remaps():
     got = g.particles()[0]
     assert np.allclose(got[0], [wl.params.box_lo + 0.25, wl.params.box_hi - 0.5, wl.params.box_lo + 0.125])
     assert np.array_equal(got[1:], x0[1:])
+    # in-box uploads commit exactly; no velocities means zero velocities
+    x1 = np.ascontiguousarray(got.copy())
+    x1[5] = wl.params.box_lo + 1.0
+    v1 = np.random.default_rng(3).standard_normal((M, 3))
+    _lib.check(L.selm_set_particles(g._h, M, x1.ctypes.data_as(dp), v1.ctypes.data_as(dp), None))
+    xg, vg, _ = g.particles()
+    assert np.array_equal(xg, x1) and np.array_equal(vg, v1)
+    _lib.check(L.selm_set_particles(g._h, M, x1.ctypes.data_as(dp), None, None))
+    assert np.array_equal(g.particles()[0], x1) and np.all(g.particles()[1] == 0)
