@@ -134,7 +134,12 @@ int selm_step(selm_sim* s, int nsteps);
 int selm_destroy(selm_sim* s);
 
 /* ---- state access (the reference's public pointers, copied) ---- */
-int selm_get_particles(selm_sim* s, double* x, double* v, double* f); /* any may be NULL */
+/* Positions, velocities and forces after the last step (any may be NULL).
+ * Returns once they are in host memory.  Right after a step of a fused form
+ * with the device force field, that is as soon as the step has written them:
+ * the rest of that step (spread and fluid solve) may still run on the device
+ * (selm_synchronize waits for it); every later call is ordered after it. */
+int selm_get_particles(selm_sim* s, double* x, double* v, double* f);
 /* t_f of the last inertial step, per monomer and component: the coupling
  * impulse -upsilon (v - Gamma u) dt plus the thermal kick, before the
  * conservative force is added (cuda/SELM_Kernel.cu:302-373).  The reference

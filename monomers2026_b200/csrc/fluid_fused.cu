@@ -533,6 +533,9 @@ struct FusedState {
   cudaGraph_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   unsigned long long graph_kernels[2] = {0, 0};
+  // the graph records s->ev_ready once the step's monomer state (x, v, f) is final
+  bool ready_node[2] = {false, false};
+  bool body_ready = false;  // set by the step body just issued
   bool fast = false;  // compile-time four-step kernels for this grid size
   // tuning knobs (SELM_TUNE_*): four-step split, blocks per SM of the z kernel
   int tune_split = 0;
@@ -803,6 +806,12 @@ template <typename T> static int fused_step_t(selm_sim* s, bool* forces_done) {
       CUF(cudaStreamWaitEvent(s->st2, s->ev_fork, 0));
       rc0 = engine_forces_on(s, xn, s->st2);
       if (rc0) return rc0;
+      // x^{n+1} and v (interpolation, which the side stream waited for) and f
+      // (just computed) are final here: an external event node lets a
+      // read-back overlap the rest of the step (the side stream only issues
+      // here inside a graph capture)
+      CUF(cudaEventRecordWithFlags(s->ev_ready, s->st2, cudaEventRecordExternal));
+      z->body_ready = true;
       CUF(cudaEventRecord(s->ev_join, s->st2));
       *forces_done = true;
     }
@@ -834,6 +843,7 @@ int fused_initial(selm_sim* s) {
 static int fused_body(selm_sim* s) {
   const bool f32 = s->fz->fp32;
   bool done = false;
+  s->fz->body_ready = false;
   int rc = f32 ? fused_step_t<float>(s, &done) : fused_step_t<double>(s, &done);
   if (rc || done) return rc;
   if (s->M > 0) s->cx ^= 1;
@@ -843,12 +853,14 @@ static int fused_body(selm_sim* s) {
 }
 
 void fused_invalidate_graphs(selm_sim* s) {
+  s->ready_early = false;
   if (!s->fz) return;
   for (int q = 0; q < 2; q++) {
     if (s->fz->gexec[q]) cudaGraphExecDestroy(s->fz->gexec[q]);
     if (s->fz->graph[q]) cudaGraphDestroy(s->fz->graph[q]);
     s->fz->gexec[q] = nullptr;
     s->fz->graph[q] = nullptr;
+    s->fz->ready_node[q] = false;
   }
   if (s->batch) batch_mark_dirty(s->batch, s);
 }
@@ -881,6 +893,7 @@ static int fused_capture(selm_sim* s, int par) {
   if (ec != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
   z->graph[par] = g;
   z->graph_kernels[par] = k;
+  z->ready_node[par] = z->body_ready;
   return SELM_OK;
 }
 
@@ -923,6 +936,7 @@ int fused_step(selm_sim* s) {
     if (rc) return rc;
     count_launches((unsigned)z->graph_kernels[par]);
     CUF(cudaGraphLaunch(z->gexec[par], s->st));
+    s->ready_early = z->ready_node[par];
   } else {
     const int rc = fused_body(s);
     if (rc) return rc;

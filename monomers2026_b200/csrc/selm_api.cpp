@@ -316,6 +316,7 @@ static int set_particles_staged(selm_sim* s, int M, const double* x, const doubl
 
 extern "C" int selm_set_particles(selm_sim* s, int M, const double* x, const double* v, const double* mass) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  s->ready_early = false;
   if (M < 0 || (M > 0 && !x)) return selm_fail(SELM_ERR_INVALID, "bad particle arrays");
   if (s->M != 0 && M != s->M) return selm_fail(SELM_ERR_STATE, "monomer count is fixed once set");
   // masses may be left out once set: a per-step host round trip moves positions and velocities only
@@ -598,6 +599,7 @@ int engine_side_stream(selm_sim* s) {
   CU(cudaStreamCreateWithPriority(&s->st2, cudaStreamNonBlocking, prio_hi));
   CU(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+  CU(cudaEventCreateWithFlags(&s->ev_ready, cudaEventDisableTiming));
   return SELM_OK;
 }
 
@@ -692,6 +694,7 @@ static int plain_step(selm_sim* s) {
 extern "C" int selm_initial(selm_sim* s) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
   s->step = 0;
+  s->ready_early = false;
   int rc = engine_forces(s);
   if (rc) return rc;
   if (s->prm.form == SELM_FORM_PLAIN64) {
@@ -712,6 +715,7 @@ extern "C" int selm_step(selm_sim* s, int nsteps) {
   if (!s->initialized) return selm_fail(SELM_ERR_STATE, "selm_initial has not been called");
   if (s->batch) return selm_fail(SELM_ERR_STATE, "the simulation belongs to a batch: step it with selm_batch_step");
   if (nsteps < 0) return selm_fail(SELM_ERR_INVALID, "nsteps < 0");
+  if (nsteps > 0) s->ready_early = false;  // a graph step sets it again
   for (int i = 0; i < nsteps; i++) {
     const int rc = (s->prm.form == SELM_FORM_PLAIN64) ? plain_step(s) : fused_step(s);
     if (rc) return rc;
@@ -728,6 +732,7 @@ extern "C" int selm_destroy(selm_sim* s) {
     cudaEventDestroy(ev.b);
   }
   if (s->st2) cudaStreamSynchronize(s->st2);
+  if (s->st_copy) cudaStreamSynchronize(s->st_copy);
   analysis_detach_all(s);
   fused_release(s);
   free_all(s->allocs);
@@ -736,6 +741,8 @@ extern "C" int selm_destroy(selm_sim* s) {
   if (s->st2) cudaStreamDestroy(s->st2);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->ev_ready) cudaEventDestroy(s->ev_ready);
+  if (s->st_copy) cudaStreamDestroy(s->st_copy);
   delete s;
   return SELM_OK;
 }
@@ -745,10 +752,18 @@ extern "C" int selm_get_particles(selm_sim* s, double* x, double* v, double* f) 
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
   if (s->M == 0) return SELM_OK;
   const size_t b = sizeof(double) * 3 * s->M;
-  if (x) CU(cudaMemcpyAsync(x, s->x[s->cx], b, cudaMemcpyDeviceToHost, s->st));
-  if (v) CU(cudaMemcpyAsync(v, s->v, b, cudaMemcpyDeviceToHost, s->st));
-  if (f) CU(cudaMemcpyAsync(f, s->f, b, cudaMemcpyDeviceToHost, s->st));
-  CU(cudaStreamSynchronize(s->st));
+  // right after a graph step: copy once the step's monomer state is final,
+  // while the spread and the fluid solve of that step still run
+  cudaStream_t cs = s->st;
+  if (s->ready_early && s->ev_ready && !s->batch) {
+    if (!s->st_copy) CU(cudaStreamCreateWithFlags(&s->st_copy, cudaStreamNonBlocking));
+    CU(cudaStreamWaitEvent(s->st_copy, s->ev_ready, 0));
+    cs = s->st_copy;
+  }
+  if (x) CU(cudaMemcpyAsync(x, s->x[s->cx], b, cudaMemcpyDeviceToHost, cs));
+  if (v) CU(cudaMemcpyAsync(v, s->v, b, cudaMemcpyDeviceToHost, cs));
+  if (f) CU(cudaMemcpyAsync(f, s->f, b, cudaMemcpyDeviceToHost, cs));
+  CU(cudaStreamSynchronize(cs));
   return SELM_OK;
 }
 
@@ -812,6 +827,7 @@ extern "C" int selm_set_stream(selm_sim* s, void* stream) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
   if (s->batch) return selm_fail(SELM_ERR_STATE, "the simulation belongs to a batch and runs on its stream");
   CU(cudaStreamSynchronize(s->st));
+  s->ready_early = false;
   if (s->own_st) cudaStreamDestroy(s->st);
   if (stream) {
     s->st = (cudaStream_t)stream;
