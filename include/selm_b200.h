@@ -61,7 +61,8 @@ extern "C" {
 /* Model.SELM keys (cuda/SELM.cu:17-48) plus the box and dt that the
  * reference takes from LAMMPS (domain->boxlo/hi, update->dt). */
 typedef struct selm_params {
-  int num_mesh_pts[3];       /* numMeshPtsPerDir (all equal, as the reference assumes) */
+  int num_mesh_pts[3];       /* numMeshPtsPerDir (all equal, as the reference assumes), in [4, 1024]
+                                with no prime factor above 61 (the FFT's radices) */
   double box_lo, box_hi;     /* cubic periodic box; dx = (hi - lo)/Nx */
   double rho, mu, KB, T, dt; /* rho mu KB T, timestep */
   int flag_stochastic;       /* flagStochasticDriving */

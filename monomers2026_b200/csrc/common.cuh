@@ -213,6 +213,21 @@ __device__ __forceinline__ void stockham_stage(const C* __restrict__ a, C* __res
     }
     const C* ai = a + line * sb;
     C* bo = b + line * sb;
+    if (p > 8) {
+      // primes 11..61: the inputs are re-read from shared memory for each
+      // output (a p-point DFT, p^2 products, in the oracle's order)
+      const int np = n / p;
+      for (int v = 0; v < p; v++) {
+        C acc = ai[(q * rs + k) * st];
+        for (int s = 1; s < p; s++) {
+          const C y = ai[(q * rs + k + s * r) * st];
+          const C ys = (q == 0) ? y : cmul(y, w[s * q * r]);
+          acc = cadd(acc, cmul(ys, w[((s * v) % p) * np]));
+        }
+        bo[((q + v * Ls) * r + k) * st] = acc;
+      }
+      continue;
+    }
     C c[8];
 #pragma unroll 1
     for (int s = 0; s < p; s++) {

@@ -63,9 +63,12 @@ static void free_all(std::vector<void*>& v) {
 }
 
 // ================================================================ FFT tables
-static bool smooth7(int n) {
+// Line lengths the FFT stages take: prime factors up to 61 (radix 4, 2, 3, 5
+// and 7 butterflies, a p-point DFT for the primes 11..61), as the oracle.
+constexpr int kMaxFftPrime = 61;
+static bool fft_size_ok(int n) {
   if (n < 1) return false;
-  for (int p : {2, 3, 5, 7})
+  for (int p = 2; p <= kMaxFftPrime; p++)
     while (n % p == 0) n /= p;
   return n == 1;
 }
@@ -143,8 +146,8 @@ static void prof_collect(selm_sim* s) {
 static int validate(const selm_params* p) {
   if (!p) return selm_fail(SELM_ERR_INVALID, "params is NULL");
   for (int a = 0; a < 3; a++)
-    if (p->num_mesh_pts[a] < 4 || p->num_mesh_pts[a] > 1024 || !smooth7(p->num_mesh_pts[a]))
-      return selm_fail(SELM_ERR_INVALID, "numMeshPtsPerDir must be in [4,1024] with prime factors 2,3,5,7");
+    if (p->num_mesh_pts[a] < 4 || p->num_mesh_pts[a] > 1024 || !fft_size_ok(p->num_mesh_pts[a]))
+      return selm_fail(SELM_ERR_INVALID, "numMeshPtsPerDir must be in [4,1024] with no prime factor above 61");
   if (p->num_mesh_pts[0] != p->num_mesh_pts[1] || p->num_mesh_pts[0] != p->num_mesh_pts[2])
     return selm_fail(SELM_ERR_INVALID, "numMeshPtsPerDir must be equal in every dimension (cubic box)");
   if (!(p->box_hi > p->box_lo)) return selm_fail(SELM_ERR_INVALID, "box_hi must exceed box_lo");
@@ -891,8 +894,8 @@ struct OpScope {
 int check_dims(const int dims[3]) {
   if (!dims) return selm_fail(SELM_ERR_INVALID, "dims is NULL");
   for (int a = 0; a < 3; a++)
-    if (dims[a] < 4 || dims[a] > 1024 || !smooth7(dims[a]))
-      return selm_fail(SELM_ERR_INVALID, "dims must be in [4,1024] with prime factors 2,3,5,7");
+    if (dims[a] < 4 || dims[a] > 1024 || !fft_size_ok(dims[a]))
+      return selm_fail(SELM_ERR_INVALID, "dims must be in [4,1024] with no prime factor above 61");
   return SELM_OK;
 }
 

@@ -20,7 +20,9 @@ def rel(a, b):
     return float(np.abs(a - b).max() / (s if s > 0 else 1.0))
 
 
-FFT_DIMS = [(8, 8, 8), (24, 24, 24), (30, 30, 30), (32, 32, 32), (48, 48, 48), (12, 16, 20), (128, 128, 128)]
+FFT_DIMS = [(8, 8, 8), (24, 24, 24), (30, 30, 30), (32, 32, 32), (48, 48, 48), (12, 16, 20), (128, 128, 128),
+            # odd lengths, and prime factors 11..61 (p-point DFT stages)
+            (27, 25, 21), (22, 26, 34), (62, 58, 46), (61, 12, 10)]
 
 
 @pytest.mark.parametrize("dims", FFT_DIMS)
@@ -220,6 +222,16 @@ def test_fused_128_cubed_with_noise(oracle, form, tol):
 def test_fused64_nonpow2_grid_with_noise(oracle, grid):
     wl = W.config(3, kT=1.0, nchains=3, length=20, grid=grid, form="fused64")
     _compare_run(oracle, wl, 8, 1e-11)
+
+
+@pytest.mark.parametrize("grid", [22, 26, 27])
+@pytest.mark.parametrize("form,tol", [("plain64", 1e-11), ("fused64", 1e-11), ("fused32", 1e-4)])
+def test_grids_with_larger_primes_and_odd_grids_with_noise(oracle, grid, form, tol):
+    """Grids of 22 = 2 x 11 and 26 = 2 x 13 points per side (p-point DFT
+    stages in every FFT) and an odd grid (27, no Nyquist plane), thermal
+    noise on: whole steps against the oracle on the same Philox stream."""
+    wl = W.config(3, kT=1.0, nchains=3, length=20, grid=grid, form=form)
+    _compare_run(oracle, wl, 6, tol)
 
 
 def test_fused64_exact_noise_mode(oracle):

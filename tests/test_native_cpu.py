@@ -44,7 +44,7 @@ def test_version_string(lib):
 def test_create_rejects_bad_params_without_gpu(lib):
     from monomers2026_b200.selm import Params
     h = C.c_void_p()
-    for bad in [dict(numMeshPtsPerDir=(32, 32, 30)), dict(numMeshPtsPerDir=(22, 22, 22)),
+    for bad in [dict(numMeshPtsPerDir=(32, 32, 30)), dict(numMeshPtsPerDir=(134, 134, 134)),
                 dict(box_hi=-1.0), dict(dt=0.0), dict(rho=0.0)]:
         p = Params(**bad).to_c()
         assert lib.selm_create(C.byref(p), C.byref(h)) == 1  # SELM_ERR_INVALID
@@ -52,10 +52,10 @@ def test_create_rejects_bad_params_without_gpu(lib):
 
 
 def test_operator_dims_validation(lib):
-    d = (C.c_int * 3)(22, 8, 8)
+    d = (C.c_int * 3)(67, 8, 8)
     x = np.zeros(3)
     out = np.zeros(3)
-    u = np.zeros(3 * 22 * 8 * 8)
+    u = np.zeros(3 * 67 * 8 * 8)
     dp = C.POINTER(C.c_double)
     rc = lib.selm_op_interp(64, d, 0.0, 1.0, u.ctypes.data_as(dp), 1, x.ctypes.data_as(dp), out.ctypes.data_as(dp))
     assert rc == 1
