@@ -802,14 +802,15 @@ template <typename T> static int fused_step_t(selm_sim* s, bool* forces_done) {
     if (s->have_topo && !s->cb && !s->prof && !s->batch) {
       int rc0 = engine_side_stream(s);
       if (rc0) return rc0;
+      CUF(cudaEventRecordWithFlags(s->ev_xv, s->st, cudaEventRecordExternal));  // x^{n+1} and v final
       CUF(cudaEventRecord(s->ev_fork, s->st));
       CUF(cudaStreamWaitEvent(s->st2, s->ev_fork, 0));
       rc0 = engine_forces_on(s, xn, s->st2);
       if (rc0) return rc0;
       // x^{n+1} and v (interpolation, which the side stream waited for) and f
-      // (just computed) are final here: an external event node lets a
-      // read-back overlap the rest of the step (the side stream only issues
-      // here inside a graph capture)
+      // (just computed) are final here: external event nodes (ev_xv above,
+      // ev_ready here) let a read-back overlap the rest of the step (the
+      // side stream only issues here inside a graph capture)
       CUF(cudaEventRecordWithFlags(s->ev_ready, s->st2, cudaEventRecordExternal));
       z->body_ready = true;
       CUF(cudaEventRecord(s->ev_join, s->st2));

@@ -602,6 +602,7 @@ int engine_side_stream(selm_sim* s) {
   CU(cudaStreamCreateWithPriority(&s->st2, cudaStreamNonBlocking, prio_hi));
   CU(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+  CU(cudaEventCreateWithFlags(&s->ev_xv, cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&s->ev_ready, cudaEventDisableTiming));
   return SELM_OK;
 }
@@ -744,6 +745,7 @@ extern "C" int selm_destroy(selm_sim* s) {
   if (s->st2) cudaStreamDestroy(s->st2);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->ev_xv) cudaEventDestroy(s->ev_xv);
   if (s->ev_ready) cudaEventDestroy(s->ev_ready);
   if (s->st_copy) cudaStreamDestroy(s->st_copy);
   delete s;
@@ -758,13 +760,15 @@ extern "C" int selm_get_particles(selm_sim* s, double* x, double* v, double* f) 
   // right after a graph step: copy once the step's monomer state is final,
   // while the spread and the fluid solve of that step still run
   cudaStream_t cs = s->st;
-  if (s->ready_early && s->ev_ready && !s->batch) {
+  const bool early = s->ready_early && s->ev_ready && !s->batch;
+  if (early) {
     if (!s->st_copy) CU(cudaStreamCreateWithFlags(&s->st_copy, cudaStreamNonBlocking));
-    CU(cudaStreamWaitEvent(s->st_copy, s->ev_ready, 0));
+    CU(cudaStreamWaitEvent(s->st_copy, s->ev_xv, 0));
     cs = s->st_copy;
   }
   if (x) CU(cudaMemcpyAsync(x, s->x[s->cx], b, cudaMemcpyDeviceToHost, cs));
   if (v) CU(cudaMemcpyAsync(v, s->v, b, cudaMemcpyDeviceToHost, cs));
+  if (early) CU(cudaStreamWaitEvent(cs, s->ev_ready, 0));  // f: after the side-stream forces
   if (f) CU(cudaMemcpyAsync(f, s->f, b, cudaMemcpyDeviceToHost, cs));
   CU(cudaStreamSynchronize(cs));
   return SELM_OK;

@@ -29,11 +29,12 @@ struct selm_sim {
   bool own_st = false;
   cudaStream_t st2 = nullptr;  // side stream: the forces of a step beside its fluid solve
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  // Early read-back: ev_ready is recorded by the step graph (an external event
-  // node) when x, v and f are final; ready_early says that the last step was
-  // such a graph and nothing has written the monomer state since.  A read-back
-  // then waits for ev_ready on st_copy instead of for the whole step.
-  cudaEvent_t ev_ready = nullptr;
+  // Early read-back: the step graph records ev_xv (external event node) when
+  // x and v are final and ev_ready when f is too; ready_early says that the
+  // last step was such a graph and nothing has written the monomer state
+  // since.  A read-back then waits for those on st_copy instead of for the
+  // whole step.
+  cudaEvent_t ev_xv = nullptr, ev_ready = nullptr;
   cudaStream_t st_copy = nullptr;
   bool ready_early = false;
   std::vector<void*> allocs;
