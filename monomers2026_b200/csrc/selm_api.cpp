@@ -286,9 +286,12 @@ static long count_nonpositive(const double* __restrict__ m, long n) {
 static int set_particles_host(selm_sim* s, int M, const double* x, const double* v, const double* mass);
 
 // Upload of a simulation that already holds its monomers (the per-step round
-// trip): the positions and velocities go to device staging buffers, checked
-// and committed there (no host pass over them); the rare upload with
-// positions outside the box is redone by the host path, which remaps them.
+// trip): the positions and velocities go to device staging buffers and are
+// checked there on the copy stream (no host pass over them; a step still
+// running on the simulation's stream is not waited for); the call returns
+// the verdict and leaves the commit into the state queued on the
+// simulation's stream.  The rare upload with positions outside the box is
+// redone by the host path, which remaps them.
 static int set_particles_staged(selm_sim* s, int M, const double* x, const double* v, const double* mass) {
   int rc;
   const long n = 3L * M;
@@ -301,15 +304,25 @@ static int set_particles_staged(selm_sim* s, int M, const double* x, const doubl
       return selm_fail(SELM_ERR_NOMEM, "cudaMallocHost failed");
     }
   }
+  if (!s->st_copy) CU(cudaStreamCreateWithFlags(&s->st_copy, cudaStreamNonBlocking));
+  if (!s->ev_staged) {
+    CU(cudaEventCreateWithFlags(&s->ev_staged, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&s->ev_committed, cudaEventDisableTiming));
+  }
   const double L = s->hi - s->lo;
-  CU(cudaMemcpyAsync(s->xin, x, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
-  if (v) CU(cudaMemcpyAsync(s->vin, v, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
-  CU(selm::stage_check(s->xin, n, s->lo, s->hi, 1e6 * L, s->stage_cnt, s->st));
-  CU(selm::stage_commit(s->xin, v ? s->vin : nullptr, s->x[s->cx], s->v, n, s->stage_cnt, s->st));
-  CU(cudaMemcpyAsync(s->hstage_cnt, s->stage_cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->st));
-  CU(cudaStreamSynchronize(s->st));
+  cudaStream_t cs = s->st_copy;
+  CU(cudaStreamWaitEvent(cs, s->ev_committed, 0));  // the last commit has read the staging buffers
+  CU(cudaMemcpyAsync(s->xin, x, sizeof(double) * n, cudaMemcpyHostToDevice, cs));
+  if (v) CU(cudaMemcpyAsync(s->vin, v, sizeof(double) * n, cudaMemcpyHostToDevice, cs));
+  CU(selm::stage_check(s->xin, n, s->lo, s->hi, 1e6 * L, s->stage_cnt, cs));
+  CU(cudaMemcpyAsync(s->hstage_cnt, s->stage_cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, cs));
+  CU(cudaStreamSynchronize(cs));
   if (s->hstage_cnt[0]) return selm_fail(SELM_ERR_INVALID, "non-finite or far out-of-box position");
   if (s->hstage_cnt[1]) return set_particles_host(s, M, x, v, mass);
+  CU(cudaEventRecord(s->ev_staged, cs));
+  CU(cudaStreamWaitEvent(s->st, s->ev_staged, 0));
+  CU(selm::stage_commit(s->xin, v ? s->vin : nullptr, s->x[s->cx], s->v, n, s->stage_cnt, s->st));
+  CU(cudaEventRecord(s->ev_committed, s->st));
   if (mass) {
     CU(cudaMemcpyAsync(s->m, mass, sizeof(double) * M, cudaMemcpyHostToDevice, s->st));
     CU(cudaStreamSynchronize(s->st));
@@ -746,6 +759,8 @@ extern "C" int selm_destroy(selm_sim* s) {
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
   if (s->ev_xv) cudaEventDestroy(s->ev_xv);
+  if (s->ev_staged) cudaEventDestroy(s->ev_staged);
+  if (s->ev_committed) cudaEventDestroy(s->ev_committed);
   if (s->ev_ready) cudaEventDestroy(s->ev_ready);
   if (s->st_copy) cudaStreamDestroy(s->st_copy);
   delete s;

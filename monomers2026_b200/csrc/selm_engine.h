@@ -51,6 +51,8 @@ struct selm_sim {
   double *xin = nullptr, *vin = nullptr;
   unsigned long long* stage_cnt = nullptr;   // device: bad, outside
   unsigned long long* hstage_cnt = nullptr;  // pinned host copy
+  cudaEvent_t ev_staged = nullptr;     // staged and checked (copy stream)
+  cudaEvent_t ev_committed = nullptr;  // committed (simulation stream): staging free again
   // plain-form grid (Eulerian::d_u[2], d_f, d_p, cuda/SELM_Eulerian.cuh:12-20)
   double* u64[2] = {nullptr, nullptr};
   double *fg64 = nullptr, *p64 = nullptr, *work64 = nullptr, *partial = nullptr, *sum = nullptr;
