@@ -121,7 +121,9 @@ int selm_create_from_files(const char* case_dir, selm_sim** out);
  * SELM_ERR_INVALID and leaves the monomers as they were; positions outside
  * the box are moved by whole box lengths into [lo, hi).  After the first call
  * the positions are checked on the device (staging buffers, 48 bytes per
- * monomer, allocated by the second call). */
+ * monomer, allocated by the second call); the call returns once the host
+ * buffers have been read and checked, with the update of the state queued on
+ * the simulation's stream ahead of every later call. */
 int selm_set_particles(selm_sim* s, int natoms, const double* x, const double* v, const double* mass);
 /* device force field (replaces the per-step LAMMPS round trip) */
 int selm_set_topology(selm_sim* s, const selm_topology* topo);
