@@ -75,6 +75,28 @@ def test_continuous_batching_join_and_leave():
     b.final()
 
 
+def test_read_back_around_joining_and_leaving():
+    """Read back right after stepping alone (the read-back that overlaps the
+    rest of that step), then after batch steps (on the batch's stream), then
+    after leaving: every read-back equals that of the same simulation
+    stepped alone throughout."""
+    mk = lambda: _sim(W.replica(24, 3, 20, 1.0, 31))
+    ref, s = mk(), mk()
+    b = Batch()
+    for alone_steps, batch_steps in ((2, 3), (1, 2)):
+        s.run(alone_steps)
+        ref.run(alone_steps)
+        assert _same(s.particles(), ref.particles())
+        b.add(s)
+        b.run(batch_steps)
+        ref.run(batch_steps)
+        assert _same(s.particles(), ref.particles())
+        b.remove(s)
+        assert _same(s.particles(), ref.particles())
+    assert _same(_state(s), _state(ref))
+    b.final()
+
+
 def test_groups_shared_by_several_members():
     """More members than groups (eight): groups hold two members each; a
     member leaving a shared group and members joining at odd steps (other
