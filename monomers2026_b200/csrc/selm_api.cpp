@@ -295,20 +295,18 @@ static int set_particles_host(selm_sim* s, int M, const double* x, const double*
 static int set_particles_staged(selm_sim* s, int M, const double* x, const double* v, const double* mass) {
   int rc;
   const long n = 3L * M;
-  if (!s->xin) {
-    if ((rc = dalloc(s, &s->xin, n)) || (rc = dalloc(s, &s->vin, n)) || (rc = dalloc(s, &s->stage_cnt, 2)))
-      return rc;
-    if (cudaMallocHost((void**)&s->hstage_cnt, 2 * sizeof(unsigned long long)) != cudaSuccess) {
-      cudaGetLastError();
-      s->hstage_cnt = nullptr;
-      return selm_fail(SELM_ERR_NOMEM, "cudaMallocHost failed");
-    }
+  // each piece made when missing (a call that failed part way leaves the rest to the next)
+  if (!s->xin && (rc = dalloc(s, &s->xin, n))) return rc;
+  if (!s->vin && (rc = dalloc(s, &s->vin, n))) return rc;
+  if (!s->stage_cnt && (rc = dalloc(s, &s->stage_cnt, 2))) return rc;
+  if (!s->hstage_cnt && cudaMallocHost((void**)&s->hstage_cnt, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    s->hstage_cnt = nullptr;
+    return selm_fail(SELM_ERR_NOMEM, "cudaMallocHost failed");
   }
   if (!s->st_copy) CU(cudaStreamCreateWithFlags(&s->st_copy, cudaStreamNonBlocking));
-  if (!s->ev_staged) {
-    CU(cudaEventCreateWithFlags(&s->ev_staged, cudaEventDisableTiming));
-    CU(cudaEventCreateWithFlags(&s->ev_committed, cudaEventDisableTiming));
-  }
+  if (!s->ev_staged) CU(cudaEventCreateWithFlags(&s->ev_staged, cudaEventDisableTiming));
+  if (!s->ev_committed) CU(cudaEventCreateWithFlags(&s->ev_committed, cudaEventDisableTiming));
   const double L = s->hi - s->lo;
   cudaStream_t cs = s->st_copy;
   CU(cudaStreamWaitEvent(cs, s->ev_committed, 0));  // the last commit has read the staging buffers
@@ -608,15 +606,15 @@ extern "C" int selm_set_force_callback(selm_sim* s, selm_force_fn fn, void* user
 
 // ---------------------------------------------------------------- forces
 int engine_side_stream(selm_sim* s) {
-  if (s->st2) return SELM_OK;
-  // high priority: on a neighbour-list rebuild the side stream holds the step's critical path
-  int prio_lo = 0, prio_hi = 0;
-  CU(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-  CU(cudaStreamCreateWithPriority(&s->st2, cudaStreamNonBlocking, prio_hi));
-  CU(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
-  CU(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
-  CU(cudaEventCreateWithFlags(&s->ev_xv, cudaEventDisableTiming));
-  CU(cudaEventCreateWithFlags(&s->ev_ready, cudaEventDisableTiming));
+  // each piece made when missing (a call that failed part way leaves the rest to the next)
+  if (!s->st2) {
+    // high priority: on a neighbour-list rebuild the side stream holds the step's critical path
+    int prio_lo = 0, prio_hi = 0;
+    CU(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    CU(cudaStreamCreateWithPriority(&s->st2, cudaStreamNonBlocking, prio_hi));
+  }
+  for (cudaEvent_t* e : {&s->ev_fork, &s->ev_join, &s->ev_xv, &s->ev_ready})
+    if (!*e) CU(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   return SELM_OK;
 }
 
