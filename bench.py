@@ -335,6 +335,12 @@ def run_ours(args, rank, world, local_rank):
         roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(ach / hbm, 4), "peak_kind": peak_kind, "algorithmic_bytes": ab,
                 "traffic": traffic_from_profiles(dom, args.form, N)}
+        # the whole step beside it: fluid 30 N s (one compulsory sweep of each field) plus the
+        # monomers M (48 + 6 s + 8), over the timed step
+        step_bytes = 30.0 * N * s + M * (48 + 6 * s + 8)
+        step_ach = step_bytes / (total_ms / args.steps / 1e3) / 1e9
+        roof["step"] = {"algorithmic_bytes": step_bytes, "achieved": round(step_ach, 1),
+                        "frac": round(step_ach / hbm, 4)}
 
     # ---- batched ensemble and serving (rank 0 at N=1)
     batched = serving = None
