@@ -25,7 +25,7 @@ EXPORTED = [
     "selm_dcd_open", "selm_dcd_open_sim", "selm_dcd_write", "selm_dcd_write_sim", "selm_dcd_close", "selm_case_dump",
     "selm_analysis_create", "selm_analysis_sample", "selm_analysis_msd", "selm_analysis_structure",
     "selm_analysis_kinetic", "selm_analysis_reset", "selm_analysis_device_bytes", "selm_analysis_destroy",
-    "selm_get_coupling_impulse",
+    "selm_get_coupling_impulse", "selm_host_register", "selm_host_unregister",
 ]
 
 SELM_OK = 0
@@ -105,6 +105,8 @@ def load():
     L.selm_batch_synchronize.argtypes = [vp]
     L.selm_batch_destroy.argtypes = [vp]
     L.selm_device_bytes.argtypes = [vp, C.POINTER(C.c_ulonglong)]
+    L.selm_host_register.argtypes = [vp, C.c_ulonglong]
+    L.selm_host_unregister.argtypes = [vp]
     L.selm_tune_set.argtypes = [vp, C.c_int, C.c_int]
     L.selm_tune_get.argtypes = [vp, C.c_int, ip]
     L.selm_tune_default.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]

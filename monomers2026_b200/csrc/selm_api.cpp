@@ -867,6 +867,33 @@ extern "C" int selm_synchronize(selm_sim* s) {
   return SELM_OK;
 }
 
+// Page-locks host memory that the caller owns (LAMMPS' atom->x/v/f, say), so
+// that the per-step copies through selm_set_particles / selm_get_particles
+// run as direct transfers instead of through the driver's pageable staging.
+extern "C" int selm_host_register(void* ptr, unsigned long long bytes) {
+  if (!ptr || bytes == 0) return selm_fail(SELM_ERR_INVALID, "selm_host_register: NULL pointer or zero bytes");
+  const cudaError_t e = cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault);
+  if (e == cudaErrorHostMemoryAlreadyRegistered) {
+    cudaGetLastError();
+    return SELM_OK;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return selm_fail(SELM_ERR_CUDA, std::string("cudaHostRegister: ") + cudaGetErrorString(e));
+  }
+  return SELM_OK;
+}
+
+extern "C" int selm_host_unregister(void* ptr) {
+  if (!ptr) return selm_fail(SELM_ERR_INVALID, "selm_host_unregister: NULL pointer");
+  const cudaError_t e = cudaHostUnregister(ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return selm_fail(SELM_ERR_CUDA, std::string("cudaHostUnregister: ") + cudaGetErrorString(e));
+  }
+  return SELM_OK;
+}
+
 extern "C" int selm_profile_enable(selm_sim* s, int enable) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
   if (s->batch && enable) return selm_fail(SELM_ERR_STATE, "a batch member is timed through its batch, not per kernel");

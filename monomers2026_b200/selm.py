@@ -242,6 +242,19 @@ TUNE_FFT_SPLIT = 1
 TUNE_Z_BLOCKS = 2
 
 
+def host_register(a: np.ndarray) -> None:
+    """Page-lock a C-contiguous host array (selm_host_register) so that the
+    per-step copies to and from it run as direct transfers; unregister it
+    (host_unregister) before it is freed."""
+    if not a.flags.c_contiguous or a.nbytes == 0:
+        raise ValueError("host_register needs a non-empty C-contiguous array")
+    check(_lib.load().selm_host_register(a.ctypes.data, a.nbytes))
+
+
+def host_unregister(a: np.ndarray) -> None:
+    check(_lib.load().selm_host_unregister(a.ctypes.data))
+
+
 def tune_default(grid: int, precision: int, knob: int, value: int) -> None:
     """Value of a knob for fused-form simulations created later with this cubic
     grid size and precision (selm_tune_default)."""
