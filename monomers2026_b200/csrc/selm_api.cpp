@@ -635,16 +635,27 @@ int engine_forces(selm_sim* s) {
     return rc;
   }
   if (s->cb) {
-    // host round trip, as Lagrangian_LAMMPS::compute_f (cuda/SELM_Lagrangian_LAMMPS.cu:107-130)
-    s->hx.resize(3 * (size_t)s->M);
-    s->hv.resize(3 * (size_t)s->M);
-    s->hf.resize(3 * (size_t)s->M);
-    CU(cudaMemcpyAsync(s->hx.data(), x, sizeof(double) * 3 * s->M, cudaMemcpyDeviceToHost, s->st));
-    CU(cudaMemcpyAsync(s->hv.data(), s->v, sizeof(double) * 3 * s->M, cudaMemcpyDeviceToHost, s->st));
+    // host round trip, as Lagrangian_LAMMPS::compute_f (cuda/SELM_Lagrangian_LAMMPS.cu:107-130),
+    // through page-locked buffers (direct transfers, not pageable staging)
+    const size_t n = 3 * (size_t)s->M;
+    if (!s->hcb || s->hcb_n < s->M) {
+      if (s->hcb) cudaFreeHost(s->hcb);
+      s->hcb = nullptr;
+      s->hcb_n = 0;
+      if (cudaMallocHost((void**)&s->hcb, sizeof(double) * 3 * n) != cudaSuccess) {
+        cudaGetLastError();
+        s->hcb = nullptr;
+        return selm_fail(SELM_ERR_NOMEM, "cudaMallocHost failed (force callback buffers)");
+      }
+      s->hcb_n = s->M;
+    }
+    double *hx = s->hcb, *hv = s->hcb + n, *hf = s->hcb + 2 * n;
+    CU(cudaMemcpyAsync(hx, x, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
+    CU(cudaMemcpyAsync(hv, s->v, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
-    const int r = s->cb(s->cb_user, s->M, s->hx.data(), s->hv.data(), s->hf.data());
+    const int r = s->cb(s->cb_user, s->M, hx, hv, hf);
     if (r != 0) return selm_fail(SELM_ERR_INVALID, "force callback returned an error");
-    CU(cudaMemcpyAsync(s->f, s->hf.data(), sizeof(double) * 3 * s->M, cudaMemcpyHostToDevice, s->st));
+    CU(cudaMemcpyAsync(s->f, hf, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
     CU(cudaStreamSynchronize(s->st));
     return SELM_OK;
   }
@@ -752,6 +763,7 @@ extern "C" int selm_destroy(selm_sim* s) {
   fused_release(s);
   free_all(s->allocs);
   if (s->hstage_cnt) cudaFreeHost(s->hstage_cnt);
+  if (s->hcb) cudaFreeHost(s->hcb);
   if (s->own_st && s->st) cudaStreamDestroy(s->st);
   if (s->st2) cudaStreamDestroy(s->st2);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);

@@ -69,6 +69,8 @@ struct selm_sim {
   selm_force_fn cb = nullptr;
   void* cb_user = nullptr;
   std::vector<double> hx, hv, hf;
+  double* hcb = nullptr;  // pinned host x, v, f [3][3M] of the host force callback's round trip
+  long hcb_n = 0;         // monomers it holds
   uint64_t step = 0;
   int case_nsteps = 0;  // nsteps of Model.SELM when created from a case directory
   int dump_every = 0;   // the case's "dump ... dcd N file" (0: none)

@@ -478,3 +478,32 @@ def test_registered_host_arrays_round_trip():
         host_unregister(a)
     with pytest.raises(RuntimeError):
         host_unregister(bufs[1][0])
+
+
+@pytest.mark.parametrize("form", ["plain64", "fused32"])
+def test_host_force_callback_matches_device_force_field(oracle, form):
+    """A host force provider (the reference's per-step LAMMPS round trip,
+    through the library's page-locked buffers) computing the same FENE + WCA
+    forces with the oracle's force field gives the steps of the device force
+    field: 1e-12 relative (the two sum the pair forces in another order)."""
+    wl = W.config(3, kT=0.0, nchains=4, length=25, grid=24, body=0.01, form=form)
+    wl.params.flagStochasticDriving = 0
+    p = wl.params
+    ff = oracle.ForceField(wl.topology.as_dict(), p.box_lo, p.box_hi)
+    calls = []
+
+    def host_forces(x, v):
+        calls.append(1)
+        f = ff.forces(x)
+        return f[0] if isinstance(f, tuple) else f
+
+    dev = _gpu_sim(wl)
+    host = Selm(p, wl.x, wl.mass, v=wl.v, topology=wl.topology)
+    host.set_force_callback(host_forces)
+    host.initial()
+    for _ in range(5):
+        dev.run(2)
+        host.run(2)
+        (xd, vd, fd), (xh, vh, fh) = dev.particles(), host.particles()
+        assert rel(xh, xd) < 1e-12 and rel(vh, vd) < 1e-12 and rel(fh, fd) < 1e-12
+    assert len(calls) >= 10 and host.status() == 0
