@@ -103,7 +103,8 @@ typedef struct selm_sim selm_sim;
 
 /* Host force provider, the role LAMMPS plays in the reference
  * (Lagrangian_LAMMPS::compute_f, cuda/SELM_Lagrangian_LAMMPS.cu:107-130):
- * called once per step with the new positions/velocities; writes f. */
+ * called once per step with the new positions/velocities; f arrives zeroed,
+ * so the provider may add into it or leave atoms without force untouched. */
 typedef int (*selm_force_fn)(void* user, int natoms, const double* x, const double* v, double* f);
 
 /* ---- lifecycle (Selm::Selm / initial / run / final) ---- */
@@ -147,7 +148,11 @@ int selm_get_particles(selm_sim* s, double* x, double* v, double* f);
  * atom->f after each reallocation) so that the per-step copies above run as
  * direct transfers (about 50 GB/s here) rather than through pageable staging
  * (about 19 GB/s).  The caller unregisters before freeing the memory.
- * Registering memory already registered is not an error. */
+ * Registering a range that is already wholly page-locked is not an error; a
+ * range that overlaps an earlier registration only in part (an array grown
+ * in place) returns SELM_ERR_STATE: unregister the old range first.
+ * selm_host_unregister undoes whatever registration starts at ptr, also one
+ * made by another component of the process (cudaHostUnregister). */
 int selm_host_register(void* ptr, unsigned long long bytes);
 int selm_host_unregister(void* ptr);
 /* t_f of the last inertial step, per monomer and component: the coupling
@@ -187,8 +192,11 @@ int selm_op_spread(int precision, const int dims[3], double lo, double dx, doubl
  * No counterpart in the reference.  Inputs and output are DEVICE pointers
  * (fgrid is double* for precision 64, float* for 32; x and tf are [M][3]
  * doubles); the call is ordered on `stream` (NULL = the legacy default stream).
- * Scratch is a fixed file-scope device array (about 4.5 MB): at most 65536
- * monomers and grids up to 128^3; larger sizes are rejected.  Calls that
+ * It accumulates, fgrid -= Lambda(tf), as selm_op_spread does: zero fgrid
+ * first for a fresh spread.  Scratch is a fixed file-scope device array
+ * (about 4.5 MB): at most 65536 monomers and 4096 spread tiles of 16x8x16
+ * cells, ceil(nx/16)*ceil(ny/8)*ceil(nz/16) (128^3 uses 1024); larger sizes
+ * are rejected.  Calls that
  * overlap on the GPU share that array and race.  The first call on a device
  * looks up the array's address; make it before any stream capture. */
 int selm_op_spread_noalloc(int precision, const int dims[3], double lo, double dx, void* fgrid, int natoms,

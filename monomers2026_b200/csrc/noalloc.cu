@@ -11,8 +11,12 @@
 // file-scope __device__ array of fixed size that every GPU loading this
 // library holds until the process exits.
 //
-// Limits: at most kNoAllocMaxAtoms monomers, kNoAllocMaxTiles spread tiles
-// (grids up to 128^3) and kNoAllocEntries tile entries per monomer (a monomer
+// The call accumulates: fgrid -= Lambda(tf), as selm_op_spread does; a caller
+// that wants a fresh spread zeroes fgrid first.
+//
+// Limits: at most kNoAllocMaxAtoms monomers, kNoAllocMaxTiles spread tiles of
+// 16x8x16 cells, ceil(nx/16)*ceil(ny/8)*ceil(nz/16) (128^3 uses 1024), and
+// kNoAllocEntries tile entries per monomer (a monomer
 // is filed under every tile its stencil reaches: at most 8 on grids whose
 // tiles span at least 5 cells per axis), about 4.5 MB in all.  All calls
 // share the one array, so calls whose work overlaps on the GPU (different streams, no ordering between them) race on
@@ -79,7 +83,8 @@ extern "C" int selm_op_spread_noalloc(int precision, const int dims[3], double l
   const BinSpec bs = spread_bin_spec(dims, lo, dx);
   const long nbk = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
   if (nbk > kNoAllocMaxTiles)
-    return selm_fail(SELM_ERR_INVALID, "selm_op_spread_noalloc: grid needs more than 4096 spread tiles (max 128^3)");
+    return selm_fail(SELM_ERR_INVALID, "selm_op_spread_noalloc: grid needs more than 4096 spread tiles of 16x8x16 cells "
+                      "(ceil(nx/16)*ceil(ny/8)*ceil(nz/16); 128^3 uses 1024)");
   const long per = spread_entries_per_monomer(bs);
   if (per > kNoAllocEntries)
     return selm_fail(SELM_ERR_INVALID, "selm_op_spread_noalloc: grid tiles too small for the fixed scratch");

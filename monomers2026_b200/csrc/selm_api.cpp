@@ -653,6 +653,9 @@ int engine_forces(selm_sim* s) {
     CU(cudaMemcpyAsync(hx, x, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
     CU(cudaMemcpyAsync(hv, s->v, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
     CU(cudaStreamSynchronize(s->st));
+    // the provider may add into f (LAMMPS clears f, then each style adds) or
+    // write only some atoms: it starts from zeros, as a fresh force array does
+    memset(hf, 0, sizeof(double) * n);
     const int r = s->cb(s->cb_user, s->M, hx, hv, hf);
     if (r != 0) return selm_fail(SELM_ERR_INVALID, "force callback returned an error");
     CU(cudaMemcpyAsync(s->f, hf, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
@@ -887,6 +890,17 @@ extern "C" int selm_host_register(void* ptr, unsigned long long bytes) {
   const cudaError_t e = cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault);
   if (e == cudaErrorHostMemoryAlreadyRegistered) {
     cudaGetLastError();
+    // already page-locked is fine only if the whole range is: an array that
+    // grew in place past an earlier registration keeps a pageable tail
+    unsigned int flags = 0;
+    const bool first = cudaHostGetFlags(&flags, ptr) == cudaSuccess;
+    cudaGetLastError();
+    const bool last = cudaHostGetFlags(&flags, static_cast<char*>(ptr) + (bytes - 1)) == cudaSuccess;
+    cudaGetLastError();
+    if (!first || !last)
+      return selm_fail(SELM_ERR_STATE,
+                       "selm_host_register: the range overlaps an earlier registration but is not wholly page-locked; "
+                       "unregister the earlier range first");
     return SELM_OK;
   }
   if (e != cudaSuccess) {

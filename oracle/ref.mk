@@ -4,7 +4,9 @@
 # shims, into oracle/_ref/libselm_ref.so.  TEST INFRASTRUCTURE ONLY.
 # Usage: make -f oracle/ref.mk
 HERE := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
-REF ?= /root/reference/data/src/selm-main/src/mpi
+# the reference project root comes from SELM_REFERENCE_ROOT (default /root/reference)
+SELM_REFERENCE_ROOT ?= /root/reference
+REF ?= $(SELM_REFERENCE_ROOT)/data/src/selm-main/src/mpi
 OUT := $(HERE)_ref/libselm_ref.so
 CXX := $(firstword $(wildcard /usr/bin/g++) g++)
 CC := $(firstword $(wildcard /usr/bin/gcc) gcc)

@@ -5,7 +5,7 @@ into a small fixture that pins the DCD layout: header, titles and atom count
 import os
 import sys
 
-SRC = os.path.join(sys.argv[1] if len(sys.argv) > 1 else "/root/reference",
+SRC = os.path.join(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SELM_REFERENCE_ROOT", "/root/reference"),
                    "data", "cases", "SELM", "DIffusion Coefficient", "1base.dcd")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "dcd_1base_head.dcd")
 buf = open(SRC, "rb").read()

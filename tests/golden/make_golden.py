@@ -96,7 +96,7 @@ def parse_case(d):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SELM_REFERENCE_ROOT", "/root/reference")
     case = os.path.join(ref_root, "data/src/selm-main/test/NucleotideMonomer")
     from oracle import refdriver
     if not refdriver.available():

@@ -16,7 +16,7 @@ import pytest
 from oracle import analysis as oa
 from monomers2026_b200.analysis import fit_line, wavevectors
 
-REF = "/root/reference/data/cases/SELM"
+REF = os.path.join(os.environ.get("SELM_REFERENCE_ROOT", "/root/reference"), "data/cases/SELM")
 
 
 def _traj(rng, F, M, L):

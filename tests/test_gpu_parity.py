@@ -480,6 +480,59 @@ def test_registered_host_arrays_round_trip():
         host_unregister(bufs[1][0])
 
 
+def test_host_register_refuses_a_partly_registered_range():
+    """An array that grew past an earlier registration (same start, larger
+    size) is refused, not reported as page-locked; the earlier range itself
+    registers again without error."""
+    from monomers2026_b200.selm import host_register, host_unregister
+    a = np.zeros(1 << 20)
+    head = a[: 1 << 18]
+    host_register(head)
+    with pytest.raises(RuntimeError):
+        host_register(a)
+    host_register(head)
+    host_unregister(head)
+    host_register(a)
+    host_unregister(a)
+
+
+def test_host_force_callback_may_add_into_f(oracle):
+    """The force array handed to a host provider starts at zero, so a
+    provider that adds its forces into f (as LAMMPS' styles do after clearing
+    it) steps exactly as one that overwrites f."""
+    from monomers2026_b200 import _lib
+    wl = W.config(3, kT=0.0, nchains=4, length=25, grid=24, body=0.01, form="fused32")
+    wl.params.flagStochasticDriving = 0
+    p = wl.params
+    ff = oracle.ForceField(wl.topology.as_dict(), p.box_lo, p.box_hi)
+
+    def forces(x):
+        f = ff.forces(x)
+        return f[0] if isinstance(f, tuple) else f
+
+    def adder(user, natoms, x, v, f):
+        xa = np.ctypeslib.as_array(x, (natoms, 3)).copy()
+        fa = np.ctypeslib.as_array(f, (natoms, 3))
+        fa += forces(xa)
+        return 0
+
+    sims = []
+    for mode in ("set", "add"):
+        s = Selm(p, wl.x, wl.mass, v=wl.v, topology=wl.topology)
+        if mode == "set":
+            s.set_force_callback(lambda x, v: forces(x))
+        else:
+            s._cb_keep = _lib.FORCE_FN(adder)
+            _lib.check(s._L.selm_set_force_callback(s._h, s._cb_keep, None))
+        s.initial()
+        sims.append(s)
+    for _ in range(4):
+        for s in sims:
+            s.run(2)
+        (x0, v0, f0), (x1, v1, f1) = sims[0].particles(), sims[1].particles()
+        assert np.array_equal(x0, x1) and np.array_equal(v0, v1) and np.array_equal(f0, f1)
+
+
 @pytest.mark.parametrize("form", ["plain64", "fused32"])
 def test_host_force_callback_matches_device_force_field(oracle, form):
     """A host force provider (the reference's per-step LAMMPS round trip,
