@@ -118,8 +118,15 @@ __device__ __forceinline__ void philox_normal2(const Key& key, uint32_t c0, uint
   z1 = r * s;
 }
 
-// FP32 Box-Muller pair from the same Philox block (24-bit open-interval
-// uniforms); used by the FP32 form, whose noise needs no more than FP32
+// FP32 Box-Muller pair from the same Philox block, the same normals as
+// philox_normal2 to FP32 precision.  The FP64 uniforms are u = (x + 1/2) 2^-52
+// with x = o0 2^20 + (o1 >> 12).  Rounding u to FP32 costs 2^-24 absolute,
+// which near u = 1 (radius sqrt(-2 ln u) ~ sqrt(2 (1 - u))) is a large
+// relative error of the radius; so for u >= 1/2 the complement 1 - u is built
+// from the complemented integer bits (exact to FP32 rounding, relative) and
+// -ln u = -log1p(-(1 - u)).  The angle 2 pi u2 is taken as pi t with the
+// signed t = 2 u2 (mod 2) in [-1, 1), through sincospif, so neither the
+// argument nor the evaluation loses more than an FP32 ulp.
 template <typename Key>
 __device__ __forceinline__ void philox_normal2_f32(const Key& key, uint32_t c0, uint32_t c1, uint64_t step, float& z0,
                                                    float& z1) {
@@ -128,13 +135,18 @@ __device__ __forceinline__ void philox_normal2_f32(const Key& key, uint32_t c0, 
     philox4x32_10(c0, c1, (uint32_t)step, (uint32_t)(step >> 32), key, o);
   else
     philox4x32_10(c0, c1, (uint32_t)step, (uint32_t)(step >> 32), (uint32_t)key, (uint32_t)(key >> 32), o);
-  const float u1 = ((float)(o[0] >> 8) + 0.5f) * (1.0f / 16777216.0f);
-  const float u2 = ((float)(o[2] >> 8) + 0.5f) * (1.0f / 16777216.0f);
-  // fast intrinsics: u1 in (0, 1] and the angle in [0, 2 pi) keep their
-  // errors near 1e-6, well inside what an FP32 noise field resolves
-  const float r = sqrtf(-2.0f * __logf(u1));
+  float nl;  // -ln u1
+  if (o[0] & 0x80000000u) {
+    const float d = fmaf((float)(~o[0]), 0x1p-32f, ((float)((~o[1]) >> 12) + 0.5f) * 0x1p-52f);
+    nl = -log1pf(-d);
+  } else {
+    const float u = fmaf((float)o[0], 0x1p-32f, ((float)(o[1] >> 12) + 0.5f) * 0x1p-52f);
+    nl = -logf(u);
+  }
+  const float r = sqrtf(2.0f * nl);
+  const float t = fmaf((float)(int32_t)o[2], 0x1p-31f, ((float)(o[3] >> 12) + 0.5f) * 0x1p-51f);
   float sn, cs;
-  __sincosf(6.283185307f * u2, &sn, &cs);
+  sincospif(t, &sn, &cs);
   z0 = r * cs;
   z1 = r * sn;
 }

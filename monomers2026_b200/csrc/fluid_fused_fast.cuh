@@ -202,8 +202,12 @@ struct ZGeom {
 // reference noise draw of a half-spectrum mode (cuda/SELM_Kernel.cu:56-79); the
 // amplitude sqrt(lambda_h) comes from the symbol tables (cm = cos - 1).  The
 // FP64 forms draw FP64 normals (same stream as the plain form) and scale them
-// in FP64; the FP32 form draws FP32 normals from the same Philox counters and
-// scales them in FP32.
+// in FP64; the caller multiplies by the prefactor noise_amp.  The FP32 form
+// draws FP32 normals from the same Philox counters (philox_normal2_f32, the
+// FP64 normals to FP32 precision) and scales them by the whole per-mode
+// amplitude noise_amp sqrt(lambda_h) (times 1/sqrt 2 for a complex draw),
+// which is formed in FP64 and rounded to FP32 once: the noise-variance
+// prefactor stays FP64 (cuda/SELM_Eulerian_Period.cu:141-148).
 template <typename T, int N>
 __device__ __forceinline__ void noise_draw_fast(const ZGeom& g, uint64_t step, int i, int j, int k, double cmx,
                                                 double cmy, double cmz, cpx<T> out[3]) {
@@ -222,9 +226,9 @@ __device__ __forceinline__ void noise_draw_fast(const ZGeom& g, uint64_t step, i
       out[d] = make_double2(z0 * re, z1 * im);
     }
   } else {
-    const float lam = (float)(-2.0 * (cmx + cmy + cmz) * g.idx2);
-    const float coef = sqrtf(fmaxf(lam, 0.0f));
-    const float re = selfc ? coef : coef * 0.70710678f;
+    const double lam = -2.0 * (cmx + cmy + cmz) * g.idx2;
+    const double amp = g.noise_amp * sqrt(fmax(lam, 0.0));
+    const float re = (float)(selfc ? amp : amp * 0.7071067811865476);
     const float im = selfc ? 0.0f : re;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -328,11 +332,19 @@ __global__ void __launch_bounds__(TPB, MINB) k_z_update_fast(cpx<T>* __restrict_
           for (int c = 0; c < 3; c++) Xn[c].y = T(0);
         }
       }
-      const T amp = (T)g.noise_amp;
+      if constexpr (sizeof(T) == 8) {
+        const T amp = (T)g.noise_amp;
 #pragma unroll
-      for (int c = 0; c < 3; c++) {
-        X[c].x += amp * Xn[c].x;
-        X[c].y += amp * Xn[c].y;
+        for (int c = 0; c < 3; c++) {
+          X[c].x += amp * Xn[c].x;
+          X[c].y += amp * Xn[c].y;
+        }
+      } else {  // FP32: the FP64 prefactor is already in the draw
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          X[c].x += Xn[c].x;
+          X[c].y += Xn[c].y;
+        }
       }
     }
     C un[3];
