@@ -458,10 +458,60 @@ __device__ __forceinline__ int axis_tile_set(double g, int a, const BinSpec& bs,
   return cnt;
 }
 
-// File monomer p under every spread tile its union stencil reaches: a slot
-// of the tile while it has room, else the overflow list.
+// Home cell of a grid coordinate along one axis: floor(g) wrapped into
+// [0, n), and whether frac(g) < 1/2 (the half-shifted stencil then starts two
+// cells below it, else one).  Non-finite or absurd coordinates count as 0, so
+// that tile and box indices stay in range (their impulses are non-finite
+// anyway, or the step has already flagged the displacement).
+__device__ __forceinline__ int home_cell(double g, int n, bool& low_half) {
+  if (!(fabs(g) < 1.0e9)) g = 0.0;
+  const double fl = floor(g);
+  low_half = (g - fl) < 0.5;
+  return wrapi((int)fl, n);
+}
+
+// Home mode: the coordinates, in the home tile's box (the tile plus 2 cells
+// on each side), of the stencil bases that the thread of component d stores
+// in the record (axis d unshifted, axis d+1 shifted; record_store's split, so
+// the three threads write distinct bytes).  With home cell c (tile origin t0)
+// the unshifted base floor(g) - 1 sits at c - t0 + 1, the shifted base
+// floor(g - 1/2) - 1 at c - t0 or c - t0 + 1: always in [0, tile], and the
+// 4 stencil points stay inside the box.
+__device__ __forceinline__ void home_box_store(unsigned char (&hb)[3][2], int d, double gx, double gy, double gz,
+                                               const BinSpec& bs) {
+  const double g[3] = {gx, gy, gz};
+  const int a1 = (d + 1) % 3;
+#pragma unroll
+  for (int ax = 0; ax < 3; ax++) {
+    if (ax == d || ax == a1) {
+      bool low;
+      const int c = home_cell(g[ax], bs.n[ax], low);
+      const int l = c % bs.tile[ax];
+      hb[ax][ax == d ? 0 : 1] = (unsigned char)((ax == d) ? l + 1 : (low ? l : l + 1));
+    }
+  }
+}
+
+// File monomer p under every spread tile its union stencil reaches (home
+// mode: under its home tile only): a slot of the tile while it has room,
+// else the overflow list.
 __device__ __forceinline__ void tile_append(const TileSlots& ts, int p, double gx, double gy, double gz, uint32_t* err) {
   const BinSpec& bs = ts.bs;
+  if (ts.home) {
+    bool lo_half;
+    const int cx = home_cell(gx, bs.n[0], lo_half), cy = home_cell(gy, bs.n[1], lo_half),
+              cz = home_cell(gz, bs.n[2], lo_half);
+    const int t = ((cz / bs.tile[2]) * bs.nb[1] + cy / bs.tile[1]) * bs.nb[0] + cx / bs.tile[0];
+    const int slot = atomicAdd(&ts.count[t], 1);
+    if (slot < ts.cap) {
+      ts.slots[(long)t * ts.cap + slot] = p;
+    } else {
+      const int q = atomicAdd(ts.ovf_count, 1);
+      if (q < ts.ovf_cap) ts.ovf[q] = make_int2(t, p);
+      else atomicOr(err, ERR_BUCKET_OVERFLOW);
+    }
+    return;
+  }
   if (!isfinite(gx)) gx = 0.0;
   if (!isfinite(gy)) gy = 0.0;
   if (!isfinite(gz)) gz = 0.0;
@@ -536,7 +586,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_interp_update(c
   T w[3][4];
   stencil_of<T>(gx, gy, gz, d, base, w);
   const T val = stencil_gather<T>(u + d * N, base, w, a);
-  if (rec) record_store<T>(rec[p], d, base, w, a);
+  if (rec) {
+    record_store<T>(rec[p], d, base, w, a);
+    if (ts.home) home_box_store(rec[p].hb, d, gx, gy, gz, ts.bs);
+  }
   if (ts.count && d == 0) tile_append(ts, p, gx, gy, gz, err);  // the spread of this step reads x_old
   const double vg = v[g];
   double t_f = -a.upsilon * (vg - (double)val) * a.dt;
@@ -578,6 +631,7 @@ __global__ void __launch_bounds__(256) k_qs_prepare(const double* __restrict__ x
   T w[3][4];
   stencil_of<T>(gx, gy, gz, d, base, w);
   record_store<T>(rec[p], d, base, w, a);
+  if (ts.home) home_box_store(rec[p].hb, d, gx, gy, gz, ts.bs);
   if (ts.count && d == 0) tile_append(ts, p, gx, gy, gz, err);
   tf_out[gid] = -f[gid] * inv_dv;
 }
@@ -971,6 +1025,300 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
   }
 }
 
+
+// ================================================================ FP32 spread by home tiles
+// Every monomer is filed once, under the tile of its cell; the block of a
+// tile adds its monomers' 3 x 64 stencil points into a shared-memory box of
+// the tile plus two cells on each side (20 x 12 x 20 cells per component:
+// the union of the staggered stencils of a monomer is 5 cells wide, from 2
+// below its cell to 2 above), writes the box to global memory, and
+// k_spread_fold sums the boxes that cover each cell in a fixed order.
+//
+// Accumulation: one warp per monomer and component, lane l adding the points
+// (ix, jy, kz) = (l & 3, (l >> 2) & 3, l >> 4) and (ix, jy, kz + 2) of the
+// 4^3 stencil.  Rows of the box are 20 words and planes 240 (= 16 mod 32), so
+// the 32 lanes of one atomic instruction hit 32 distinct banks wherever the
+// stencil sits.  Values are fixed point in one 32-bit word per cell, at a
+// per-tile scale 2^S: integer sums do not depend on the order of addition,
+// so the box, and the fold's fixed-order float sum of at most 8 boxes, repeat
+// bit for bit.
+//
+// Scale: with n monomers in the tile (k = ceil(log2 n)), the largest impulse
+// component m < 2^em and every weight factor <= 2^(ew/3) (ew = -3 when all
+// factors are <= 1/2, as the Peskin function is; 0 when the reference's
+// distance-2 factor of 1 occurs), a contribution is < 2^(em + ew + S) and a
+// cell's sum < n 2^(em + ew + S).  S = min(30 - k, 22) - em - ew keeps a
+// cell's sum below 2^30 (plus n/2 of rounding) and a contribution below 2^22,
+// the range of the float-to-integer rounding by adding 1.5 2^23.  That is a
+// step of 2^-25 of the tile's largest impulse for n <= 256.  Tiles of more
+// than 2048 monomers take the split path: one component at a time, two words
+// per cell (low word L = 32 - k bits, unsigned; high word signed), a step of
+// 2^-(62 - 2k - ew) of the largest impulse, below the FP32 rounding of the
+// products for k <= 16.
+constexpr int kHX = kTX + 4, kHY = kTY + 4, kHZ = kTZ + 4;
+constexpr int kHBox = kHX * kHY * kHZ;  // cells per component
+constexpr int kHomeThreads = 256;
+constexpr int kHomeWarps = kHomeThreads / 32;
+constexpr int kHomeSplitK = 11;  // single-word path for n <= 2^11
+static_assert(kHX % 32 == 20 && (kHX * kHY) % 32 == 16, "bank pattern of the box atomics");
+constexpr size_t kHomeSmem = sizeof(unsigned) * 3 * kHBox;  // 57,600 B
+
+__device__ __forceinline__ int round_small(float v) {  // rint(v) for |v| < 2^22
+  return __float_as_int(v + 12582912.0f) - 0x4B400000;
+}
+
+template <int SPLIT>
+__device__ __forceinline__ void home_add(const int* __restrict__ ids, int n_prim, int n_ovf, const TileSlots& ts, int tb,
+                                         int dsel, double scale, int L, unsigned* acc,
+                                         const double* __restrict__ tf, const WRec<float>* __restrict__ rec) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int ix = lane & 3, jy = (lane >> 2) & 3, kz = lane >> 4;
+  const int loff = (kz * kHY + jy) * kHX + ix;
+  auto one = [&](int p) {
+    const WRec<float>& R = rec[p];
+    const uint2 hbw = *reinterpret_cast<const uint2*>(&R.hb[0][0]);
+    const unsigned char* hb = reinterpret_cast<const unsigned char*>(&hbw);  // hb[ax * 2 + shifted]
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      if (SPLIT && d != dsel) continue;
+      const int sx = (d != 0), sy = (d != 1), sz = (d != 2);
+      const int bx = hb[0 + sx], by = hb[2 + sy], bz = hb[4 + sz];
+      const float wx = R.w[0][sx][ix], wy = R.w[1][sy][jy];
+      const float wz0 = R.w[2][sz][kz], wz1 = R.w[2][sz][kz + 2];
+      const float A = (float)(-tf[3L * p + d] * scale) * wy * wx;
+      const int slot = (SPLIT ? 0 : d * kHBox) + (bz * kHY + by) * kHX + bx + loff;
+      if (!SPLIT) {
+        atomicAdd(acc + slot, (unsigned)round_small(A * wz0));
+        atomicAdd(acc + slot + 2 * kHY * kHX, (unsigned)round_small(A * wz1));
+      } else {
+        // v = hi 2^L + lo, 0 <= lo < 2^L, split exactly in FP32, lo rounded
+        const float tL = ldexpf(1.0f, L), itL = ldexpf(1.0f, -L);
+        const float p0 = A * wz0, p1 = A * wz1;
+        const float h0 = floorf(p0 * itL), h1 = floorf(p1 * itL);
+        const float r0 = fmaf(-h0, tL, p0), r1 = fmaf(-h1, tL, p1);
+        int l0 = (int)rintf(r0), l1 = (int)rintf(r1);
+        int g0 = (int)h0, g1 = (int)h1;
+        if (l0 >= (1 << L)) { l0 -= (1 << L); g0 += 1; }  // r rounded up onto 2^L
+        if (l1 >= (1 << L)) { l1 -= (1 << L); g1 += 1; }
+        atomicAdd(acc + slot, (unsigned)l0);
+        atomicAdd(acc + kHBox + slot, (unsigned)g0);
+        atomicAdd(acc + slot + 2 * kHY * kHX, (unsigned)l1);
+        atomicAdd(acc + kHBox + slot + 2 * kHY * kHX, (unsigned)g1);
+      }
+    }
+  };
+  for (int c = wid; c < n_prim; c += kHomeWarps) one(ids[c]);
+  for (int q = wid; q < n_ovf; q += kHomeWarps) {
+    const int2 e = ts.ovf[q];
+    if (e.x == tb) one(e.y);
+  }
+}
+
+__global__ void __launch_bounds__(kHomeThreads) k_spread_home(const double* __restrict__ tf, TileSlots ts,
+                                                              const WRec<float>* __restrict__ rec) {
+  extern __shared__ __align__(16) unsigned hacc[];  // [3][kHZ][kHY][kHX], or [2][kHZ][kHY][kHX] (split path)
+  __shared__ double wmax[kHomeWarps];
+  __shared__ float wwm[kHomeWarps];
+  __shared__ int wbad[kHomeWarps];
+  const int tb = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int n = ts.count[tb];
+  const int n_prim = min(n, ts.cap);
+  const int* ids = ts.slots + (long)tb * ts.cap;
+  const int n_ovf = (n > n_prim) ? min(*ts.ovf_count, ts.ovf_cap) : 0;
+  float* out = ts.box + (long)tb * 3 * kHBox;
+  if (tid == 0) ts.live[tb] = (n > 0);
+  if (n > 0) {
+    // scale: largest impulse component and largest weight factor of the tile's monomers
+    double m = 0.0;
+    float wm = 0.0f;
+    int bad = 0;
+    auto see = [&](int p) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const double v = fabs(tf[3L * p + c]);
+        bad |= !(v <= 1.0e300);
+        m = fmax(m, v);
+      }
+      const float4* w4 = reinterpret_cast<const float4*>(&rec[p].w[0][0][0]);
+#pragma unroll
+      for (int r = 0; r < 6; r++) {
+        const float4 q = w4[r];
+        wm = fmaxf(wm, fmaxf(fmaxf(fabsf(q.x), fabsf(q.y)), fmaxf(fabsf(q.z), fabsf(q.w))));
+      }
+    };
+    for (int q = tid; q < n_prim; q += kHomeThreads) see(ids[q]);
+    for (int q = tid; q < n_ovf; q += kHomeThreads) {
+      const int2 e = ts.ovf[q];
+      if (e.x == tb) see(e.y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      wm = fmaxf(wm, __shfl_xor_sync(0xffffffffu, wm, o));
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) {
+      wmax[wid] = m;
+      wwm[wid] = wm;
+      wbad[wid] = bad;
+    }
+    // zero the accumulators meanwhile
+    uint4* z4 = reinterpret_cast<uint4*>(hacc);
+    for (int i = tid; i < 3 * kHBox / 4; i += kHomeThreads) z4[i] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
+#pragma unroll
+    for (int w = 0; w < kHomeWarps; w++) {
+      m = fmax(m, wmax[w]);
+      wm = fmaxf(wm, wwm[w]);
+      bad |= wbad[w];
+    }
+    if (bad) {
+      for (int i = tid; i < 3 * kHBox; i += kHomeThreads) out[i] = __int_as_float(0x7fc00000);
+    } else {
+      const int k = (n > 1) ? 32 - __clz(n - 1) : 1;  // ceil(log2 n)
+      const int ew = (wm <= 0.5f) ? -3 : 0;
+      int em = 0;
+      if (m > 0.0) frexp(m, &em);  // m < 2^em
+      if (k <= kHomeSplitK) {
+        const int S = max(-1000, min(1000, min(30 - k, 22) - em - ew));
+        home_add<0>(ids, n_prim, n_ovf, ts, tb, 0, ldexp(1.0, S), 0, hacc, tf, rec);
+        __syncthreads();
+        const double inv = ldexp(1.0, -S);
+        for (int i = tid; i < 3 * kHBox; i += kHomeThreads) out[i] = (float)((double)(int)hacc[i] * inv);
+      } else {
+        const int L = 32 - k;
+        const int S = max(-1000, min(1000, 62 - 2 * k - em - ew));
+        const double inv = ldexp(1.0, -S);
+        for (int d = 0; d < 3; d++) {
+          if (d > 0) {
+            __syncthreads();
+            for (int i = tid; i < 2 * kHBox / 4; i += kHomeThreads) z4[i] = make_uint4(0u, 0u, 0u, 0u);
+            __syncthreads();
+          }
+          home_add<1>(ids, n_prim, n_ovf, ts, tb, d, ldexp(1.0, S), L, hacc, tf, rec);
+          __syncthreads();
+          for (int i = tid; i < kHBox; i += kHomeThreads) {
+            const long long v = (long long)(int)hacc[kHBox + i] * (1ll << L) + (long long)hacc[i];
+            out[d * kHBox + i] = (float)((double)v * inv);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();  // every thread has read count[tb] and the overflow counter
+  if (tid == 0) {
+    ts.count[tb] = 0;
+    __threadfence();
+    if (atomicAdd(ts.done, 1u) == gridDim.x - 1) {  // the last block to finish: no block reads it any more
+      *ts.ovf_count = 0;
+      *ts.done = 0u;
+    }
+  }
+}
+
+// Boxes of the tiles along one axis that hold cell c: (tile, box coordinate)
+// pairs in a fixed order.  Tile t covers cells [t T, t T + e) (e = T but for
+// a partial last tile); its box holds coordinates 0 .. e + 3 for the cells
+// t T - 2 .. t T + e + 1, taken periodically.  Tiles up to two away are
+// looked at (a last tile of one cell lets the box two tiles away reach past
+// it); small grids can hold a cell twice in one box.
+struct BoxAxis {
+  int t[8], b[8];
+  int n;
+};
+__device__ __forceinline__ void box_axis(int c, int n, int T, int nb, BoxAxis& L) {
+  const int th = c / T;
+  L.n = 0;
+  int seen[5];
+#pragma unroll
+  for (int dt = -2; dt <= 2; dt++) {
+    int t = (th + dt) % nb;
+    if (t < 0) t += nb;
+    bool dup = false;
+#pragma unroll
+    for (int q = 0; q < dt + 2; q++) dup |= (seen[q] == t);
+    seen[dt + 2] = t;
+    if (dup) continue;
+    const int t0 = t * T, e = min(T, n - t0);
+#pragma unroll
+    for (int kk = -1; kk <= 1; kk++) {
+      const int bc = c - t0 + 2 + kk * n;
+      if (bc >= 0 && bc < e + 4 && L.n < 8) {
+        L.t[L.n] = t;
+        L.b[L.n] = bc;
+        L.n++;
+      }
+    }
+  }
+}
+
+// The same on grids of 3 or more tiles per axis, none narrower than 4 cells
+// (so no cell lies both in the lowest 2 and the highest 2 of its tile), in
+// registers: the home tile's box, and below (cells 0, 1 of the tile: the
+// previous tile's box) or above (the last 2 cells: the next tile's box).
+__device__ __forceinline__ int box_axis2(int c, int n, int T, int nb, int& t0, int& b0, int& t1, int& b1) {
+  const int th = c / T, l = c - th * T, e = min(T, n - th * T);
+  if (l < 2) {
+    t0 = (th == 0) ? nb - 1 : th - 1;
+    b0 = c - t0 * T + 2 + ((th == 0) ? n : 0);
+    t1 = th;
+    b1 = l + 2;
+    return 2;
+  }
+  t0 = th;
+  b0 = l + 2;
+  if (l >= e - 2) {
+    t1 = (th == nb - 1) ? 0 : th + 1;
+    b1 = l - e + 2;  // the next tile starts at th T + e
+    return 2;
+  }
+  return 1;
+}
+
+// f[d][z][y][x] (=, or +=) the sum over the boxes holding the cell, in a
+// fixed order (z, y, x entries nested); boxes of empty tiles are skipped.
+// GENERAL: any grid (lists in local memory); else box_axis2's grids.
+template <typename T, bool GENERAL>
+__global__ void __launch_bounds__(256) k_spread_fold(T* __restrict__ f, int accumulate, const float* __restrict__ box,
+                                                     const int* __restrict__ live, BinSpec bs) {
+  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y;
+  const int nx = bs.n[0], ny = bs.n[1], nz = bs.n[2];
+  const int z = blockIdx.z % nz, d = blockIdx.z / nz;
+  if (x >= nx || y >= ny) return;
+  float s = 0.0f;
+  if constexpr (GENERAL) {
+    BoxAxis Lx, Ly, Lz;
+    box_axis(x, nx, bs.tile[0], bs.nb[0], Lx);
+    box_axis(y, ny, bs.tile[1], bs.nb[1], Ly);
+    box_axis(z, nz, bs.tile[2], bs.nb[2], Lz);
+    for (int iz = 0; iz < Lz.n; iz++)
+      for (int iy = 0; iy < Ly.n; iy++)
+        for (int ix = 0; ix < Lx.n; ix++) {
+          const int t = (Lz.t[iz] * bs.nb[1] + Ly.t[iy]) * bs.nb[0] + Lx.t[ix];
+          if (!live[t]) continue;
+          s += __ldg(box + ((long)t * 3 + d) * kHBox + (Lz.b[iz] * kHY + Ly.b[iy]) * kHX + Lx.b[ix]);
+        }
+  } else {
+    int tx[2], bx[2], ty[2], by[2], tz[2], bz[2];
+    const int cx = box_axis2(x, nx, kTX, bs.nb[0], tx[0], bx[0], tx[1], bx[1]);
+    const int cy = box_axis2(y, ny, kTY, bs.nb[1], ty[0], by[0], ty[1], by[1]);
+    const int cz = box_axis2(z, nz, kTZ, bs.nb[2], tz[0], bz[0], tz[1], bz[1]);
+#pragma unroll
+    for (int iz = 0; iz < 2; iz++)
+#pragma unroll
+      for (int iy = 0; iy < 2; iy++)
+#pragma unroll
+        for (int ix = 0; ix < 2; ix++) {
+          if (iz >= cz || iy >= cy || ix >= cx) continue;
+          const int t = (tz[iz] * bs.nb[1] + ty[iy]) * bs.nb[0] + tx[ix];
+          if (!live[t]) continue;
+          s += __ldg(box + ((long)t * 3 + d) * kHBox + (bz[iz] * kHY + by[iy]) * kHX + bx[ix]);
+        }
+  }
+  T* dst = f + ((long)(d * nz + z) * ny + y) * nx + x;
+  *dst = accumulate ? (T)((double)*dst + (double)s) : (T)s;
+}
+
 BinSpec spread_bin_spec(const int dims[3], double lo, double dx) {
   BinSpec bs{};
   bs.mode = 2;
@@ -1036,6 +1384,23 @@ cudaError_t spread_slots(T* fgrid, bool accumulate, const double* x_old, const d
     return cudaErrorInvalidValue;
   cudaError_t e = spread_prepare_attributes();
   if (e != cudaSuccess) return e;
+  if constexpr (sizeof(T) == 4) {
+    if (ts.home) {
+      if (!ts.box || !ts.live || !rec) return cudaErrorInvalidValue;
+      k_spread_home<<<ntiles, kHomeThreads, kHomeSmem, st>>>(tf, ts, rec);
+      const dim3 fb(32, 8), fg((unsigned)((a.nx + 31) / 32), (unsigned)((a.ny + 7) / 8), (unsigned)(3 * a.nz));
+      bool regs = true;  // box_axis2 holds: 3 or more tiles per axis, none narrower than 4 cells
+      for (int ax = 0; ax < 3; ax++)
+        regs &= bs.nb[ax] >= 3 && (bs.n[ax] % bs.tile[ax] == 0 || bs.n[ax] % bs.tile[ax] >= 4);
+      if (regs)
+        k_spread_fold<T, false><<<fg, fb, 0, st>>>(fgrid, accumulate ? 1 : 0, ts.box, ts.live, bs);
+      else
+        k_spread_fold<T, true><<<fg, fb, 0, st>>>(fgrid, accumulate ? 1 : 0, ts.box, ts.live, bs);
+      count_launches(2);
+      return cudaGetLastError();
+    }
+  }
+  if (ts.home) return cudaErrorInvalidValue;
   k_spread_tiles<T><<<ntiles, kSpreadThreads, spread_smem<T>(), st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, nullptr,
                                                                   nullptr, ts, rec, a);
   count_launches(1);
@@ -1068,6 +1433,9 @@ cudaError_t spread_prepare_attributes() {
     return e;
   if ((e = cudaFuncSetAttribute((const void*)k_spread_tiles<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)spread_smem<double>())) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute((const void*)k_spread_home, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kHomeSmem)) != cudaSuccess)
     return e;
   if (dev >= 0 && dev < kMaxSpreadDevices) done[dev] = true;
   return cudaSuccess;

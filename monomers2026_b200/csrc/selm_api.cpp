@@ -240,18 +240,28 @@ static int alloc_bins(selm_sim* s, const BinSpec& bs, BinBuffers& bb, int M) {
 // Spread-tile slots: a tile holds four times its expected candidate count
 // (plus 64) before its further candidates go to the overflow list, which has
 // room for every entry a monomer can make.
+// FP32 grids file each monomer under its home tile only (home mode), with a
+// box buffer of the tiles' halo-extended boxes for the fold pass.
 static int alloc_slots(selm_sim* s, const BinSpec& bs, TileSlots& ts, int M) {
   const long ntiles = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
-  double per = 1.0;  // expected tiles a union stencil (5 cells per axis) reaches
-  for (int a = 0; a < 3; a++) per *= (bs.nb[a] == 1) ? 1.0 : 1.0 + 4.0 / bs.tile[a];
+  const bool home = (s->prm.form == SELM_FORM_FUSED32);
+  double per = 1.0;  // expected tiles a monomer is filed under (a union stencil is 5 cells per axis)
+  if (!home)
+    for (int a = 0; a < 3; a++) per *= (bs.nb[a] == 1) ? 1.0 : 1.0 + 4.0 / bs.tile[a];
   const double avg = (double)M * per / (double)ntiles;
   long cap = ((long)std::ceil(4.0 * avg) + 64 + 31) / 32 * 32;
   cap = std::max(128L, std::min(65536L, cap));
   ts = TileSlots{};
   ts.bs = bs;
   ts.cap = (int)cap;
-  ts.ovf_cap = (int)std::min<long>(2147483647L, (long)M * spread_entries_per_monomer(bs) + 1024);
+  ts.ovf_cap = (int)std::min<long>(2147483647L, (long)M * (home ? 1 : spread_entries_per_monomer(bs)) + 1024);
+  ts.home = home ? 1 : 0;
   int rc;
+  if (home) {
+    const long box = 3L * (bs.tile[0] + 4) * (bs.tile[1] + 4) * (bs.tile[2] + 4);
+    if ((rc = dalloc(s, &ts.box, ntiles * box))) return rc;
+    if ((rc = dalloc(s, &ts.live, ntiles))) return rc;
+  }
   if ((rc = dalloc(s, &ts.count, ntiles))) return rc;
   if ((rc = dalloc(s, &ts.slots, ntiles * cap))) return rc;
   if ((rc = dalloc(s, &ts.ovf, (size_t)ts.ovf_cap))) return rc;

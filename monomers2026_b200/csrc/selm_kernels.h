@@ -80,10 +80,19 @@ struct TileSlots {
   int ovf_cap = 0;
   unsigned* done = nullptr;   // [1] spread blocks finished; the last one resets ovf_count
   BinSpec bs{};               // the spread tiles (mode 2)
+  // home mode (FP32 grids): a monomer is filed once, under the tile of its
+  // cell floor((x - lo)/dx); the spread accumulates each tile's monomers into
+  // a box of the tile plus a 2-cell halo, written to box[], and a fold pass
+  // sums the boxes that cover each cell.  live[t] = tile t had monomers.
+  int home = 0;
+  float* box = nullptr;       // [ntiles][3][tile z + 4][tile y + 4][tile x + 4]
+  int* live = nullptr;        // [ntiles]
 };
 template <typename T> struct alignas(16) WRec {
   T w[3][2][4];  // weight factors [axis][unshifted, shifted][point] (16-byte aligned rows)
   int b[3][2];   // stencil bases wrapped into [0, n): [axis][unshifted, shifted]
+  // home mode: the bases' coordinates in the home tile's box, [axis][unshifted, shifted]
+  unsigned char hb[3][2];
 };
 // the bases of record 0 and the record stride in ints, for the binning kernels
 template <typename T> inline const int* wrec_bases(const WRec<T>* rec) {

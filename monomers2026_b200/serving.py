@@ -47,11 +47,15 @@ def estimate_device_bytes(params, natoms: int, pairs: bool = True) -> int:
     nb = [-(-n // t) for n, t in zip((nx, ny, nz), tile)]
     tiles = nb[0] * nb[1] * nb[2]
     M = max(1, int(natoms))
+    home = params.form == "fused32"  # FP32 grids: one filing per monomer, plus the tiles' halo boxes
     per = 1.0
-    for b, t in zip(nb, tile):
-        per *= 1.0 if b == 1 else 1.0 + 4.0 / t
+    if not home:
+        for b, t in zip(nb, tile):
+            per *= 1.0 if b == 1 else 1.0 + 4.0 / t
     cap = max(128, -(-(int(math.ceil(4.0 * M * per / tiles)) + 64) // 32) * 32)
-    slots = 4 * tiles * (cap + 1) + 8 * (27 * M + 1024)  # tile slots and the overflow list
+    slots = 4 * tiles * (cap + 1) + 8 * ((1 if home else 27) * M + 1024)  # tile slots and the overflow list
+    if home:
+        slots += tiles * (4 * 3 * (tile[0] + 4) * (tile[1] + 4) * (tile[2] + 4) + 4)
     # x (two buffers), v, f, tf, m, the staged upload of a per-step round trip, stencil records
     mono = M * (2 * 24 + 3 * 24 + 8 + 2 * 24 + (128 if s == 4 else 224)) + slots
     nl = 0
