@@ -359,6 +359,16 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu:
         log("CPU baseline")
         cpu = cpu_baseline(wl, budget_s=args.cpu_seconds)
+    acc = None
+    if rank == 0 and world == 1 and args.form == "fused32" and not args.no_forms:
+        log("FP32 against FP64 velocities")
+        acc = fp32_accuracy(wl, stream)
+        log(f"FP32 error: {acc}")
+    ref_gpu = xcheck = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        log("reference GPU step and cuFFT cross-check")
+        ref_gpu, xcheck = reference_gpu_baseline(wl, kern)
+        log(f"reference GPU: {ref_gpu and ref_gpu['ms_per_step']} ms/step; cuFFT: {xcheck}")
 
     if rank == 0:
         out = {
@@ -383,6 +393,9 @@ def run_ours(args, rank, world, local_rank):
             "interp_union_points": U,
             "roofline": roof,
             "cpu_baseline": cpu,
+            "fp32_vs_fp64_velocity_rel_err": acc,
+            "reference_gpu": ref_gpu,
+            "cufft_xcheck": xcheck,
             "e2e": e2e,
             "analysis_and_output": extras,
             "autotune": tuned,
@@ -495,6 +508,83 @@ def cpu_baseline(wl, budget_s=15.0):
     return {"value": value, "unit": "fluid-cell-steps/s", "cores": workers, "kind": kind,
             "sample": f"{workers} concurrent single-rank instances x {steps} full steps of the same workload "
                       f"({what}), {window:.1f} s from the first start to the last end"}
+
+
+def fp32_accuracy(wl, stream, marks=(1, 10, 100)):
+    """Relative velocity error of the FP32 fused form against the FP64 fused
+    form (which matches the reference's own code to 1e-12 per step) on the
+    headline workload, both started from the same state: monomer velocities
+    and the fluid velocity, each as max |v32 - v64| / max |v64|, after
+    `marks` steps; at kT = 1 (same Philox stream) and at kT = 0 with a body
+    force of 0.01.  Step 1 is the error of one step; later marks add the
+    growth of a chaotic trajectory (WCA collisions amplify any difference)."""
+    from dataclasses import replace
+
+    from monomers2026_b200.selm import Selm
+
+    def rel(a, b):
+        s = np.abs(b).max()
+        return float(np.abs(a - b).max() / (s if s > 0 else 1.0))
+
+    out = {}
+    topo0 = replace(wl.topology, body_force=(0.01, 0.0, 0.0))
+    cases = (("kT1", wl.params, wl.topology),
+             ("kT0_body", replace(wl.params, T=0.0, flagStochasticDriving=0), topo0))
+    for tag, prm, topo in cases:
+        sims = []
+        for form in ("fused64", "fused32"):
+            s = Selm(replace(prm, form=form, integrator="inertial"), wl.x, wl.mass, topology=topo)
+            s.set_stream(stream.cuda_stream)
+            s.initial()
+            sims.append(s)
+        rows = {"steps": list(marks), "v": [], "u": []}
+        done = 0
+        for m in marks:
+            for s in sims:
+                s.run(m - done)
+            done = m
+            (_, v64, _), (_, v32, _) = sims[0].particles(), sims[1].particles()
+            rows["v"].append(rel(v32, v64))
+            rows["u"].append(rel(sims[1].get_field(0), sims[0].get_field(0)))
+        for s in sims:
+            s.final()
+        out[tag] = rows
+    out["one_step_max"] = max(max(out[t]["v"][0], out[t]["u"][0]) for t in ("kT1", "kT0_body"))
+    return out
+
+
+def reference_gpu_baseline(wl, kern, steps=10):
+    """The reference's own GPU step (oracle/_ref/libselm_refgpu.so: its
+    cuda/SELM_Eulerian_Period.cu and cuda/SELM_Kernel.cu built unchanged for
+    sm_100a with a stub driver) on the same workload, the host LAMMPS force
+    call left out (the conservative force is held at zero), per phase with
+    CUDA events; and cuFFT's batched R2C + C2R of the three 128^3 fields
+    (FP32 and FP64) beside this library's three fluid kernels, whose FFTs
+    carry the spectral update as well.  A baseline, like cpu_baseline: not
+    part of this library's step."""
+    from oracle import refgpu
+    if not refgpu.available():
+        return None, None
+    n = wl.params.numMeshPtsPerDir[0]
+    r = refgpu.ReferenceGpuRun(wl)
+    r.step(3)
+    t = r.time(steps)
+    r.close()
+    N = n ** 3
+    ref = {"ms_per_step": t["step"], "kernels_ms": {k: round(v, 4) for k, v in t.items() if k != "step"},
+           "value": N / (t["step"] / 1e3), "unit": "fluid-cell-steps/s", "steps": steps,
+           "what": "reference cuda/ step (lagrangian_update with FP64 atomics, cuFFT D2Z/Z2D projection, "
+                   "CUB mean removal, cuRAND + cuFFT thermal forcing), host LAMMPS forces left out"}
+    fl = sum(kern.get(k, (0.0, 0))[0] for k in ("xy_forward", "z_update", "xy_inverse"))
+    x32 = refgpu.cufft_time(n, 32)
+    x64 = refgpu.cufft_time(n, 64)
+    xc = {"grid": n, "fields": 3,
+          "cufft_fp32_ms": {k: round(v, 4) for k, v in x32.items()},
+          "cufft_fp64_ms": {k: round(v, 4) for k, v in x64.items()},
+          "cufft_fp32_r2c_plus_c2r_ms": round(x32["r2c_ms"] + x32["c2r_ms"], 4),
+          "own_fluid_kernels_ms": round(fl, 4),
+          "note": "own = xy forward + z update (z FFTs, spectral update, noise) + xy inverse of the headline form"}
+    return ref, xc
 
 
 # --------------------------------------------------------------------------- reference arm

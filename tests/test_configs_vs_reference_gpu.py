@@ -1,0 +1,92 @@
+"""The configurations at their stated sizes, against the reference's own CPU
+code (oracle/_ref: mpi/SELM.cpp, SELM_Eulerian_Period.cpp and
+SELM_Lagrangian_LAMMPS.cpp compiled unchanged against single-rank shims).
+
+* Large single instance, deterministic check: 1000 FENE + WCA chains of 100
+  monomers (1e5) in L = 128 on a 128^3 grid, kT = 0, a uniform body force of
+  0.01 along x, dt = 0.005.  Per step the FP64 forms (plain64, fused64) agree
+  with the reference to 1e-12 relative (every field against its maximum:
+  positions, velocities, forces, fluid velocity); the FP32 form's velocities
+  (monomer and fluid) to 1e-5 relative, its positions to 1e-9.
+* Plain method, small: one harmonic chain of 20 monomers in L = 32 on a 32^3
+  grid, kT = 0, dt = 0.01, 1000 steps.  The FP64 forms agree with the
+  reference to 1e-12 at every 50th step through step 1000 (no chaotic pair
+  forces: the error does not grow).
+"""
+import numpy as np
+import pytest
+
+from monomers2026_b200 import workloads as W
+from monomers2026_b200.selm import Selm
+from oracle import refdriver
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not refdriver.available(), reason="oracle/_ref not built (needs the reference source)")]
+
+
+def rel(a, b):
+    s = np.abs(b).max()
+    return float(np.abs(a - b).max() / (s if s > 0 else 1.0))
+
+
+def _sim(wl, form):
+    from dataclasses import replace
+    s = Selm(replace(wl.params, form=form), wl.x, wl.mass, v=wl.v, topology=wl.topology)
+    s.initial()
+    return s
+
+
+def test_large_config_kT0_body_force_vs_reference_per_step():
+    wl = W.config(3, kT=0.0, body=0.01)
+    wl.params.flagStochasticDriving = 0
+    assert len(wl.mass) == 100000 and tuple(wl.params.numMeshPtsPerDir) == (128, 128, 128)
+    nsteps = 5
+    ref = refdriver.ReferenceRun(wl, nsteps=nsteps)
+    sims = {f: _sim(wl, f) for f in ("plain64", "fused64", "fused32")}
+    worst = {f: 0.0 for f in sims}
+    for k in range(1, nsteps + 1):
+        ref.step(1)
+        xr, vr, fr, ur = ref.state()
+        for form, s in sims.items():
+            s.run(1)
+            x, v, f = s.particles()
+            u = s.get_field(0)
+            if form == "fused32":
+                ev = max(rel(v, vr), rel(u, ur))
+                assert ev < 1e-5, f"step {k} {form}: velocity rel err {ev:.3e}"
+                assert rel(x, xr) < 1e-9
+                worst[form] = max(worst[form], ev)
+            else:
+                e = max(rel(x, xr), rel(v, vr), rel(f, fr), rel(u, ur))
+                assert e < 1e-12, f"step {k} {form}: rel err {e:.3e}"
+                worst[form] = max(worst[form], e)
+    for s in sims.values():
+        assert s.status() == 0
+        s.final()
+    ref.close()
+    print("worst per-step relative error vs the reference:", worst)
+
+
+def test_small_config_kT0_1000_steps_vs_reference():
+    wl = W.config(1, kT=0.0)
+    wl.params.flagStochasticDriving = 0
+    wl.v = np.random.default_rng(3).normal(0.0, 0.3, wl.x.shape)  # moving from the start
+    assert tuple(wl.params.numMeshPtsPerDir) == (32, 32, 32) and len(wl.mass) == 20
+    ref = refdriver.ReferenceRun(wl, nsteps=1000)
+    sims = {f: _sim(wl, f) for f in ("plain64", "fused64")}
+    growth = {f: [] for f in sims}
+    for k in range(20):
+        ref.step(50)
+        xr, vr, fr, ur = ref.state()
+        for form, s in sims.items():
+            s.run(50)
+            x, v, f = s.particles()
+            u = s.get_field(0)
+            e = max(rel(x, xr), rel(v, vr), rel(f, fr), rel(u, ur))
+            growth[form].append(e)
+            assert e < 1e-12, f"step {50 * (k + 1)} {form}: rel err {e:.3e}"
+    for s in sims.values():
+        assert s.status() == 0
+        s.final()
+    ref.close()
+    print("error every 50 steps:", {f: ["%.1e" % e for e in g] for f, g in growth.items()})
