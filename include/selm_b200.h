@@ -222,6 +222,18 @@ int selm_batch_add(selm_batch* b, selm_sim* s);    /* s initialised, fused form,
 int selm_batch_remove(selm_batch* b, selm_sim* s); /* waits for the batch's work */
 int selm_batch_step(selm_batch* b, int nsteps);    /* asynchronous, like selm_step */
 int selm_batch_size(selm_batch* b);
+/* Serving (the reference serves one job per process, cuda/main.cu:5-12).
+ * A job is a member with a step budget: it is stepped by the next nsteps
+ * calls of selm_batch_step and then leaves the step graphs.
+ * selm_batch_poll lists, without waiting, up to cap jobs whose budget is
+ * spent and whose last step has finished on the device (*ndone of them).
+ * selm_batch_retire removes such a job and reads back its x, v, f (any may
+ * be NULL) on the job's own stream, without waiting for the batch's later
+ * steps; SELM_ERR_STATE if its budget is not spent.  The simulation is not
+ * destroyed. */
+int selm_batch_add_job(selm_batch* b, selm_sim* s, long long nsteps);
+int selm_batch_poll(selm_batch* b, selm_sim** done, int cap, int* ndone);
+int selm_batch_retire(selm_batch* b, selm_sim* s, double* x, double* v, double* f);
 void* selm_batch_get_stream(selm_batch* b);
 int selm_batch_synchronize(selm_batch* b);
 int selm_batch_destroy(selm_batch* b); /* members leave (not destroyed) */

@@ -21,6 +21,7 @@ EXPORTED = [
     "selm_last_error", "selm_version",
     "selm_batch_create", "selm_batch_add", "selm_batch_remove", "selm_batch_step", "selm_batch_size",
     "selm_batch_get_stream", "selm_batch_synchronize", "selm_batch_destroy", "selm_device_bytes",
+    "selm_batch_add_job", "selm_batch_poll", "selm_batch_retire",
     "selm_tune_set", "selm_tune_get", "selm_tune_default",
     "selm_dcd_open", "selm_dcd_open_sim", "selm_dcd_write", "selm_dcd_write_sim", "selm_dcd_close", "selm_case_dump",
     "selm_analysis_create", "selm_analysis_sample", "selm_analysis_msd", "selm_analysis_structure",
@@ -104,6 +105,9 @@ def load():
     L.selm_batch_get_stream.restype = vp
     L.selm_batch_synchronize.argtypes = [vp]
     L.selm_batch_destroy.argtypes = [vp]
+    L.selm_batch_add_job.argtypes = [vp, vp, C.c_longlong]
+    L.selm_batch_poll.argtypes = [vp, C.POINTER(vp), C.c_int, C.POINTER(C.c_int)]
+    L.selm_batch_retire.argtypes = [vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.selm_device_bytes.argtypes = [vp, C.POINTER(C.c_ulonglong)]
     L.selm_host_register.argtypes = [vp, C.c_ulonglong]
     L.selm_host_unregister.argtypes = [vp]

@@ -22,6 +22,13 @@
 // is stepped only through its batch.  The kernels, buffers and Philox counters
 // are the member's own, so its results are the same bit for bit whether it
 // steps alone or in a batch.
+//
+// Jobs (serving): a member added with a step budget leaves the step graphs
+// once the budget is spent (its group is rebuilt at the next step), and an
+// event recorded after its last step tells selm_batch_poll, without waiting,
+// when its state is final.  selm_batch_retire then reads it back on the
+// member's own stream, so the read-back does not wait for the batch's later
+// steps.
 #include <algorithm>
 #include <string>
 #include <vector>
@@ -38,7 +45,9 @@ struct selm_batch {
     selm_sim* s;
     cudaStream_t st;  // the member's own stream, restored when it leaves
     bool own_st;
-    int group;
+    int group;               // -1: a job whose budget is spent (no longer stepped)
+    long long left = -1;     // steps left of a job's budget (-1: no budget)
+    cudaEvent_t done = nullptr;  // recorded after a job's last step
   };
   struct Group {
     cudaStream_t st = nullptr;
@@ -111,6 +120,8 @@ static void restore(selm_batch::Member& m) {
   m.s->st = m.st;
   m.s->own_st = m.own_st;
   m.s->batch = nullptr;
+  if (m.done) cudaEventDestroy(m.done);
+  m.done = nullptr;
 }
 
 int batch_detach(selm_sim* s) {
@@ -154,7 +165,7 @@ extern "C" int selm_batch_create(void* stream, selm_batch** out) {
   return SELM_OK;
 }
 
-extern "C" int selm_batch_add(selm_batch* b, selm_sim* s) {
+static int batch_join(selm_batch* b, selm_sim* s, long long budget) {
   if (!b || !s) return selm_fail(SELM_ERR_INVALID, "NULL argument");
   if (s->batch) return selm_fail(SELM_ERR_STATE, "the simulation already belongs to a batch");
   if (!s->fz) return selm_fail(SELM_ERR_STATE, "only the fused forms step in a batch");
@@ -167,14 +178,29 @@ extern "C" int selm_batch_add(selm_batch* b, selm_sim* s) {
   int gi = 0;
   for (int i = 1; i < kGroups; i++)
     if (b->groups[i].size < b->groups[gi].size) gi = i;
-  b->members.push_back({s, s->st, s->own_st, gi});
+  selm_batch::Member m{s, s->st, s->own_st, gi};
+  if (budget >= 0) {
+    m.left = budget;
+    e = cudaEventCreateWithFlags(&m.done, cudaEventDisableTiming);
+    if (e != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("cudaEventCreate: ") + cudaGetErrorString(e));
+  }
+  b->members.push_back(m);
   b->groups[gi].size++;
   b->groups[gi].dirty = true;
   s->st = b->st;
   s->own_st = false;
   s->batch = b;
+  s->ready_early = false;  // no early read-back events in a batch's step graphs
   fused_invalidate_graphs(s);  // a member's step is captured on one stream
+  if (budget == 0) cudaEventRecord(b->members.back().done, b->st);  // nothing to step: final at once
   return SELM_OK;
+}
+
+extern "C" int selm_batch_add(selm_batch* b, selm_sim* s) { return batch_join(b, s, -1); }
+
+extern "C" int selm_batch_add_job(selm_batch* b, selm_sim* s, long long nsteps) {
+  if (nsteps < 0) return selm_fail(SELM_ERR_INVALID, "selm_batch_add_job: nsteps < 0");
+  return batch_join(b, s, nsteps);
 }
 
 extern "C" int selm_batch_remove(selm_batch* b, selm_sim* s) {
@@ -185,8 +211,10 @@ extern "C" int selm_batch_remove(selm_batch* b, selm_sim* s) {
   const int gi = it->group;
   restore(*it);
   b->members.erase(it);
-  b->groups[gi].size--;
-  b->groups[gi].dirty = true;
+  if (gi >= 0) {
+    b->groups[gi].size--;
+    b->groups[gi].dirty = true;
+  }
   fused_invalidate_graphs(s);  // alone again: the step with the side stream
   if (e != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
   return SELM_OK;
@@ -197,6 +225,13 @@ extern "C" int selm_batch_step(selm_batch* b, int nsteps) {
   if (nsteps < 0) return selm_fail(SELM_ERR_INVALID, "nsteps < 0");
   if (b->members.empty() || nsteps == 0) return SELM_OK;
   for (int i = 0; i < nsteps; i++) {
+    // jobs whose budget is spent leave the step graphs
+    for (auto& m : b->members)
+      if (m.left == 0 && m.group >= 0) {
+        b->groups[m.group].size--;
+        b->groups[m.group].dirty = true;
+        m.group = -1;
+      }
     int active = 0;
     for (int gi = 0; gi < kGroups; gi++) {
       selm_batch::Group& G = b->groups[gi];
@@ -228,10 +263,53 @@ extern "C" int selm_batch_step(selm_batch* b, int nsteps) {
     }
     if (e != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     selm::count_launches((unsigned)k);
-    for (auto& m : b->members) fused_step_taken(m.s);
+    for (auto& m : b->members) {
+      if (m.group < 0) continue;
+      fused_step_taken(m.s);
+      if (m.left > 0 && --m.left == 0) {
+        e = cudaEventRecord(m.done, b->st);
+        if (e != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("cudaEventRecord: ") + cudaGetErrorString(e));
+      }
+    }
     for (auto& G : b->groups)
       if (G.size > 0) G.phase ^= 1;
   }
+  return SELM_OK;
+}
+
+extern "C" int selm_batch_poll(selm_batch* b, selm_sim** done, int cap, int* ndone) {
+  if (!b || !ndone || (cap > 0 && !done)) return selm_fail(SELM_ERR_INVALID, "NULL argument");
+  int n = 0;
+  for (auto& m : b->members) {
+    if (m.left != 0 || !m.done) continue;
+    const cudaError_t q = cudaEventQuery(m.done);
+    if (q == cudaErrorNotReady) continue;
+    if (q != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("cudaEventQuery: ") + cudaGetErrorString(q));
+    if (n < cap) done[n] = m.s;
+    n++;
+  }
+  *ndone = n < cap ? n : cap;
+  return SELM_OK;
+}
+
+extern "C" int selm_batch_retire(selm_batch* b, selm_sim* s, double* x, double* v, double* f) {
+  if (!b || !s) return selm_fail(SELM_ERR_INVALID, "NULL argument");
+  auto it = std::find_if(b->members.begin(), b->members.end(), [&](const selm_batch::Member& m) { return m.s == s; });
+  if (it == b->members.end()) return selm_fail(SELM_ERR_INVALID, "the simulation is not in this batch");
+  if (it->left != 0) return selm_fail(SELM_ERR_STATE, "selm_batch_retire: the job's step budget is not spent");
+  // its last step is final once the event has completed; the batch's later steps
+  // do not touch it (it left the step graphs), so its own stream reads it back
+  cudaError_t e = cudaEventSynchronize(it->done);
+  if (e != cudaSuccess) return selm_fail(SELM_ERR_CUDA, std::string("cudaEventSynchronize: ") + cudaGetErrorString(e));
+  const int gi = it->group;
+  restore(*it);
+  b->members.erase(it);
+  if (gi >= 0) {
+    b->groups[gi].size--;
+    b->groups[gi].dirty = true;
+  }
+  fused_invalidate_graphs(s);
+  if (x || v || f) return selm_get_particles(s, x, v, f);
   return SELM_OK;
 }
 

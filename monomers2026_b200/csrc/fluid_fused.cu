@@ -595,15 +595,7 @@ extern "C" int selm_tune_get(selm_sim* s, int knob, int* value) {
 template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
   using C = cpx<T>;
   const long N = s->N, N2 = s->N2;
-  auto al = [&](void** p, size_t bytes) -> int {
-    if (cudaMalloc(p, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return selm_fail(SELM_ERR_NOMEM, "cudaMalloc failed (fused form)");
-    }
-    s->allocs.push_back(*p);
-    s->dev_bytes += bytes;
-    return SELM_OK;
-  };
+  auto al = [&](void** p, size_t bytes) -> int { return sim_alloc(s, p, bytes); };
   int rc;
   if ((rc = al(&z->u, sizeof(T) * 3 * N))) return rc;
   if ((rc = al(&z->fp, sizeof(T) * 3 * N))) return rc;

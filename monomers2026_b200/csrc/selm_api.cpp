@@ -12,6 +12,7 @@
 #include <cstring>
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -44,22 +45,74 @@ int selm_fail(int code, const std::string& msg) {
   } while (0)
 
 // ================================================================ allocation
-template <typename T> static int dalloc(selm_sim* s, T** p, size_t n) {
+// A simulation's device memory comes from one stream-ordered pool per device
+// (cudaMallocFromPoolAsync on the simulation's stream, cudaFreeAsync when it
+// is destroyed).  cudaMalloc and cudaFree synchronise the whole device, so a
+// serving loop that creates and retires simulations while a batch runs
+// would wait for the batch at every admission and retirement; from the pool
+// neither call waits for other streams' work.  The pool keeps freed memory
+// for the next simulation (release threshold: never), so a steady stream of
+// jobs reuses the same memory.  Each allocation waits for its own stream
+// only (idle at creation), so the synchronous copies and sets that
+// initialise the buffers see them allocated.
+namespace {
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxPoolDevices] = {};
+}  // namespace
+
+static cudaError_t device_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxPoolDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if ((e = cudaMemPoolCreate(&pool, &props)) != cudaSuccess) return e;
+    uint64_t keep = UINT64_MAX;
+    if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+    g_pool[dev] = pool;
+  }
+  *out = g_pool[dev];
+  return cudaSuccess;
+}
+
+int sim_alloc(selm_sim* s, void** p, size_t bytes) {
   *p = nullptr;
-  if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * n);
+  if (bytes == 0) bytes = 1;
+  cudaMemPool_t pool = nullptr;
+  cudaError_t e = device_pool(&pool);
+  if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes, pool, s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    return selm_fail(SELM_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    if (*p) cudaFreeAsync(*p, s->st);
+    *p = nullptr;
+    return selm_fail(SELM_ERR_NOMEM, std::string("device allocation failed: ") + cudaGetErrorString(e));
   }
-  s->allocs.push_back(*p);
-  s->dev_bytes += sizeof(T) * n;
+  s->pool_allocs.push_back(*p);
+  s->dev_bytes += bytes;
   return SELM_OK;
+}
+
+template <typename T> static int dalloc(selm_sim* s, T** p, size_t n) {
+  return sim_alloc(s, reinterpret_cast<void**>(p), sizeof(T) * (n ? n : 1));
 }
 
 static void free_all(std::vector<void*>& v) {
   for (void* p : v) cudaFree(p);
   v.clear();
+}
+
+// ordered after everything queued on the simulation's stream so far
+static void sim_free_all(selm_sim* s) {
+  for (void* p : s->pool_allocs) cudaFreeAsync(p, s->st);
+  s->pool_allocs.clear();
 }
 
 // ================================================================ FFT tables
@@ -83,8 +136,9 @@ template <typename C> static std::vector<C> twiddles(int n, int sign) {
   return w;
 }
 
+// allocs (s NULL: cudaMalloc, freed by the caller) or the simulation's pool
 template <typename T>
-static int make_tables(std::vector<void*>& allocs, const int dims[3], FftTables<T>& tb) {
+static int make_tables(std::vector<void*>& allocs, const int dims[3], FftTables<T>& tb, selm_sim* s = nullptr) {
   using C = cpx<T>;
   const int n[3] = {dims[0], dims[1], dims[2]};
   const C* ptr[6];
@@ -92,8 +146,12 @@ static int make_tables(std::vector<void*>& allocs, const int dims[3], FftTables<
     for (int sgn = 0; sgn < 2; sgn++) {
       auto w = twiddles<C>(n[a], sgn == 0 ? -1 : 1);
       C* d = nullptr;
-      if (cudaMalloc((void**)&d, sizeof(C) * n[a]) != cudaSuccess) return SELM_ERR_NOMEM;
-      allocs.push_back(d);
+      if (s) {
+        if (sim_alloc(s, (void**)&d, sizeof(C) * n[a])) return SELM_ERR_NOMEM;
+      } else {
+        if (cudaMalloc((void**)&d, sizeof(C) * n[a]) != cudaSuccess) return SELM_ERR_NOMEM;
+        allocs.push_back(d);
+      }
       if (cudaMemcpy(d, w.data(), sizeof(C) * n[a], cudaMemcpyHostToDevice) != cudaSuccess) return SELM_ERR_CUDA;
       ptr[2 * a + sgn] = d;
     }
@@ -198,8 +256,8 @@ int engine_allocate_grid(selm_sim* s) {
   if ((rc = dalloc(s, &s->err, 1))) return rc;
   CU(cudaMemset(s->err, 0, sizeof(uint32_t)));
   CU(spread_prepare_attributes());
-  if ((rc = make_tables<double>(s->allocs, s->prm.num_mesh_pts, s->tb64))) return selm_fail(rc, "FFT tables");
-  if ((rc = make_tables<float>(s->allocs, s->prm.num_mesh_pts, s->tb32))) return selm_fail(rc, "FFT tables");
+  if ((rc = make_tables<double>(s->allocs, s->prm.num_mesh_pts, s->tb64, s))) return selm_fail(rc, "FFT tables");
+  if ((rc = make_tables<float>(s->allocs, s->prm.num_mesh_pts, s->tb32, s))) return selm_fail(rc, "FFT tables");
   if (s->prm.form == SELM_FORM_PLAIN64) {
     if ((rc = dalloc(s, &s->u64[0], 3 * N))) return rc;
     if ((rc = dalloc(s, &s->u64[1], 3 * N))) return rc;
@@ -775,6 +833,7 @@ extern "C" int selm_destroy(selm_sim* s) {
   analysis_detach_all(s);
   fused_release(s);
   free_all(s->allocs);
+  sim_free_all(s);
   if (s->hstage_cnt) cudaFreeHost(s->hstage_cnt);
   if (s->hcb) cudaFreeHost(s->hcb);
   if (s->own_st && s->st) cudaStreamDestroy(s->st);

@@ -37,7 +37,8 @@ struct selm_sim {
   cudaEvent_t ev_xv = nullptr, ev_ready = nullptr;
   cudaStream_t st_copy = nullptr;
   bool ready_early = false;
-  std::vector<void*> allocs;
+  std::vector<void*> allocs;       // cudaMalloc'd (freed with cudaFree)
+  std::vector<void*> pool_allocs;  // from the library's stream-ordered pool (sim_alloc)
   unsigned long long dev_bytes = 0;  // device bytes allocated for this simulation
   selm_batch* batch = nullptr;       // the batch this simulation steps in, if any
   std::vector<selm_analysis*> analyses;  // released with the simulation
@@ -84,6 +85,8 @@ struct selm_sim {
 };
 
 int selm_fail(int code, const std::string& msg);
+// device memory of simulation s from the library's stream-ordered pool, on s->st
+int sim_alloc(selm_sim* s, void** p, size_t bytes);
 void prof_mark(selm_sim* s, const char* name, bool begin);
 int engine_allocate_grid(selm_sim* s);
 int engine_forces(selm_sim* s);

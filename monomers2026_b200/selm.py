@@ -290,6 +290,31 @@ class Batch:
 
     step = run
 
+    def add_job(self, sim: Selm, nsteps: int) -> None:
+        """A member with a step budget (selm_batch_add_job)."""
+        check(self._L.selm_batch_add_job(self._h, sim._h, int(nsteps)))
+        sim._batch = self
+        self._members.append(sim)
+
+    def poll(self) -> list:
+        """Jobs whose budget is spent and whose last step has finished (no wait)."""
+        cap = max(1, len(self._members))
+        arr = (C.c_void_p * cap)()
+        n = C.c_int()
+        check(self._L.selm_batch_poll(self._h, arr, cap, C.byref(n)))
+        by_h = {m._h.value: m for m in self._members}
+        return [by_h[arr[i]] for i in range(n.value)]
+
+    def retire(self, sim: Selm):
+        """Remove a finished job and read back its x, v, f on its own stream."""
+        x = np.zeros((sim.M, 3))
+        v = np.zeros((sim.M, 3))
+        f = np.zeros((sim.M, 3))
+        check(self._L.selm_batch_retire(self._h, sim._h, _dp(x), _dp(v), _dp(f)))
+        sim._batch = None
+        self._members.remove(sim)
+        return x, v, f
+
     def __len__(self) -> int:
         return int(self._L.selm_batch_size(self._h))
 

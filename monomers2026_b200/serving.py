@@ -13,12 +13,20 @@ launch per step (``Batch``):
   HBM budget, adds them to the running batch between steps, and retires each
   job when its steps are done (state read back, memory freed): continuous
   batching.  A job's result does not depend on what else is in the batch
-  (each member keeps its own buffers and Philox counters).
+  (each member keeps its own buffers and Philox counters).  The host stays
+  off the step's critical path: simulations are created on a worker thread
+  while the batch steps, a job carries its step budget into the batch
+  (selm_batch_add_job), finished jobs are found by an event query
+  (selm_batch_poll) and read back on their own stream (selm_batch_retire),
+  and device memory comes from the library's stream-ordered pool, so neither
+  creation nor release waits for the batch.
 """
 from __future__ import annotations
 
 import dataclasses
 import math
+import queue as _queue
+import threading
 import time
 from collections import deque
 
@@ -148,6 +156,7 @@ class Job:
     x: np.ndarray | None = None
     v: np.ndarray | None = None
     status: int = 0
+    est_bytes: int = 0
 
 
 class Server:
@@ -169,56 +178,82 @@ class Server:
         import torch
 
         stream = torch.cuda.ExternalStream(self.batch.stream)
+        dev = torch.cuda.current_device()
         pending = deque(sorted(jobs, key=lambda j: j.arrival))
-        queue: deque = deque()
-        active: list = []  # (job, sim, steps done, bytes)
+        waiting: deque = deque()  # arrived, not yet admitted
+        todo: _queue.Queue = _queue.Queue()  # admitted: created by the worker
+        ready: _queue.Queue = _queue.Queue()  # (job, sim or exception)
+        creating = 0
+        active: dict = {}  # sim handle -> (job, sim)
         step_ev = []
         finished = []
+
+        def worker():
+            torch.cuda.set_device(dev)
+            while True:
+                j = todo.get()
+                if j is None:
+                    return
+                try:
+                    ready.put((j, _make(j.workload, self.form)))
+                except Exception as e:  # reported by the loop
+                    ready.put((j, e))
+
+        th = threading.Thread(target=worker, daemon=True)
+        th.start()
         t0 = time.perf_counter()
-        while pending or queue or active:
-            now = time.perf_counter() - t0
-            if now > max_seconds:
-                raise RuntimeError("serving run exceeded its time bound")
-            while pending and pending[0].arrival <= now:
-                queue.append(pending.popleft())
-            while queue:
-                j = queue[0]
-                est = estimate_device_bytes(dataclasses.replace(j.workload.params, form=self.form),
-                                            len(j.workload.mass))
-                if self.used + est > self.budget and active:
-                    break
-                queue.popleft()
-                s = _make(j.workload, self.form)
-                nb = s.device_bytes()
-                self.used += nb
-                self.peak = max(self.peak, self.used)
-                self.batch.add(s)
-                j.admitted = time.perf_counter() - t0
-                active.append([j, s, 0, nb])
-            if not active:
-                if pending:
-                    time.sleep(max(0.0, min(0.01, pending[0].arrival - (time.perf_counter() - t0))))
-                continue
-            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            self.batch.run(1)
-            e.record(stream)
-            step_ev.append((a, e, len(active)))
-            keep = []
-            for rec in active:
-                rec[2] += 1
-                j, s, k, nb = rec
-                if k >= j.nsteps:
-                    j.x, j.v, _ = s.particles()  # waits for the batch's work
+        try:
+            while pending or waiting or creating or active:
+                now = time.perf_counter() - t0
+                if now > max_seconds:
+                    raise RuntimeError("serving run exceeded its time bound")
+                while pending and pending[0].arrival <= now:
+                    waiting.append(pending.popleft())
+                # admission by the HBM budget, first come first served; creation on the worker
+                while waiting:
+                    j = waiting[0]
+                    est = estimate_device_bytes(dataclasses.replace(j.workload.params, form=self.form),
+                                                len(j.workload.mass))
+                    if self.used + est > self.budget and (active or creating):
+                        break
+                    waiting.popleft()
+                    self.used += est
+                    self.peak = max(self.peak, self.used)
+                    j.est_bytes = est
+                    creating += 1
+                    todo.put(j)
+                # jobs created since the last step join the batch with their budgets
+                while True:
+                    try:
+                        j, s = ready.get_nowait()
+                    except _queue.Empty:
+                        break
+                    creating -= 1
+                    if isinstance(s, Exception):
+                        raise s
+                    self.batch.add_job(s, j.nsteps)
+                    j.admitted = time.perf_counter() - t0
+                    active[s._h.value] = (j, s)
+                if not active:
+                    time.sleep(0.0005)
+                    continue
+                a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                self.batch.run(1)
+                e.record(stream)
+                step_ev.append((a, e, len(active)))
+                # finished jobs: an event query, then a read-back on the job's own stream
+                for s in self.batch.poll():
+                    j, _ = active.pop(s._h.value)
+                    j.x, j.v, _f = self.batch.retire(s)
                     j.status = s.status()
                     j.done = time.perf_counter() - t0
-                    self.batch.remove(s)
                     s.final()
-                    self.used -= nb
+                    self.used -= j.est_bytes
                     finished.append(j)
-                else:
-                    keep.append(rec)
-            active = keep
+        finally:
+            todo.put(None)
+            th.join(timeout=30)
         self.batch.synchronize()
         per = [a.elapsed_time(e) for a, e, _ in step_ev]
         wall = time.perf_counter() - t0

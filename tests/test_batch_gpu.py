@@ -183,3 +183,35 @@ def test_estimate_covers_device_bytes():
         est = estimate_device_bytes(wl.params, M)
         assert s.device_bytes() <= est < 3 * s.device_bytes() + (8 << 20), (n, M, s.device_bytes(), est)
         s.final()
+
+
+def test_jobs_poll_and_retire_match_alone():
+    """Jobs with step budgets (selm_batch_add_job): each leaves the step
+    graphs when its budget is spent, selm_batch_poll reports it once its last
+    step has finished, and selm_batch_retire reads it back on its own stream;
+    the states equal the same simulations stepped alone, bit for bit.  A job
+    whose budget is not spent cannot be retired."""
+    wls = [W.replica(16, 1, 40, 1.0, 801), W.replica(24, 1, 120, 0.7, 802), W.replica(16, 2, 30, 1.5, 803)]
+    budgets = [3, 7, 5]
+    b = Batch()
+    sims = [_sim(w) for w in wls]
+    for s, n in zip(sims, budgets):
+        b.add_job(s, n)
+    with pytest.raises(RuntimeError):
+        b.retire(sims[0])
+    got = {}
+    for _ in range(12):
+        b.run(1)
+        b.synchronize()
+        for s in b.poll():
+            got[sims.index(s)] = b.retire(s)
+    assert sorted(got) == [0, 1, 2] and len(b) == 0
+    for i, (w, n) in enumerate(zip(wls, budgets)):
+        alone = _sim(w)
+        alone.run(n)
+        x, v, f = alone.particles()
+        assert np.array_equal(x, got[i][0]) and np.array_equal(v, got[i][1]) and np.array_equal(f, got[i][2]), i
+        alone.final()
+        assert sims[i].status() == 0
+        sims[i].final()
+    b.final()
