@@ -614,6 +614,121 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_interp_update(c
   if (!isfinite(vn) || !isfinite(tx)) atomicOr(err, ERR_NONFINITE);
 }
 
+
+// The FP32 form's interpolation and monomer update with four threads per
+// (monomer, component): thread q of a quad gathers z-plane q of the 4^3
+// stencil (4 rows of 4 points, loaded as two aligned 16-byte vectors each,
+// all 8 loads issued before any arithmetic), and the four plane sums combine
+// by two shuffles (the same sum on every lane: (s0+s1)+(s2+s3)).  The
+// gathers are bound by L2 latency; a quad keeps four times as many
+// independent loads in flight per monomer as one thread per component
+// does.  Per term the product order is that of stencil_gather.  Lane 0 of a
+// quad then makes the reference's update (lagrangian_update,
+// cuda/SELM_Kernel.cu:302-373), lane 1 draws its normal, lane 2 files the
+// monomer for the spread; the record's weight rows are written one element
+// per lane.  Needs nx a multiple of 4 (the vector path).
+__global__ void __launch_bounds__(256) k_interp_update_q4(const float* __restrict__ u, const double* __restrict__ x_old,
+                                                          double* __restrict__ x_new, double* __restrict__ v,
+                                                          double* __restrict__ f, const double* __restrict__ m,
+                                                          double* __restrict__ tf_out, const int* __restrict__ order,
+                                                          WRec<float>* __restrict__ rec, CouplingArgs a,
+                                                          uint32_t* __restrict__ err, TileSlots ts) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 12L * a.M) return;  // quads leave whole: 12 M is a multiple of 4
+  const int q = (int)(gid & 3);
+  const long sc = gid >> 2;
+  const int s = (int)(sc / 3), d = (int)(sc - 3L * s);
+  const int p = order ? order[s] : s;
+  const long g = 3L * p + d;
+  const long N = (long)a.nx * a.ny * a.nz;
+  const unsigned qmask = 0xFu << (threadIdx.x & 28);
+  const int qlane0 = threadIdx.x & 28;
+  const double gx = (x_old[3L * p] - a.lo) / a.dx, gy = (x_old[3L * p + 1] - a.lo) / a.dx,
+               gz = (x_old[3L * p + 2] - a.lo) / a.dx;
+  const double r[3] = {d == 0 ? gx : gx - 0.5, d == 1 ? gy : gy - 0.5, d == 2 ? gz : gz - 0.5};
+  int base[3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ax++) base[ax] = (int)floor(r[ax]) - 1;
+  float wx[4], wy[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    wx[i] = ref_weight<float>(fabs(r[0] - (double)(base[0] + i)));
+    wy[i] = ref_weight<float>(fabs(r[1] - (double)(base[1] + i)));
+  }
+  const float wzq = ref_weight<float>(fabs(r[2] - (double)(base[2] + q)));
+  // plane q: 4 rows, two aligned float4 chunks each (the second holds stencil
+  // points only when the window is not chunk-aligned)
+  const int x0 = wrapi(base[0], a.nx);
+  const int a0 = x0 & ~3, off = x0 - a0;
+  const int v1 = (a0 + 4 >= a.nx) ? a0 + 4 - a.nx : a0 + 4;
+  const long zoff = (long)wrapi(base[2] + q, a.nz) * a.ny;
+  const float* ud = u + d * N;
+  float4 ch[4][2];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const float* row = ud + (zoff + wrapi(base[1] + j, a.ny)) * a.nx;
+    ch[j][0] = __ldg(reinterpret_cast<const float4*>(row + a0));
+    ch[j][1] = (off > 0) ? __ldg(reinterpret_cast<const float4*>(row + v1)) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  float wsel[8];
+#pragma unroll
+  for (int t = 0; t < 8; t++) {
+    const int i = t - off;
+    wsel[t] = (i == 0) ? wx[0] : (i == 1) ? wx[1] : (i == 2) ? wx[2] : (i == 3) ? wx[3] : 0.0f;
+  }
+  float val = 0.0f;
+  const float dk = 1.0f * wzq;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const float dj = dk * wy[j];
+    const float e[8] = {ch[j][0].x, ch[j][0].y, ch[j][0].z, ch[j][0].w, ch[j][1].x, ch[j][1].y, ch[j][1].z, ch[j][1].w};
+#pragma unroll
+    for (int t = 0; t < 8; t++) val += e[t] * (dj * wsel[t]);
+  }
+  val += __shfl_xor_sync(qmask, val, 1);
+  val += __shfl_xor_sync(qmask, val, 2);
+  // the stencil record of this step's spread: element q of each weight row
+  if (rec) {
+    WRec<float>& R = rec[p];
+    const int a1 = (d + 1) % 3;
+    const int nn[3] = {a.nx, a.ny, a.nz};
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) {
+      if (ax == d || ax == a1) {
+        const int sh = (ax == d) ? 0 : 1;
+        R.w[ax][sh][q] = (ax == 0) ? wx[q] : (ax == 1) ? wy[q] : wzq;
+        if (q == 0) R.b[ax][sh] = wrapi(base[ax], nn[ax]);
+      }
+    }
+    if (ts.home && q == 1) home_box_store(R.hb, d, gx, gy, gz, ts.bs);
+  }
+  if (ts.count && d == 0 && q == 2) tile_append(ts, p, gx, gy, gz, err);  // the spread of this step reads x_old
+  double z0 = 0.0;
+  if (a.stochastic && q == 1) {
+    double z1;
+    const uint64_t step = a.step_ptr ? *a.step_ptr : a.step;
+    philox_normal2(a.seed, (uint32_t)p, 4u + (uint32_t)d, step, z0, z1);
+  }
+  z0 = __shfl_sync(qmask, z0, qlane0 + 1);
+  if (q != 0) return;
+  const double vg = v[g];
+  double t_f = -a.upsilon * (vg - (double)val) * a.dt;
+  if (a.stochastic) t_f += z0 * a.coef;
+  tf_out[g] = t_f;
+  t_f += a.dt * f[g];
+  f[g] = t_f / a.dt;
+  const double tmp = vg * a.dt;
+  const double L = a.hi - a.lo;
+  if (fabs(tmp) > L / 2) atomicOr(err, ERR_DISPLACEMENT);
+  double tx = x_old[g] + tmp;
+  if (tx > a.hi) tx -= L;
+  else if (tx < a.lo) tx += L;
+  x_new[g] = tx;
+  const double vn = vg + t_f / m[p];
+  v[g] = vn;
+  if (!isfinite(vn) || !isfinite(tx)) atomicOr(err, ERR_NONFINITE);
+}
+
 // ---- quasi-steady (overdamped) form, no reference counterpart
 // Before the fluid solve: the stencil records at x^n for binning and spreading,
 // and the impulse array the spread subtracts, tf = -F / dV, so that the grid
@@ -724,6 +839,15 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
                           double* tf, const int* order, WRec<T>* rec, const CouplingArgs& a, uint32_t* err,
                           cudaStream_t st, const TileSlots* ts) {
   if (a.M <= 0) return cudaSuccess;
+  if constexpr (sizeof(T) == 4) {
+    if (a.nx % 4 == 0) {
+      const long nq = 12L * a.M;
+      k_interp_update_q4<<<(unsigned)((nq + 255) / 256), 256, 0, st>>>(u, x_old, x_new, v, f, m, tf, order, rec, a,
+                                                                      err, ts ? *ts : TileSlots{});
+      count_launches(1);
+      return cudaGetLastError();
+    }
+  }
   const long nt = 3L * a.M;
   k_interp_update<T><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(u, x_old, x_new, v, f, m, tf, order, rec, a,
                                                                     err, ts ? *ts : TileSlots{});
