@@ -122,11 +122,14 @@ __device__ __forceinline__ void philox_normal2(const Key& key, uint32_t c0, uint
 // philox_normal2 to FP32 precision.  The FP64 uniforms are u = (x + 1/2) 2^-52
 // with x = o0 2^20 + (o1 >> 12).  Rounding u to FP32 costs 2^-24 absolute,
 // which near u = 1 (radius sqrt(-2 ln u) ~ sqrt(2 (1 - u))) is a large
-// relative error of the radius; so for u >= 1/2 the complement 1 - u is built
-// from the complemented integer bits (exact to FP32 rounding, relative) and
-// -ln u = -log1p(-(1 - u)).  The angle 2 pi u2 is taken as pi t with the
-// signed t = 2 u2 (mod 2) in [-1, 1), through sincospif, so neither the
-// argument nor the evaluation loses more than an FP32 ulp.
+// relative error of the radius; so for u >= 1/2 the complement d = 1 - u is
+// built from the complemented integer bits (exact to FP32 rounding, relative)
+// and -ln u = -ln(1 - d) = 2 atanh(s), s = d / (2 - d) <= 1/3, by its odd
+// series to s^13 (the first term left out is below 5e-9 of the sum).  For
+// u < 1/2, -ln u >= ln 2 and the fast logarithm's 3-ulp error is already
+// FP32 precision.  The angle 2 pi u2 is taken as pi t with the signed
+// t = 2 u2 (mod 2) in [-1, 1), so the fast sine and cosine see |pi t| <= pi,
+// where their absolute error is below 2^-21.4.
 template <typename Key>
 __device__ __forceinline__ void philox_normal2_f32(const Key& key, uint32_t c0, uint32_t c1, uint64_t step, float& z0,
                                                    float& z1) {
@@ -138,15 +141,23 @@ __device__ __forceinline__ void philox_normal2_f32(const Key& key, uint32_t c0, 
   float nl;  // -ln u1
   if (o[0] & 0x80000000u) {
     const float d = fmaf((float)(~o[0]), 0x1p-32f, ((float)((~o[1]) >> 12) + 0.5f) * 0x1p-52f);
-    nl = -log1pf(-d);
+    const float s = __fdividef(d, 2.0f - d), s2 = s * s;
+    float p = 1.0f / 13.0f;
+    p = fmaf(p, s2, 1.0f / 11.0f);
+    p = fmaf(p, s2, 1.0f / 9.0f);
+    p = fmaf(p, s2, 1.0f / 7.0f);
+    p = fmaf(p, s2, 1.0f / 5.0f);
+    p = fmaf(p, s2, 1.0f / 3.0f);
+    p = fmaf(p, s2, 1.0f);
+    nl = 2.0f * s * p;
   } else {
     const float u = fmaf((float)o[0], 0x1p-32f, ((float)(o[1] >> 12) + 0.5f) * 0x1p-52f);
-    nl = -logf(u);
+    nl = -__logf(u);
   }
   const float r = sqrtf(2.0f * nl);
   const float t = fmaf((float)(int32_t)o[2], 0x1p-31f, ((float)(o[3] >> 12) + 0.5f) * 0x1p-51f);
   float sn, cs;
-  sincospif(t, &sn, &cs);
+  __sincosf(3.14159265358979f * t, &sn, &cs);
   z0 = r * cs;
   z1 = r * sn;
 }

@@ -492,16 +492,36 @@ __device__ __forceinline__ void home_box_store(unsigned char (&hb)[3][2], int d,
   }
 }
 
+// Home mode: the tile of the monomer's cell.
+__device__ __forceinline__ int home_tile(double gx, double gy, double gz, const BinSpec& bs) {
+  bool lo_half;
+  const int cx = home_cell(gx, bs.n[0], lo_half), cy = home_cell(gy, bs.n[1], lo_half),
+            cz = home_cell(gz, bs.n[2], lo_half);
+  return ((cz / bs.tile[2]) * bs.nb[1] + cy / bs.tile[1]) * bs.nb[0] + cx / bs.tile[0];
+}
+
+// Home mode: the scale data of the home tile's fixed-point box, from the
+// thread of one component: its impulse |tf| and its weight factors.
+template <typename T>
+__device__ __forceinline__ void home_scale_note(const TileSlots& ts, double gx, double gy, double gz, double tf,
+                                                const T (&w)[3][4]) {
+  const int t = home_tile(gx, gy, gz, ts.bs);
+  atomicMax(&ts.tmax[t], (unsigned long long)__double_as_longlong(fabs(tf)));
+  bool big = false;
+#pragma unroll
+  for (int ax = 0; ax < 3; ax++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) big |= (w[ax][i] > T(0.5));
+  if (big) atomicOr(&ts.quirk[t], 1);
+}
+
 // File monomer p under every spread tile its union stencil reaches (home
 // mode: under its home tile only): a slot of the tile while it has room,
 // else the overflow list.
 __device__ __forceinline__ void tile_append(const TileSlots& ts, int p, double gx, double gy, double gz, uint32_t* err) {
   const BinSpec& bs = ts.bs;
   if (ts.home) {
-    bool lo_half;
-    const int cx = home_cell(gx, bs.n[0], lo_half), cy = home_cell(gy, bs.n[1], lo_half),
-              cz = home_cell(gz, bs.n[2], lo_half);
-    const int t = ((cz / bs.tile[2]) * bs.nb[1] + cy / bs.tile[1]) * bs.nb[0] + cx / bs.tile[0];
+    const int t = home_tile(gx, gy, gz, bs);
     const int slot = atomicAdd(&ts.count[t], 1);
     if (slot < ts.cap) {
       ts.slots[(long)t * ts.cap + slot] = p;
@@ -600,6 +620,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_interp_update(c
     t_f += z0 * a.coef;
   }
   tf_out[g] = t_f;
+  if (ts.home) home_scale_note<T>(ts, gx, gy, gz, t_f, w);
   t_f += a.dt * f[g];
   f[g] = t_f / a.dt;
   const double tmp = vg * a.dt;
@@ -614,120 +635,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_interp_update(c
   if (!isfinite(vn) || !isfinite(tx)) atomicOr(err, ERR_NONFINITE);
 }
 
-
-// The FP32 form's interpolation and monomer update with four threads per
-// (monomer, component): thread q of a quad gathers z-plane q of the 4^3
-// stencil (4 rows of 4 points, loaded as two aligned 16-byte vectors each,
-// all 8 loads issued before any arithmetic), and the four plane sums combine
-// by two shuffles (the same sum on every lane: (s0+s1)+(s2+s3)).  The
-// gathers are bound by L2 latency; a quad keeps four times as many
-// independent loads in flight per monomer as one thread per component
-// does.  Per term the product order is that of stencil_gather.  Lane 0 of a
-// quad then makes the reference's update (lagrangian_update,
-// cuda/SELM_Kernel.cu:302-373), lane 1 draws its normal, lane 2 files the
-// monomer for the spread; the record's weight rows are written one element
-// per lane.  Needs nx a multiple of 4 (the vector path).
-__global__ void __launch_bounds__(256) k_interp_update_q4(const float* __restrict__ u, const double* __restrict__ x_old,
-                                                          double* __restrict__ x_new, double* __restrict__ v,
-                                                          double* __restrict__ f, const double* __restrict__ m,
-                                                          double* __restrict__ tf_out, const int* __restrict__ order,
-                                                          WRec<float>* __restrict__ rec, CouplingArgs a,
-                                                          uint32_t* __restrict__ err, TileSlots ts) {
-  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= 12L * a.M) return;  // quads leave whole: 12 M is a multiple of 4
-  const int q = (int)(gid & 3);
-  const long sc = gid >> 2;
-  const int s = (int)(sc / 3), d = (int)(sc - 3L * s);
-  const int p = order ? order[s] : s;
-  const long g = 3L * p + d;
-  const long N = (long)a.nx * a.ny * a.nz;
-  const unsigned qmask = 0xFu << (threadIdx.x & 28);
-  const int qlane0 = threadIdx.x & 28;
-  const double gx = (x_old[3L * p] - a.lo) / a.dx, gy = (x_old[3L * p + 1] - a.lo) / a.dx,
-               gz = (x_old[3L * p + 2] - a.lo) / a.dx;
-  const double r[3] = {d == 0 ? gx : gx - 0.5, d == 1 ? gy : gy - 0.5, d == 2 ? gz : gz - 0.5};
-  int base[3];
-#pragma unroll
-  for (int ax = 0; ax < 3; ax++) base[ax] = (int)floor(r[ax]) - 1;
-  float wx[4], wy[4];
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    wx[i] = ref_weight<float>(fabs(r[0] - (double)(base[0] + i)));
-    wy[i] = ref_weight<float>(fabs(r[1] - (double)(base[1] + i)));
-  }
-  const float wzq = ref_weight<float>(fabs(r[2] - (double)(base[2] + q)));
-  // plane q: 4 rows, two aligned float4 chunks each (the second holds stencil
-  // points only when the window is not chunk-aligned)
-  const int x0 = wrapi(base[0], a.nx);
-  const int a0 = x0 & ~3, off = x0 - a0;
-  const int v1 = (a0 + 4 >= a.nx) ? a0 + 4 - a.nx : a0 + 4;
-  const long zoff = (long)wrapi(base[2] + q, a.nz) * a.ny;
-  const float* ud = u + d * N;
-  float4 ch[4][2];
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    const float* row = ud + (zoff + wrapi(base[1] + j, a.ny)) * a.nx;
-    ch[j][0] = __ldg(reinterpret_cast<const float4*>(row + a0));
-    ch[j][1] = (off > 0) ? __ldg(reinterpret_cast<const float4*>(row + v1)) : make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  float wsel[8];
-#pragma unroll
-  for (int t = 0; t < 8; t++) {
-    const int i = t - off;
-    wsel[t] = (i == 0) ? wx[0] : (i == 1) ? wx[1] : (i == 2) ? wx[2] : (i == 3) ? wx[3] : 0.0f;
-  }
-  float val = 0.0f;
-  const float dk = 1.0f * wzq;
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    const float dj = dk * wy[j];
-    const float e[8] = {ch[j][0].x, ch[j][0].y, ch[j][0].z, ch[j][0].w, ch[j][1].x, ch[j][1].y, ch[j][1].z, ch[j][1].w};
-#pragma unroll
-    for (int t = 0; t < 8; t++) val += e[t] * (dj * wsel[t]);
-  }
-  val += __shfl_xor_sync(qmask, val, 1);
-  val += __shfl_xor_sync(qmask, val, 2);
-  // the stencil record of this step's spread: element q of each weight row
-  if (rec) {
-    WRec<float>& R = rec[p];
-    const int a1 = (d + 1) % 3;
-    const int nn[3] = {a.nx, a.ny, a.nz};
-#pragma unroll
-    for (int ax = 0; ax < 3; ax++) {
-      if (ax == d || ax == a1) {
-        const int sh = (ax == d) ? 0 : 1;
-        R.w[ax][sh][q] = (ax == 0) ? wx[q] : (ax == 1) ? wy[q] : wzq;
-        if (q == 0) R.b[ax][sh] = wrapi(base[ax], nn[ax]);
-      }
-    }
-    if (ts.home && q == 1) home_box_store(R.hb, d, gx, gy, gz, ts.bs);
-  }
-  if (ts.count && d == 0 && q == 2) tile_append(ts, p, gx, gy, gz, err);  // the spread of this step reads x_old
-  double z0 = 0.0;
-  if (a.stochastic && q == 1) {
-    double z1;
-    const uint64_t step = a.step_ptr ? *a.step_ptr : a.step;
-    philox_normal2(a.seed, (uint32_t)p, 4u + (uint32_t)d, step, z0, z1);
-  }
-  z0 = __shfl_sync(qmask, z0, qlane0 + 1);
-  if (q != 0) return;
-  const double vg = v[g];
-  double t_f = -a.upsilon * (vg - (double)val) * a.dt;
-  if (a.stochastic) t_f += z0 * a.coef;
-  tf_out[g] = t_f;
-  t_f += a.dt * f[g];
-  f[g] = t_f / a.dt;
-  const double tmp = vg * a.dt;
-  const double L = a.hi - a.lo;
-  if (fabs(tmp) > L / 2) atomicOr(err, ERR_DISPLACEMENT);
-  double tx = x_old[g] + tmp;
-  if (tx > a.hi) tx -= L;
-  else if (tx < a.lo) tx += L;
-  x_new[g] = tx;
-  const double vn = vg + t_f / m[p];
-  v[g] = vn;
-  if (!isfinite(vn) || !isfinite(tx)) atomicOr(err, ERR_NONFINITE);
-}
 
 // ---- quasi-steady (overdamped) form, no reference counterpart
 // Before the fluid solve: the stencil records at x^n for binning and spreading,
@@ -749,6 +656,7 @@ __global__ void __launch_bounds__(256) k_qs_prepare(const double* __restrict__ x
   if (ts.home) home_box_store(rec[p].hb, d, gx, gy, gz, ts.bs);
   if (ts.count && d == 0) tile_append(ts, p, gx, gy, gz, err);
   tf_out[gid] = -f[gid] * inv_dv;
+  if (ts.home) home_scale_note<T>(ts, gx, gy, gz, tf_out[gid], w);
 }
 
 // After the fluid solve: v = Gamma u (x^n), x^{n+1} = x^n + dt v with the
@@ -839,15 +747,6 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
                           double* tf, const int* order, WRec<T>* rec, const CouplingArgs& a, uint32_t* err,
                           cudaStream_t st, const TileSlots* ts) {
   if (a.M <= 0) return cudaSuccess;
-  if constexpr (sizeof(T) == 4) {
-    if (a.nx % 4 == 0) {
-      const long nq = 12L * a.M;
-      k_interp_update_q4<<<(unsigned)((nq + 255) / 256), 256, 0, st>>>(u, x_old, x_new, v, f, m, tf, order, rec, a,
-                                                                      err, ts ? *ts : TileSlots{});
-      count_launches(1);
-      return cudaGetLastError();
-    }
-  }
   const long nt = 3L * a.M;
   k_interp_update<T><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(u, x_old, x_new, v, f, m, tf, order, rec, a,
                                                                     err, ts ? *ts : TileSlots{});
@@ -1170,7 +1069,8 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
 // Scale: with n monomers in the tile (k = ceil(log2 n)), the largest impulse
 // component m < 2^em and every weight factor <= 2^(ew/3) (ew = -3 when all
 // factors are <= 1/2, as the Peskin function is; 0 when the reference's
-// distance-2 factor of 1 occurs), a contribution is < 2^(em + ew + S) and a
+// distance-2 factor of 1 occurs; m and the flag come from the interpolation,
+// TileSlots::tmax and ::quirk), a contribution is < 2^(em + ew + S) and a
 // cell's sum < n 2^(em + ew + S).  S = min(30 - k, 22) - em - ew keeps a
 // cell's sum below 2^30 (plus n/2 of rounding) and a contribution below 2^22,
 // the range of the float-to-integer rounding by adding 1.5 2^23.  That is a
@@ -1181,7 +1081,7 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
 // products for k <= 16.
 constexpr int kHX = kTX + 4, kHY = kTY + 4, kHZ = kTZ + 4;
 constexpr int kHBox = kHX * kHY * kHZ;  // cells per component
-constexpr int kHomeThreads = 256;
+constexpr int kHomeThreads = 512;
 constexpr int kHomeWarps = kHomeThreads / 32;
 constexpr int kHomeSplitK = 11;  // single-word path for n <= 2^11
 static_assert(kHX % 32 == 20 && (kHX * kHY) % 32 == 16, "bank pattern of the box atomics");
@@ -1231,20 +1131,25 @@ __device__ __forceinline__ void home_add(const int* __restrict__ ids, int n_prim
       }
     }
   };
-  for (int c = wid; c < n_prim; c += kHomeWarps) one(ids[c]);
+  // the next candidate's index is loaded while this one is added
+  int c = wid;
+  int pn = (c < n_prim) ? ids[c] : 0;
+  while (c < n_prim) {
+    const int p = pn;
+    c += kHomeWarps;
+    if (c < n_prim) pn = ids[c];
+    one(p);
+  }
   for (int q = wid; q < n_ovf; q += kHomeWarps) {
     const int2 e = ts.ovf[q];
     if (e.x == tb) one(e.y);
   }
 }
 
-__global__ void __launch_bounds__(kHomeThreads) k_spread_home(const double* __restrict__ tf, TileSlots ts,
-                                                              const WRec<float>* __restrict__ rec) {
+__global__ void __launch_bounds__(kHomeThreads, 3) k_spread_home(const double* __restrict__ tf, TileSlots ts,
+                                                                 const WRec<float>* __restrict__ rec) {
   extern __shared__ __align__(16) unsigned hacc[];  // [3][kHZ][kHY][kHX], or [2][kHZ][kHY][kHX] (split path)
-  __shared__ double wmax[kHomeWarps];
-  __shared__ float wwm[kHomeWarps];
-  __shared__ int wbad[kHomeWarps];
-  const int tb = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tb = blockIdx.x, tid = threadIdx.x;
   const int n = ts.count[tb];
   const int n_prim = min(n, ts.cap);
   const int* ids = ts.slots + (long)tb * ts.cap;
@@ -1252,55 +1157,17 @@ __global__ void __launch_bounds__(kHomeThreads) k_spread_home(const double* __re
   float* out = ts.box + (long)tb * 3 * kHBox;
   if (tid == 0) ts.live[tb] = (n > 0);
   if (n > 0) {
-    // scale: largest impulse component and largest weight factor of the tile's monomers
-    double m = 0.0;
-    float wm = 0.0f;
-    int bad = 0;
-    auto see = [&](int p) {
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        const double v = fabs(tf[3L * p + c]);
-        bad |= !(v <= 1.0e300);
-        m = fmax(m, v);
-      }
-      const float4* w4 = reinterpret_cast<const float4*>(&rec[p].w[0][0][0]);
-#pragma unroll
-      for (int r = 0; r < 6; r++) {
-        const float4 q = w4[r];
-        wm = fmaxf(wm, fmaxf(fmaxf(fabsf(q.x), fabsf(q.y)), fmaxf(fabsf(q.z), fabsf(q.w))));
-      }
-    };
-    for (int q = tid; q < n_prim; q += kHomeThreads) see(ids[q]);
-    for (int q = tid; q < n_ovf; q += kHomeThreads) {
-      const int2 e = ts.ovf[q];
-      if (e.x == tb) see(e.y);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-      wm = fmaxf(wm, __shfl_xor_sync(0xffffffffu, wm, o));
-    }
-    bad = __any_sync(0xffffffffu, bad);
-    if (lane == 0) {
-      wmax[wid] = m;
-      wwm[wid] = wm;
-      wbad[wid] = bad;
-    }
-    // zero the accumulators meanwhile
+    const double m = __longlong_as_double((long long)ts.tmax[tb]);  // largest |impulse| of the tile
+    const bool bad = !(m <= 1.0e300);
+    const int ew = ts.quirk[tb] ? 0 : -3;
     uint4* z4 = reinterpret_cast<uint4*>(hacc);
-    for (int i = tid; i < 3 * kHBox / 4; i += kHomeThreads) z4[i] = make_uint4(0u, 0u, 0u, 0u);
-    __syncthreads();
-#pragma unroll
-    for (int w = 0; w < kHomeWarps; w++) {
-      m = fmax(m, wmax[w]);
-      wm = fmaxf(wm, wwm[w]);
-      bad |= wbad[w];
-    }
     if (bad) {
+      // a non-finite impulse makes the tile non-finite, as a floating-point sum would
       for (int i = tid; i < 3 * kHBox; i += kHomeThreads) out[i] = __int_as_float(0x7fc00000);
     } else {
+      for (int i = tid; i < 3 * kHBox / 4; i += kHomeThreads) z4[i] = make_uint4(0u, 0u, 0u, 0u);
+      __syncthreads();
       const int k = (n > 1) ? 32 - __clz(n - 1) : 1;  // ceil(log2 n)
-      const int ew = (wm <= 0.5f) ? -3 : 0;
       int em = 0;
       if (m > 0.0) frexp(m, &em);  // m < 2^em
       if (k <= kHomeSplitK) {
@@ -1329,15 +1196,76 @@ __global__ void __launch_bounds__(kHomeThreads) k_spread_home(const double* __re
       }
     }
   }
-  __syncthreads();  // every thread has read count[tb] and the overflow counter
+  __syncthreads();  // every thread has read count[tb], tmax[tb], quirk[tb] and the overflow counter
   if (tid == 0) {
     ts.count[tb] = 0;
+    ts.tmax[tb] = 0ull;
+    ts.quirk[tb] = 0;
     __threadfence();
     if (atomicAdd(ts.done, 1u) == gridDim.x - 1) {  // the last block to finish: no block reads it any more
       *ts.ovf_count = 0;
       *ts.done = 0u;
     }
   }
+}
+
+// The fold on grids whose sizes are multiples of the tile (every tile full):
+// block per (tile, component), thread per 16-cell x-row (y, z) of the tile.
+// A row's cells lie in the boxes of the tiles dz, dy in {-1, 0, 1} (the
+// neighbour along y or z only for the 2 rows next to that face) and dx in
+// {-1, 0, 1}: box row (z + 2 - dz T_z, y + 2 - dy T_y) of tile (tx, ty+dy,
+// tz+dz) gives the 16 cells (columns 2..17), the same row of tile tx-1 gives
+// cells 0, 1 (its columns 18, 19) and of tile tx+1 cells 14, 15 (its columns
+// 0, 1).  Per cell the order of addition is fixed: dz, then dy, then dx, each
+// ascending.  Tiles one or two per axis wrap onto themselves: the same rule
+// holds, with tx-1 and tx+1 naming the same tile.
+template <typename T>
+__global__ void __launch_bounds__(kTY * kTZ) k_spread_fold_rows(T* __restrict__ f, int accumulate,
+                                                                  const float* __restrict__ box,
+                                                                  const int* __restrict__ live, BinSpec bs) {
+  static_assert(kTX == 16, "16-cell rows");
+  const int tb = blockIdx.x, d = blockIdx.y;
+  const int nb0 = bs.nb[0], nb1 = bs.nb[1], nb2 = bs.nb[2];
+  const int tx = tb % nb0, ty = (tb / nb0) % nb1, tz = tb / (nb0 * nb1);
+  const int ly = threadIdx.x % kTY, lz = threadIdx.x / kTY;
+  const int txl = (tx == 0) ? nb0 - 1 : tx - 1, txr = (tx == nb0 - 1) ? 0 : tx + 1;
+  float s[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) s[i] = 0.0f;
+  const int dz0 = (lz < 2) ? -1 : 0, dz1 = (lz >= kTZ - 2) ? 1 : 0;
+  const int dy0 = (ly < 2) ? -1 : 0, dy1 = (ly >= kTY - 2) ? 1 : 0;
+  for (int dz = dz0; dz <= dz1; dz++) {
+    const int tzz = (tz + dz + nb2) % nb2, bz = lz + 2 - dz * kTZ;
+    for (int dy = dy0; dy <= dy1; dy++) {
+      const int tyy = (ty + dy + nb1) % nb1, by = ly + 2 - dy * kTY;
+      const long rowoff = (long)d * kHBox + (bz * kHY + by) * kHX;
+      const int rowt = (tzz * nb1 + tyy) * nb0;
+      const int tl = rowt + txl, tm = rowt + tx, tr = rowt + txr;
+      if (live[tl]) {
+        const float2 q = __ldg(reinterpret_cast<const float2*>(box + (long)tl * 3 * kHBox + rowoff + 18));
+        s[0] += q.x;
+        s[1] += q.y;
+      }
+      if (live[tm]) {
+        const float2* r = reinterpret_cast<const float2*>(box + (long)tm * 3 * kHBox + rowoff + 2);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const float2 q = __ldg(r + i);
+          s[2 * i] += q.x;
+          s[2 * i + 1] += q.y;
+        }
+      }
+      if (live[tr]) {
+        const float2 q = __ldg(reinterpret_cast<const float2*>(box + (long)tr * 3 * kHBox + rowoff));
+        s[14] += q.x;
+        s[15] += q.y;
+      }
+    }
+  }
+  const int nx = bs.n[0], ny = bs.n[1], nz = bs.n[2];
+  T* dst = f + ((long)(d * nz + tz * kTZ + lz) * ny + ty * kTY + ly) * nx + tx * kTX;
+#pragma unroll
+  for (int i = 0; i < 16; i++) dst[i] = accumulate ? (T)((double)dst[i] + (double)s[i]) : (T)s[i];
 }
 
 // Boxes of the tiles along one axis that hold cell c: (tile, box coordinate)
@@ -1511,7 +1439,16 @@ cudaError_t spread_slots(T* fgrid, bool accumulate, const double* x_old, const d
   if constexpr (sizeof(T) == 4) {
     if (ts.home) {
       if (!ts.box || !ts.live || !rec) return cudaErrorInvalidValue;
+      if (!ts.tmax || !ts.quirk) return cudaErrorInvalidValue;
       k_spread_home<<<ntiles, kHomeThreads, kHomeSmem, st>>>(tf, ts, rec);
+      bool full = true;  // every tile full: the row fold
+      for (int ax = 0; ax < 3; ax++) full &= (bs.n[ax] % bs.tile[ax] == 0);
+      if (full) {
+        k_spread_fold_rows<T><<<dim3((unsigned)ntiles, 3), kTY * kTZ, 0, st>>>(fgrid, accumulate ? 1 : 0, ts.box,
+                                                                              ts.live, bs);
+        count_launches(2);
+        return cudaGetLastError();
+      }
       const dim3 fb(32, 8), fg((unsigned)((a.nx + 31) / 32), (unsigned)((a.ny + 7) / 8), (unsigned)(3 * a.nz));
       bool regs = true;  // box_axis2 holds: 3 or more tiles per axis, none narrower than 4 cells
       for (int ax = 0; ax < 3; ax++)

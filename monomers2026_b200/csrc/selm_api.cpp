@@ -319,6 +319,10 @@ static int alloc_slots(selm_sim* s, const BinSpec& bs, TileSlots& ts, int M) {
     const long box = 3L * (bs.tile[0] + 4) * (bs.tile[1] + 4) * (bs.tile[2] + 4);
     if ((rc = dalloc(s, &ts.box, ntiles * box))) return rc;
     if ((rc = dalloc(s, &ts.live, ntiles))) return rc;
+    if ((rc = dalloc(s, &ts.tmax, ntiles))) return rc;
+    if ((rc = dalloc(s, &ts.quirk, ntiles))) return rc;
+    CU(cudaMemset(ts.tmax, 0, sizeof(unsigned long long) * ntiles));
+    CU(cudaMemset(ts.quirk, 0, sizeof(int) * ntiles));
   }
   if ((rc = dalloc(s, &ts.count, ntiles))) return rc;
   if ((rc = dalloc(s, &ts.slots, ntiles * cap))) return rc;

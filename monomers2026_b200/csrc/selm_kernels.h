@@ -84,9 +84,16 @@ struct TileSlots {
   // cell floor((x - lo)/dx); the spread accumulates each tile's monomers into
   // a box of the tile plus a 2-cell halo, written to box[], and a fold pass
   // sums the boxes that cover each cell.  live[t] = tile t had monomers.
+  // The interpolation also leaves, per tile, the largest |impulse| of its
+  // monomers (tmax: the bits of the FP64 value, which order as unsigned
+  // integers for non-negative values, NaN above all) and whether a weight
+  // factor above 1/2 occurred (quirk: the reference's distance-2 factor of 1),
+  // the scale of the tile's fixed-point box; the spread clears both.
   int home = 0;
   float* box = nullptr;       // [ntiles][3][tile z + 4][tile y + 4][tile x + 4]
   int* live = nullptr;        // [ntiles]
+  unsigned long long* tmax = nullptr;  // [ntiles]
+  int* quirk = nullptr;                // [ntiles]
 };
 template <typename T> struct alignas(16) WRec {
   T w[3][2][4];  // weight factors [axis][unshifted, shifted][point] (16-byte aligned rows)

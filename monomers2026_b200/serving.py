@@ -63,7 +63,7 @@ def estimate_device_bytes(params, natoms: int, pairs: bool = True) -> int:
     cap = max(128, -(-(int(math.ceil(4.0 * M * per / tiles)) + 64) // 32) * 32)
     slots = 4 * tiles * (cap + 1) + 8 * ((1 if home else 27) * M + 1024)  # tile slots and the overflow list
     if home:
-        slots += tiles * (4 * 3 * (tile[0] + 4) * (tile[1] + 4) * (tile[2] + 4) + 4)
+        slots += tiles * (4 * 3 * (tile[0] + 4) * (tile[1] + 4) * (tile[2] + 4) + 16)
     # x (two buffers), v, f, tf, m, the staged upload of a per-step round trip, stencil records
     mono = M * (2 * 24 + 3 * 24 + 8 + 2 * 24 + (128 if s == 4 else 224)) + slots
     nl = 0
