@@ -7,8 +7,8 @@ that do not depend on the size.
 operators against real-space stencils and FFT passes) on the same Philox
 stream; each matches the oracle to 1e-11 per step on small grids.  After 5
 steps they agree to 1e-10 relative (each field against its maximum).
-(2) The FP32 form stays within 1e-4 of FP64 (velocities and forces; 1e-9 for
-positions, which are FP64 in both).
+(2) The FP32 form stays within 1e-5 of FP64 in the velocities (monomer and
+fluid) and the forces (1e-9 for positions, which are FP64 in both).
 (3) Two runs of the FP32 form are bitwise equal (fixed-point spreading, no
 floating-point atomics), and every run ends with a clear status word."""
 from dataclasses import replace
@@ -56,7 +56,7 @@ def test_full_size_forms_agree_and_fp32_is_deterministic(workload):
     for a, b in zip(f64[:4], p64[:4]):
         assert rel(a, b) < 1e-10
     assert rel(f32a[0], f64[0]) < 1e-9
-    for a, b in zip(f32a[1:4], f64[1:4]):
-        assert rel(a, b) < 1e-4
+    for name, a, b in zip(("v", "f", "u"), f32a[1:4], f64[1:4]):
+        assert rel(a, b) < 1e-5, f"FP32 {name}: rel err {rel(a, b):.3e}"
     for a, b in zip(f32a[:4], f32b[:4]):
         assert np.array_equal(a, b)

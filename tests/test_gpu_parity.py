@@ -210,7 +210,7 @@ def test_fused_fene_wca_vs_oracle(oracle, form, tol):
     _compare_run(oracle, wl, 20, tol)
 
 
-@pytest.mark.parametrize("form,tol", [("fused64", 1e-11), ("fused32", 1e-4)])
+@pytest.mark.parametrize("form,tol", [("fused64", 1e-11), ("fused32", 1e-5)])
 def test_fused_128_cubed_with_noise(oracle, form, tol):
     """The 128^3 kernels (their own column blocks and block shapes) with the
     thermal noise on: FENE chains against the FP64 oracle, step by step."""
