@@ -1210,62 +1210,55 @@ __global__ void __launch_bounds__(kHomeThreads, 3) k_spread_home(const double* _
 }
 
 // The fold on grids whose sizes are multiples of the tile (every tile full):
-// block per (tile, component), thread per 16-cell x-row (y, z) of the tile.
-// A row's cells lie in the boxes of the tiles dz, dy in {-1, 0, 1} (the
+// block per (tile, component), a half-warp per 16-cell x-row (y, z) of the
+// tile and a lane per cell, so that loads and stores are 64-byte runs.  A
+// row's cells lie in the boxes of the tiles dz, dy in {-1, 0, 1} (the
 // neighbour along y or z only for the 2 rows next to that face) and dx in
 // {-1, 0, 1}: box row (z + 2 - dz T_z, y + 2 - dy T_y) of tile (tx, ty+dy,
-// tz+dz) gives the 16 cells (columns 2..17), the same row of tile tx-1 gives
-// cells 0, 1 (its columns 18, 19) and of tile tx+1 cells 14, 15 (its columns
-// 0, 1).  Per cell the order of addition is fixed: dz, then dy, then dx, each
+// tz+dz) holds cell x at column x + 2, the same row of tile tx-1 holds cells
+// 0, 1 at its columns 18, 19, and of tile tx+1 cells 14, 15 at its columns
+// 0, 1.  Per cell the order of addition is fixed: dz, then dy, then dx, each
 // ascending.  Tiles one or two per axis wrap onto themselves: the same rule
 // holds, with tx-1 and tx+1 naming the same tile.
+constexpr int kFoldThreads = 256;
 template <typename T>
-__global__ void __launch_bounds__(kTY * kTZ) k_spread_fold_rows(T* __restrict__ f, int accumulate,
-                                                                  const float* __restrict__ box,
-                                                                  const int* __restrict__ live, BinSpec bs) {
+__global__ void __launch_bounds__(kFoldThreads) k_spread_fold_rows(T* __restrict__ f, int accumulate,
+                                                                   const float* __restrict__ box,
+                                                                   const int* __restrict__ live, BinSpec bs) {
   static_assert(kTX == 16, "16-cell rows");
   const int tb = blockIdx.x, d = blockIdx.y;
   const int nb0 = bs.nb[0], nb1 = bs.nb[1], nb2 = bs.nb[2];
   const int tx = tb % nb0, ty = (tb / nb0) % nb1, tz = tb / (nb0 * nb1);
-  const int ly = threadIdx.x % kTY, lz = threadIdx.x / kTY;
   const int txl = (tx == 0) ? nb0 - 1 : tx - 1, txr = (tx == nb0 - 1) ? 0 : tx + 1;
-  float s[16];
-#pragma unroll
-  for (int i = 0; i < 16; i++) s[i] = 0.0f;
-  const int dz0 = (lz < 2) ? -1 : 0, dz1 = (lz >= kTZ - 2) ? 1 : 0;
-  const int dy0 = (ly < 2) ? -1 : 0, dy1 = (ly >= kTY - 2) ? 1 : 0;
-  for (int dz = dz0; dz <= dz1; dz++) {
-    const int tzz = (tz + dz + nb2) % nb2, bz = lz + 2 - dz * kTZ;
-    for (int dy = dy0; dy <= dy1; dy++) {
-      const int tyy = (ty + dy + nb1) % nb1, by = ly + 2 - dy * kTY;
-      const long rowoff = (long)d * kHBox + (bz * kHY + by) * kHX;
-      const int rowt = (tzz * nb1 + tyy) * nb0;
-      const int tl = rowt + txl, tm = rowt + tx, tr = rowt + txr;
-      if (live[tl]) {
-        const float2 q = __ldg(reinterpret_cast<const float2*>(box + (long)tl * 3 * kHBox + rowoff + 18));
-        s[0] += q.x;
-        s[1] += q.y;
-      }
-      if (live[tm]) {
-        const float2* r = reinterpret_cast<const float2*>(box + (long)tm * 3 * kHBox + rowoff + 2);
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-          const float2 q = __ldg(r + i);
-          s[2 * i] += q.x;
-          s[2 * i + 1] += q.y;
+  const int lx = threadIdx.x & 15;
+  const int nx = bs.n[0], ny = bs.n[1], nz = bs.n[2];
+  constexpr int kRowsPerPass = kFoldThreads / 16;
+  for (int r = threadIdx.x >> 4; r < kTY * kTZ; r += kRowsPerPass) {
+    const int ly = r % kTY, lz = r / kTY;
+    float s = 0.0f;
+    const int dz0 = (lz < 2) ? -1 : 0, dz1 = (lz >= kTZ - 2) ? 1 : 0;
+    const int dy0 = (ly < 2) ? -1 : 0, dy1 = (ly >= kTY - 2) ? 1 : 0;
+    for (int dz = dz0; dz <= dz1; dz++) {
+      const int tzz = (tz + dz + nb2) % nb2, bz = lz + 2 - dz * kTZ;
+      for (int dy = dy0; dy <= dy1; dy++) {
+        const int tyy = (ty + dy + nb1) % nb1, by = ly + 2 - dy * kTY;
+        const long rowoff = (long)d * kHBox + (bz * kHY + by) * kHX;
+        const int rowt = (tzz * nb1 + tyy) * nb0;
+        if (lx < 2) {
+          const int tl = rowt + txl;
+          if (live[tl]) s += __ldg(box + (long)tl * 3 * kHBox + rowoff + 18 + lx);
+        }
+        const int tm = rowt + tx;
+        if (live[tm]) s += __ldg(box + (long)tm * 3 * kHBox + rowoff + 2 + lx);
+        if (lx >= 14) {
+          const int tr = rowt + txr;
+          if (live[tr]) s += __ldg(box + (long)tr * 3 * kHBox + rowoff + lx - 14);
         }
       }
-      if (live[tr]) {
-        const float2 q = __ldg(reinterpret_cast<const float2*>(box + (long)tr * 3 * kHBox + rowoff));
-        s[14] += q.x;
-        s[15] += q.y;
-      }
     }
+    T* dst = f + ((long)(d * nz + tz * kTZ + lz) * ny + ty * kTY + ly) * nx + tx * kTX + lx;
+    *dst = accumulate ? (T)((double)*dst + (double)s) : (T)s;
   }
-  const int nx = bs.n[0], ny = bs.n[1], nz = bs.n[2];
-  T* dst = f + ((long)(d * nz + tz * kTZ + lz) * ny + ty * kTY + ly) * nx + tx * kTX;
-#pragma unroll
-  for (int i = 0; i < 16; i++) dst[i] = accumulate ? (T)((double)dst[i] + (double)s[i]) : (T)s[i];
 }
 
 // Boxes of the tiles along one axis that hold cell c: (tile, box coordinate)
@@ -1444,8 +1437,8 @@ cudaError_t spread_slots(T* fgrid, bool accumulate, const double* x_old, const d
       bool full = true;  // every tile full: the row fold
       for (int ax = 0; ax < 3; ax++) full &= (bs.n[ax] % bs.tile[ax] == 0);
       if (full) {
-        k_spread_fold_rows<T><<<dim3((unsigned)ntiles, 3), kTY * kTZ, 0, st>>>(fgrid, accumulate ? 1 : 0, ts.box,
-                                                                              ts.live, bs);
+        k_spread_fold_rows<T><<<dim3((unsigned)ntiles, 3), kFoldThreads, 0, st>>>(fgrid, accumulate ? 1 : 0, ts.box,
+                                                                                 ts.live, bs);
         count_launches(2);
         return cudaGetLastError();
       }
