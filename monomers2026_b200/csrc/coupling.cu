@@ -1098,6 +1098,42 @@ __device__ __forceinline__ void home_add(const int* __restrict__ ids, int n_prim
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int ix = lane & 3, jy = (lane >> 2) & 3, kz = lane >> 4;
   const int loff = (kz * kHY + jy) * kHX + ix;
+  auto one2 = [&](int p0, int p1, bool two) {
+    const WRec<float>& R0 = rec[p0];
+    const WRec<float>& R1 = rec[two ? p1 : p0];
+    const uint2 h0 = *reinterpret_cast<const uint2*>(&R0.hb[0][0]);
+    const uint2 h1 = *reinterpret_cast<const uint2*>(&R1.hb[0][0]);
+    float wxa[2][2], wya[2][2], wza[2][2][2];
+    float wxb[2][2], wyb[2][2], wzb[2][2][2];
+#pragma unroll
+    for (int sh = 0; sh < 2; sh++) {
+      wxa[sh][0] = R0.w[0][sh][ix]; wya[sh][0] = R0.w[1][sh][jy];
+      wza[sh][0][0] = R0.w[2][sh][kz]; wza[sh][0][1] = R0.w[2][sh][kz + 2];
+      wxb[sh][0] = R1.w[0][sh][ix]; wyb[sh][0] = R1.w[1][sh][jy];
+      wzb[sh][0][0] = R1.w[2][sh][kz]; wzb[sh][0][1] = R1.w[2][sh][kz + 2];
+    }
+    double t0[3], t1[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      t0[d] = tf[3L * p0 + d];
+      t1[d] = two ? tf[3L * p1 + d] : 0.0;
+    }
+    auto add = [&](const uint2 hbw, const float (&wx)[2][2], const float (&wy)[2][2], const float (&wz)[2][2][2],
+                   const double (&tv)[3]) {
+      const unsigned char* hb = reinterpret_cast<const unsigned char*>(&hbw);
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const int sx = (d != 0), sy = (d != 1), sz = (d != 2);
+        const int bx = hb[0 + sx], by = hb[2 + sy], bz = hb[4 + sz];
+        const float A = (float)(-tv[d] * scale) * wy[sy][0] * wx[sx][0];
+        const int slot = d * kHBox + (bz * kHY + by) * kHX + bx + loff;
+        atomicAdd(acc + slot, (unsigned)round_small(A * wz[sz][0][0]));
+        atomicAdd(acc + slot + 2 * kHY * kHX, (unsigned)round_small(A * wz[sz][0][1]));
+      }
+    };
+    add(h0, wxa, wya, wza, t0);
+    if (two) add(h1, wxb, wyb, wzb, t1);
+  };
   auto one = [&](int p) {
     const WRec<float>& R = rec[p];
     const uint2 hbw = *reinterpret_cast<const uint2*>(&R.hb[0][0]);
@@ -1131,14 +1167,21 @@ __device__ __forceinline__ void home_add(const int* __restrict__ ids, int n_prim
       }
     }
   };
-  // the next candidate's index is loaded while this one is added
-  int c = wid;
-  int pn = (c < n_prim) ? ids[c] : 0;
-  while (c < n_prim) {
-    const int p = pn;
-    c += kHomeWarps;
-    if (c < n_prim) pn = ids[c];
-    one(p);
+  if (!SPLIT) {
+    // two candidates per pass (their loads overlap), the next pair's indices loaded ahead
+    int c = wid;
+    int pa = (c < n_prim) ? ids[c] : 0;
+    int pb = (c + kHomeWarps < n_prim) ? ids[c + kHomeWarps] : 0;
+    while (c < n_prim) {
+      const int p0 = pa, p1 = pb;
+      const bool two = c + kHomeWarps < n_prim;
+      c += 2 * kHomeWarps;
+      if (c < n_prim) pa = ids[c];
+      if (c + kHomeWarps < n_prim) pb = ids[c + kHomeWarps];
+      one2(p0, p1, two);
+    }
+  } else {
+    for (int c = wid; c < n_prim; c += kHomeWarps) one(ids[c]);
   }
   for (int q = wid; q < n_ovf; q += kHomeWarps) {
     const int2 e = ts.ovf[q];
@@ -1174,8 +1217,14 @@ __global__ void __launch_bounds__(kHomeThreads, 3) k_spread_home(const double* _
         const int S = max(-1000, min(1000, min(30 - k, 22) - em - ew));
         home_add<0>(ids, n_prim, n_ovf, ts, tb, 0, ldexp(1.0, S), 0, hacc, tf, rec);
         __syncthreads();
-        const double inv = ldexp(1.0, -S);
-        for (int i = tid; i < 3 * kHBox; i += kHomeThreads) out[i] = (float)((double)(int)hacc[i] * inv);
+        if (S >= -100 && S <= 100) {
+          // the integer rounded to FP32 once, then scaled by a power of two (exact)
+          const float inv = ldexpf(1.0f, -S);
+          for (int i = tid; i < 3 * kHBox; i += kHomeThreads) out[i] = __int2float_rn((int)hacc[i]) * inv;
+        } else {
+          const double inv = ldexp(1.0, -S);
+          for (int i = tid; i < 3 * kHBox; i += kHomeThreads) out[i] = (float)((double)(int)hacc[i] * inv);
+        }
       } else {
         const int L = 32 - k;
         const int S = max(-1000, min(1000, 62 - 2 * k - em - ew));
@@ -1233,28 +1282,39 @@ __global__ void __launch_bounds__(kFoldThreads) k_spread_fold_rows(T* __restrict
   const int lx = threadIdx.x & 15;
   const int nx = bs.n[0], ny = bs.n[1], nz = bs.n[2];
   constexpr int kRowsPerPass = kFoldThreads / 16;
+  // each lane's x neighbour (tx-1 for cells 0, 1; tx+1 for 14, 15; none else)
+  const int txe = (lx < 2) ? txl : txr;
+  const int ce = (lx < 2) ? 18 + lx : lx - 14;
+  const bool edge = (lx < 2) || (lx >= 14);
   for (int r = threadIdx.x >> 4; r < kTY * kTZ; r += kRowsPerPass) {
     const int ly = r % kTY, lz = r / kTY;
-    float s = 0.0f;
+    // up to 2 x 2 (dz, dy) pairs; every load is issued before any is used (the
+    // boxes of empty tiles hold stale values, dropped by the live flags)
     const int dz0 = (lz < 2) ? -1 : 0, dz1 = (lz >= kTZ - 2) ? 1 : 0;
     const int dy0 = (ly < 2) ? -1 : 0, dy1 = (ly >= kTY - 2) ? 1 : 0;
-    for (int dz = dz0; dz <= dz1; dz++) {
+    float vm[4], ve[4];
+    int lm[4], le[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int dz = (q & 2) ? dz1 : dz0, dy = (q & 1) ? dy1 : dy0;
       const int tzz = (tz + dz + nb2) % nb2, bz = lz + 2 - dz * kTZ;
-      for (int dy = dy0; dy <= dy1; dy++) {
-        const int tyy = (ty + dy + nb1) % nb1, by = ly + 2 - dy * kTY;
-        const long rowoff = (long)d * kHBox + (bz * kHY + by) * kHX;
-        const int rowt = (tzz * nb1 + tyy) * nb0;
-        if (lx < 2) {
-          const int tl = rowt + txl;
-          if (live[tl]) s += __ldg(box + (long)tl * 3 * kHBox + rowoff + 18 + lx);
-        }
-        const int tm = rowt + tx;
-        if (live[tm]) s += __ldg(box + (long)tm * 3 * kHBox + rowoff + 2 + lx);
-        if (lx >= 14) {
-          const int tr = rowt + txr;
-          if (live[tr]) s += __ldg(box + (long)tr * 3 * kHBox + rowoff + lx - 14);
-        }
-      }
+      const int tyy = (ty + dy + nb1) % nb1, by = ly + 2 - dy * kTY;
+      const long rowoff = (long)d * kHBox + (bz * kHY + by) * kHX;
+      const int rowt = (tzz * nb1 + tyy) * nb0;
+      vm[q] = __ldg(box + (long)(rowt + tx) * 3 * kHBox + rowoff + 2 + lx);
+      lm[q] = __ldg(live + rowt + tx);
+      ve[q] = edge ? __ldg(box + (long)(rowt + txe) * 3 * kHBox + rowoff + ce) : 0.0f;
+      le[q] = edge ? __ldg(live + rowt + txe) : 0;
+    }
+    // fixed order: dz, dy ascending, then dx ascending (tx-1, tx, tx+1)
+    float s = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const bool use = ((q & 2) == 0 || dz1 != dz0) && ((q & 1) == 0 || dy1 != dy0);
+      if (!use) continue;
+      if (lx < 2 && le[q]) s += ve[q];
+      if (lm[q]) s += vm[q];
+      if (lx >= 14 && le[q]) s += ve[q];
     }
     T* dst = f + ((long)(d * nz + tz * kTZ + lz) * ny + ty * kTY + ly) * nx + tx * kTX + lx;
     *dst = accumulate ? (T)((double)*dst + (double)s) : (T)s;
