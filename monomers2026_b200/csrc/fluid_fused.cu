@@ -605,9 +605,9 @@ template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
   if ((rc = al((void**)&z->symy, sizeof(double) * 2 * s->ny))) return rc;
   if ((rc = al((void**)&z->symz, sizeof(double) * 2 * s->nz))) return rc;
   if ((rc = al((void**)&z->d_step, sizeof(uint64_t)))) return rc;
-  CUF(cudaMemset(z->u, 0, sizeof(T) * 3 * N));
-  CUF(cudaMemset(z->uhat, 0, sizeof(C) * 3 * N2));
-  CUF(cudaMemset(z->d_step, 0, sizeof(uint64_t)));
+  CUF(cudaMemsetAsync(z->u, 0, sizeof(T) * 3 * N, s->st));
+  CUF(cudaMemsetAsync(z->uhat, 0, sizeof(C) * 3 * N2, s->st));
+  CUF(cudaMemsetAsync(z->d_step, 0, sizeof(uint64_t), s->st));
   const int nn[3] = {s->nx, s->ny, s->nz};
   double* tabs[3] = {z->symx, z->symy, z->symz};
   for (int a = 0; a < 3; a++) {
@@ -617,7 +617,8 @@ template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
       h[2 * t] = -2.0 * sh * sh;                 // cos(theta) - 1
       h[2 * t + 1] = sin(2.0 * M_PI * t / nn[a]);  // sin(theta)
     }
-    CUF(cudaMemcpy(tabs[a], h.data(), sizeof(double) * 2 * nn[a], cudaMemcpyHostToDevice));
+    CUF(cudaMemcpyAsync(tabs[a], h.data(), sizeof(double) * 2 * nn[a], cudaMemcpyHostToDevice, s->st));
+    CUF(cudaStreamSynchronize(s->st));
   }
   z->plan = plan_for<T>(s->nx, s->ny, s->nz);
   z->fast = fast_size(s->nx) && s->nx == s->ny && s->nx == s->nz;

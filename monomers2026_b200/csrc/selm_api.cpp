@@ -52,9 +52,11 @@ int selm_fail(int code, const std::string& msg) {
 // would wait for the batch at every admission and retirement; from the pool
 // neither call waits for other streams' work.  The pool keeps freed memory
 // for the next simulation (release threshold: never), so a steady stream of
-// jobs reuses the same memory.  Each allocation waits for its own stream
-// only (idle at creation), so the synchronous copies and sets that
-// initialise the buffers see them allocated.
+// jobs reuses the same memory.  Recycled memory holds what its last owner
+// left, so every allocation is zero-filled on the simulation's stream (the
+// counters and bucket counts that kernels add into start from zero, as on
+// the first use of fresh device pages); each allocation then waits for its
+// own stream only (idle at creation).
 namespace {
 constexpr int kMaxPoolDevices = 64;
 std::mutex g_pool_mu;
@@ -88,6 +90,7 @@ int sim_alloc(selm_sim* s, void** p, size_t bytes) {
   cudaMemPool_t pool = nullptr;
   cudaError_t e = device_pool(&pool);
   if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes, pool, s->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, bytes, s->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -152,7 +155,11 @@ static int make_tables(std::vector<void*>& allocs, const int dims[3], FftTables<
         if (cudaMalloc((void**)&d, sizeof(C) * n[a]) != cudaSuccess) return SELM_ERR_NOMEM;
         allocs.push_back(d);
       }
-      if (cudaMemcpy(d, w.data(), sizeof(C) * n[a], cudaMemcpyHostToDevice) != cudaSuccess) return SELM_ERR_CUDA;
+      // a simulation's tables on its stream (its kernels are not ordered after the legacy stream)
+      if (s ? (cudaMemcpyAsync(d, w.data(), sizeof(C) * n[a], cudaMemcpyHostToDevice, s->st) != cudaSuccess ||
+               cudaStreamSynchronize(s->st) != cudaSuccess)
+            : cudaMemcpy(d, w.data(), sizeof(C) * n[a], cudaMemcpyHostToDevice) != cudaSuccess)
+        return SELM_ERR_CUDA;
       ptr[2 * a + sgn] = d;
     }
   }
@@ -254,7 +261,7 @@ int engine_allocate_grid(selm_sim* s) {
   int rc;
   const long N = s->N, N2 = s->N2;
   if ((rc = dalloc(s, &s->err, 1))) return rc;
-  CU(cudaMemset(s->err, 0, sizeof(uint32_t)));
+  CU(cudaMemsetAsync(s->err, 0, sizeof(uint32_t), s->st));
   CU(spread_prepare_attributes());
   if ((rc = make_tables<double>(s->allocs, s->prm.num_mesh_pts, s->tb64, s))) return selm_fail(rc, "FFT tables");
   if ((rc = make_tables<float>(s->allocs, s->prm.num_mesh_pts, s->tb32, s))) return selm_fail(rc, "FFT tables");
@@ -266,9 +273,9 @@ int engine_allocate_grid(selm_sim* s) {
     if ((rc = dalloc(s, &s->work64, 6 * N2))) return rc;  // 3 components x N2 complex
     if ((rc = dalloc(s, &s->partial, 3 * kSumParts))) return rc;
     if ((rc = dalloc(s, &s->sum, 3))) return rc;
-    CU(cudaMemset(s->u64[0], 0, sizeof(double) * 3 * N));
-    CU(cudaMemset(s->u64[1], 0, sizeof(double) * 3 * N));
-    CU(cudaMemset(s->fg64, 0, sizeof(double) * 3 * N));
+    CU(cudaMemsetAsync(s->u64[0], 0, sizeof(double) * 3 * N, s->st));
+    CU(cudaMemsetAsync(s->u64[1], 0, sizeof(double) * 3 * N, s->st));
+    CU(cudaMemsetAsync(s->fg64, 0, sizeof(double) * 3 * N, s->st));
   } else {
     rc = fused_allocate(s);
     if (rc) return rc;
@@ -321,17 +328,17 @@ static int alloc_slots(selm_sim* s, const BinSpec& bs, TileSlots& ts, int M) {
     if ((rc = dalloc(s, &ts.live, ntiles))) return rc;
     if ((rc = dalloc(s, &ts.tmax, ntiles))) return rc;
     if ((rc = dalloc(s, &ts.quirk, ntiles))) return rc;
-    CU(cudaMemset(ts.tmax, 0, sizeof(unsigned long long) * ntiles));
-    CU(cudaMemset(ts.quirk, 0, sizeof(int) * ntiles));
+    CU(cudaMemsetAsync(ts.tmax, 0, sizeof(unsigned long long) * ntiles, s->st));
+    CU(cudaMemsetAsync(ts.quirk, 0, sizeof(int) * ntiles, s->st));
   }
   if ((rc = dalloc(s, &ts.count, ntiles))) return rc;
   if ((rc = dalloc(s, &ts.slots, ntiles * cap))) return rc;
   if ((rc = dalloc(s, &ts.ovf, (size_t)ts.ovf_cap))) return rc;
   if ((rc = dalloc(s, &ts.ovf_count, 1))) return rc;
   if ((rc = dalloc(s, &ts.done, 1))) return rc;
-  CU(cudaMemset(ts.count, 0, sizeof(int) * ntiles));
-  CU(cudaMemset(ts.ovf_count, 0, sizeof(int)));
-  CU(cudaMemset(ts.done, 0, sizeof(unsigned)));
+  CU(cudaMemsetAsync(ts.count, 0, sizeof(int) * ntiles, s->st));
+  CU(cudaMemsetAsync(ts.ovf_count, 0, sizeof(int), s->st));
+  CU(cudaMemsetAsync(ts.done, 0, sizeof(unsigned), s->st));
   return SELM_OK;
 }
 
@@ -562,14 +569,17 @@ extern "C" int selm_set_topology(selm_sim* s, const selm_topology* tp) {
   auto up_i = [&](const std::vector<int>& h, int** d) -> int {
     int r = dalloc(s, d, h.size());
     if (r) return r;
-    if (!h.empty() && cudaMemcpy(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (!h.empty() && (cudaMemcpyAsync(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, s->st) != cudaSuccess ||
+                       cudaStreamSynchronize(s->st) != cudaSuccess))
       return SELM_ERR_CUDA;
     return SELM_OK;
   };
   auto up_d = [&](const double* h, size_t n, double** d) -> int {
     int r = dalloc(s, d, n);
     if (r) return r;
-    if (n && h && cudaMemcpy(*d, h, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess) return SELM_ERR_CUDA;
+    if (n && h && (cudaMemcpyAsync(*d, h, sizeof(double) * n, cudaMemcpyHostToDevice, s->st) != cudaSuccess ||
+                   cudaStreamSynchronize(s->st) != cudaSuccess))
+      return SELM_ERR_CUDA;
     return SELM_OK;
   };
   ForceTopo& T = s->topo;
@@ -652,14 +662,15 @@ extern "C" int selm_set_topology(selm_sim* s, const selm_topology* tp) {
     for (int k = 0; k < 3; k++) NL.wtab[k + 1] = tp->special_lj[k];
     if ((rc = alloc_bins(s, s->fcells, s->fbb, M))) return rc;
     const long nbk = (long)nc * nc * nc;
-    CU(cudaMemset(s->fbb.counts, 0, sizeof(int) * (nbk + 1)));
+    CU(cudaMemsetAsync(s->fbb.counts, 0, sizeof(int) * (nbk + 1), s->st));
     if ((rc = dalloc(s, &NL.idx, (size_t)cap * M))) return rc;
     if ((rc = dalloc(s, &NL.cnt, M))) return rc;
     if ((rc = dalloc(s, &NL.xb, 3L * M))) return rc;
     if ((rc = dalloc(s, &NL.xs, 3L * M))) return rc;
     if ((rc = dalloc(s, &NL.flag, 1))) return rc;
     const int one = 1;  // first build at the next force evaluation
-    CU(cudaMemcpy(NL.flag, &one, sizeof(int), cudaMemcpyHostToDevice));
+    CU(cudaMemcpyAsync(NL.flag, &one, sizeof(int), cudaMemcpyHostToDevice, s->st));
+    CU(cudaStreamSynchronize(s->st));
   }
   s->have_topo = true;
   s->cb = nullptr;
