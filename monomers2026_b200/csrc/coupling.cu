@@ -1274,47 +1274,52 @@ template <typename T>
 __global__ void __launch_bounds__(kFoldThreads) k_spread_fold_rows(T* __restrict__ f, int accumulate,
                                                                    const float* __restrict__ box,
                                                                    const int* __restrict__ live, BinSpec bs) {
-  static_assert(kTX == 16, "16-cell rows");
+  static_assert(kTX == 16 && kTY == 8, "16-cell rows, row pairs (y even, y + 1) in a warp");
+  __shared__ int nbt[27];      // neighbour tile (dz, dy, dx) at ((dz+1) 3 + dy+1) 3 + dx+1
+  __shared__ int nbl[27];      // its live flag
   const int tb = blockIdx.x, d = blockIdx.y;
   const int nb0 = bs.nb[0], nb1 = bs.nb[1], nb2 = bs.nb[2];
   const int tx = tb % nb0, ty = (tb / nb0) % nb1, tz = tb / (nb0 * nb1);
-  const int txl = (tx == 0) ? nb0 - 1 : tx - 1, txr = (tx == nb0 - 1) ? 0 : tx + 1;
+  if (threadIdx.x < 27) {
+    const int k = threadIdx.x;
+    const int dz = k / 9 - 1, dy = (k / 3) % 3 - 1, dx = k % 3 - 1;
+    const int t = (((tz + dz + nb2) % nb2) * nb1 + (ty + dy + nb1) % nb1) * nb0 + (tx + dx + nb0) % nb0;
+    nbt[k] = t;
+    nbl[k] = live[t];
+  }
+  __syncthreads();
   const int lx = threadIdx.x & 15;
   const int nx = bs.n[0], ny = bs.n[1], nz = bs.n[2];
   constexpr int kRowsPerPass = kFoldThreads / 16;
-  // each lane's x neighbour (tx-1 for cells 0, 1; tx+1 for 14, 15; none else)
-  const int txe = (lx < 2) ? txl : txr;
+  const int dxe = (lx < 2) ? 0 : 2;  // the x neighbour of an edge lane: tx-1 for cells 0, 1; tx+1 for 14, 15
   const int ce = (lx < 2) ? 18 + lx : lx - 14;
   const bool edge = (lx < 2) || (lx >= 14);
   for (int r = threadIdx.x >> 4; r < kTY * kTZ; r += kRowsPerPass) {
-    const int ly = r % kTY, lz = r / kTY;
-    // up to 2 x 2 (dz, dy) pairs; every load is issued before any is used (the
-    // boxes of empty tiles hold stale values, dropped by the live flags)
+    const int ly = r & (kTY - 1), lz = r / kTY;
+    // the (dz, dy) pairs of this row, the same for both rows of a warp
     const int dz0 = (lz < 2) ? -1 : 0, dz1 = (lz >= kTZ - 2) ? 1 : 0;
     const int dy0 = (ly < 2) ? -1 : 0, dy1 = (ly >= kTY - 2) ? 1 : 0;
     float vm[4], ve[4];
-    int lm[4], le[4];
+    bool um[4], ue[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int dz = (q & 2) ? dz1 : dz0, dy = (q & 1) ? dy1 : dy0;
-      const int tzz = (tz + dz + nb2) % nb2, bz = lz + 2 - dz * kTZ;
-      const int tyy = (ty + dy + nb1) % nb1, by = ly + 2 - dy * kTY;
+      const bool use = ((q & 2) == 0 || dz1 != dz0) && ((q & 1) == 0 || dy1 != dy0);
+      const int k = ((dz + 1) * 3 + dy + 1) * 3;
+      const int bz = lz + 2 - dz * kTZ, by = ly + 2 - dy * kTY;
       const long rowoff = (long)d * kHBox + (bz * kHY + by) * kHX;
-      const int rowt = (tzz * nb1 + tyy) * nb0;
-      vm[q] = __ldg(box + (long)(rowt + tx) * 3 * kHBox + rowoff + 2 + lx);
-      lm[q] = __ldg(live + rowt + tx);
-      ve[q] = edge ? __ldg(box + (long)(rowt + txe) * 3 * kHBox + rowoff + ce) : 0.0f;
-      le[q] = edge ? __ldg(live + rowt + txe) : 0;
+      um[q] = use && nbl[k + 1];
+      ue[q] = use && edge && nbl[k + dxe];
+      vm[q] = um[q] ? __ldg(box + (long)nbt[k + 1] * 3 * kHBox + rowoff + 2 + lx) : 0.0f;
+      ve[q] = ue[q] ? __ldg(box + (long)nbt[k + dxe] * 3 * kHBox + rowoff + ce) : 0.0f;
     }
     // fixed order: dz, dy ascending, then dx ascending (tx-1, tx, tx+1)
     float s = 0.0f;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      const bool use = ((q & 2) == 0 || dz1 != dz0) && ((q & 1) == 0 || dy1 != dy0);
-      if (!use) continue;
-      if (lx < 2 && le[q]) s += ve[q];
-      if (lm[q]) s += vm[q];
-      if (lx >= 14 && le[q]) s += ve[q];
+      if (lx < 2 && ue[q]) s += ve[q];
+      if (um[q]) s += vm[q];
+      if (lx >= 14 && ue[q]) s += ve[q];
     }
     T* dst = f + ((long)(d * nz + tz * kTZ + lz) * ny + ty * kTY + ly) * nx + tx * kTX + lx;
     *dst = accumulate ? (T)((double)*dst + (double)s) : (T)s;
