@@ -156,20 +156,14 @@ __global__ void __launch_bounds__(kNlBuildThreads) k_nl_build(const double* __re
     scan(offsets[0], offsets[1]);
   } else {
     const int cx = force_cell(xi, t.lo, L, nc), cy = force_cell(yi, t.lo, L, nc), cz = force_cell(zi, t.lo, L, nc);
-    // the three x-neighbour cells of a (y, z) row are contiguous in the cell
-    // order, except across the periodic edge (two ranges there)
+    // the 27 cells around i's cell, each its own range (nc >= 3: all distinct)
     for (int oz = -1; oz <= 1; oz++) {
-      const int zc = wrapi(cz + oz, nc) * nc;
+      const int zc = wrapi(cz + oz, nc);
       for (int oy = -1; oy <= 1; oy++) {
-        const int rowc = (zc + wrapi(cy + oy, nc)) * nc;
-        if (cx >= 1 && cx <= nc - 2) {
-          scan(offsets[rowc + cx - 1], offsets[rowc + cx + 2]);
-        } else if (cx == 0) {
-          scan(offsets[rowc + nc - 1], offsets[rowc + nc]);
-          scan(offsets[rowc], offsets[rowc + 2]);
-        } else {
-          scan(offsets[rowc + nc - 2], offsets[rowc + nc]);
-          scan(offsets[rowc], offsets[rowc + 1]);
+        const int rowc = (zc * nc + wrapi(cy + oy, nc)) * nc;
+        for (int ox = -1; ox <= 1; ox++) {
+          const int c = rowc + wrapi(cx + ox, nc);
+          scan(offsets[c], offsets[c + 1]);
         }
       }
     }
