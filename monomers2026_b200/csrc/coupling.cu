@@ -803,6 +803,10 @@ __device__ __forceinline__ int spread_rot(int cx, int cz, int d) { return (cx + 
 __device__ __forceinline__ long long to_fixed(float v) { return __float2ll_rn(v); }
 __device__ __forceinline__ long long to_fixed(double v) { return __double2ll_rn(v); }
 
+__device__ __forceinline__ int round_small(float v) {  // rint(v) for |v| < 2^22
+  return __float_as_int(v + 12582912.0f) - 0x4B400000;
+}
+
 template <typename T> struct alignas(4 * sizeof(T)) Vec4 { T v[4]; };
 
 // Tile geometry and fixed-point state shared by the plane additions of a block.
@@ -1087,10 +1091,6 @@ constexpr int kHomeSplitK = 11;  // single-word path for n <= 2^11
 static_assert(kHX % 32 == 20 && (kHX * kHY) % 32 == 16, "bank pattern of the box atomics");
 constexpr size_t kHomeSmem = sizeof(unsigned) * 3 * kHBox;  // 57,600 B
 
-__device__ __forceinline__ int round_small(float v) {  // rint(v) for |v| < 2^22
-  return __float_as_int(v + 12582912.0f) - 0x4B400000;
-}
-
 template <int SPLIT>
 __device__ __forceinline__ void home_add(const int* __restrict__ ids, int n_prim, int n_ovf, const TileSlots& ts, int tb,
                                          int dsel, double scale, int L, unsigned* acc,
@@ -1199,8 +1199,8 @@ __global__ void __launch_bounds__(kHomeThreads, 3) k_spread_home(const double* _
   const int n_ovf = (n > n_prim) ? min(*ts.ovf_count, ts.ovf_cap) : 0;
   float* out = ts.box + (long)tb * 3 * kHBox;
   if (tid == 0) ts.live[tb] = (n > 0);
-  if (n > 0) {
-    const double m = __longlong_as_double((long long)ts.tmax[tb]);  // largest |impulse| of the tile
+  {
+    const double m = __longlong_as_double((long long)ts.tmax[tb]);  // largest |impulse| of the tile (0 if none)
     const bool bad = !(m <= 1.0e300);
     const int ew = ts.quirk[tb] ? 0 : -3;
     uint4* z4 = reinterpret_cast<uint4*>(hacc);
@@ -1220,7 +1220,13 @@ __global__ void __launch_bounds__(kHomeThreads, 3) k_spread_home(const double* _
         if (S >= -100 && S <= 100) {
           // the integer rounded to FP32 once, then scaled by a power of two (exact)
           const float inv = ldexpf(1.0f, -S);
-          for (int i = tid; i < 3 * kHBox; i += kHomeThreads) out[i] = __int2float_rn((int)hacc[i]) * inv;
+          const uint4* h4 = reinterpret_cast<const uint4*>(hacc);
+          float4* o4 = reinterpret_cast<float4*>(out);
+          for (int i = tid; i < 3 * kHBox / 4; i += kHomeThreads) {
+            const uint4 h = h4[i];
+            o4[i] = make_float4(__int2float_rn((int)h.x) * inv, __int2float_rn((int)h.y) * inv,
+                                __int2float_rn((int)h.z) * inv, __int2float_rn((int)h.w) * inv);
+          }
         } else {
           const double inv = ldexp(1.0, -S);
           for (int i = tid; i < 3 * kHBox; i += kHomeThreads) out[i] = (float)((double)(int)hacc[i] * inv);
@@ -1259,70 +1265,82 @@ __global__ void __launch_bounds__(kHomeThreads, 3) k_spread_home(const double* _
 }
 
 // The fold on grids whose sizes are multiples of the tile (every tile full):
-// block per (tile, component), a half-warp per 16-cell x-row (y, z) of the
-// tile and a lane per cell, so that loads and stores are 64-byte runs.  A
-// row's cells lie in the boxes of the tiles dz, dy in {-1, 0, 1} (the
-// neighbour along y or z only for the 2 rows next to that face) and dx in
-// {-1, 0, 1}: box row (z + 2 - dz T_z, y + 2 - dy T_y) of tile (tx, ty+dy,
-// tz+dz) holds cell x at column x + 2, the same row of tile tx-1 holds cells
-// 0, 1 at its columns 18, 19, and of tile tx+1 cells 14, 15 at its columns
-// 0, 1.  Per cell the order of addition is fixed: dz, then dy, then dx, each
-// ascending.  Tiles one or two per axis wrap onto themselves: the same rule
-// holds, with tx-1 and tx+1 naming the same tile.
-constexpr int kFoldThreads = 256;
+// block per (tile, component), a thread per (x, y) column of the tile that
+// walks its 16 cells along z, so that a half-warp reads 64-byte runs of box
+// rows.  Cell (x, y, z) of tile (tx, ty, tz) lies in the boxes of the tiles
+// (tx + dx, ty + dy, tz + dz): dx = 0 at box column x + 2, dx = -1 (cells
+// 0, 1) at column x + T_x + 2, dx = +1 (cells T_x - 2, T_x - 1) at column
+// x - T_x + 2, and the same along y and z.  Per cell the order of addition is
+// fixed: dz, then dy, then dx, each ascending.  Tiles one or two per axis wrap
+// onto themselves: the same rule holds, with tx-1 and tx+1 naming the same
+// tile.  Every box is written, zeros for a tile without monomers.
 template <typename T>
-__global__ void __launch_bounds__(kFoldThreads) k_spread_fold_rows(T* __restrict__ f, int accumulate,
-                                                                   const float* __restrict__ box,
-                                                                   const int* __restrict__ live, BinSpec bs) {
-  static_assert(kTX == 16 && kTY == 8, "16-cell rows, row pairs (y even, y + 1) in a warp");
-  __shared__ int nbt[27];      // neighbour tile (dz, dy, dx) at ((dz+1) 3 + dy+1) 3 + dx+1
-  __shared__ int nbl[27];      // its live flag
+__global__ void __launch_bounds__(kTX * kTY) k_spread_fold_cols(T* __restrict__ f, int accumulate,
+                                                               const float* __restrict__ box, BinSpec bs) {
   const int tb = blockIdx.x, d = blockIdx.y;
-  const int nb0 = bs.nb[0], nb1 = bs.nb[1], nb2 = bs.nb[2];
-  const int tx = tb % nb0, ty = (tb / nb0) % nb1, tz = tb / (nb0 * nb1);
-  if (threadIdx.x < 27) {
-    const int k = threadIdx.x;
-    const int dz = k / 9 - 1, dy = (k / 3) % 3 - 1, dx = k % 3 - 1;
-    const int t = (((tz + dz + nb2) % nb2) * nb1 + (ty + dy + nb1) % nb1) * nb0 + (tx + dx + nb0) % nb0;
-    nbt[k] = t;
-    nbl[k] = live[t];
+  const int nbx = bs.nb[0], nby = bs.nb[1], nbz = bs.nb[2];
+  const int tx = tb % nbx, ty = (tb / nbx) % nby, tz = tb / (nbx * nby);
+  const int lx = threadIdx.x % kTX, ly = threadIdx.x / kTX;
+  // (tile, box coordinate) along x and y, in ascending order of the offset
+  int xt0 = tx, xc0 = lx + 2, xt1 = tx, xc1 = lx + 2, nxe = 1;
+  if (lx < 2) {
+    xt0 = (tx == 0 ? nbx : tx) - 1;
+    xc0 = lx + kTX + 2;
+    nxe = 2;
+  } else if (lx >= kTX - 2) {
+    xt1 = (tx + 1 == nbx) ? 0 : tx + 1;
+    xc1 = lx - kTX + 2;
+    nxe = 2;
   }
-  __syncthreads();
-  const int lx = threadIdx.x & 15;
-  const int nx = bs.n[0], ny = bs.n[1], nz = bs.n[2];
-  constexpr int kRowsPerPass = kFoldThreads / 16;
-  const int dxe = (lx < 2) ? 0 : 2;  // the x neighbour of an edge lane: tx-1 for cells 0, 1; tx+1 for 14, 15
-  const int ce = (lx < 2) ? 18 + lx : lx - 14;
-  const bool edge = (lx < 2) || (lx >= 14);
-  for (int r = threadIdx.x >> 4; r < kTY * kTZ; r += kRowsPerPass) {
-    const int ly = r & (kTY - 1), lz = r / kTY;
-    // the (dz, dy) pairs of this row, the same for both rows of a warp
-    const int dz0 = (lz < 2) ? -1 : 0, dz1 = (lz >= kTZ - 2) ? 1 : 0;
-    const int dy0 = (ly < 2) ? -1 : 0, dy1 = (ly >= kTY - 2) ? 1 : 0;
-    float vm[4], ve[4];
-    bool um[4], ue[4];
+  int yt0 = ty, yr0 = ly + 2, yt1 = ty, yr1 = ly + 2, nye = 1;
+  if (ly < 2) {
+    yt0 = (ty == 0 ? nby : ty) - 1;
+    yr0 = ly + kTY + 2;
+    nye = 2;
+  } else if (ly >= kTY - 2) {
+    yt1 = (ty + 1 == nby) ? 0 : ty + 1;
+    yr1 = ly - kTY + 2;
+    nye = 2;
+  }
+  // the (y, x) part of the box offsets: entries (y0, x0), (y0, x1), (y1, x0), (y1, x1)
+  long po[4];
+  bool pu[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int dz = (q & 2) ? dz1 : dz0, dy = (q & 1) ? dy1 : dy0;
-      const bool use = ((q & 2) == 0 || dz1 != dz0) && ((q & 1) == 0 || dy1 != dy0);
-      const int k = ((dz + 1) * 3 + dy + 1) * 3;
-      const int bz = lz + 2 - dz * kTZ, by = ly + 2 - dy * kTY;
-      const long rowoff = (long)d * kHBox + (bz * kHY + by) * kHX;
-      um[q] = use && nbl[k + 1];
-      ue[q] = use && edge && nbl[k + dxe];
-      vm[q] = um[q] ? __ldg(box + (long)nbt[k + 1] * 3 * kHBox + rowoff + 2 + lx) : 0.0f;
-      ve[q] = ue[q] ? __ldg(box + (long)nbt[k + dxe] * 3 * kHBox + rowoff + ce) : 0.0f;
+  for (int q = 0; q < 4; q++) {
+    const int ye = q >> 1, xe = q & 1;
+    pu[q] = ye < nye && xe < nxe;
+    const int t = (ye ? yt1 : yt0) * nbx + (xe ? xt1 : xt0);
+    po[q] = ((long)t * 3 + d) * kHBox + (ye ? yr1 : yr0) * kHX + (xe ? xc1 : xc0);
+  }
+  const long tzs = (long)nbx * nby * 3 * kHBox;  // one tile along z in the box buffer
+  const int nx = bs.n[0], ny = bs.n[1], nz = bs.n[2];
+  T* dst = f + ((long)(d * nz + tz * kTZ) * ny + ty * kTY + ly) * nx + tx * kTX + lx;
+  for (int lz = 0; lz < kTZ; lz++) {
+    int zt0 = tz, zp0 = lz + 2, zt1 = tz, zp1 = lz + 2, nze = 1;
+    if (lz < 2) {
+      zt0 = (tz == 0 ? nbz : tz) - 1;
+      zp0 = lz + kTZ + 2;
+      nze = 2;
+    } else if (lz >= kTZ - 2) {
+      zt1 = (tz + 1 == nbz) ? 0 : tz + 1;
+      zp1 = lz - kTZ + 2;
+      nze = 2;
     }
-    // fixed order: dz, dy ascending, then dx ascending (tx-1, tx, tx+1)
+    float v[2][4];
+#pragma unroll
+    for (int ze = 0; ze < 2; ze++) {
+      const long zo = (ze ? zt1 : zt0) * tzs + (long)(ze ? zp1 : zp0) * (kHY * kHX);
+#pragma unroll
+      for (int q = 0; q < 4; q++) v[ze][q] = (ze < nze && pu[q]) ? __ldg(box + zo + po[q]) : 0.0f;
+    }
     float s = 0.0f;
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      if (lx < 2 && ue[q]) s += ve[q];
-      if (um[q]) s += vm[q];
-      if (lx >= 14 && ue[q]) s += ve[q];
-    }
-    T* dst = f + ((long)(d * nz + tz * kTZ + lz) * ny + ty * kTY + ly) * nx + tx * kTX + lx;
-    *dst = accumulate ? (T)((double)*dst + (double)s) : (T)s;
+    for (int ze = 0; ze < 2; ze++)
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (ze < nze && pu[q]) s += v[ze][q];
+    T* o = dst + (long)lz * ny * nx;
+    *o = accumulate ? (T)((double)*o + (double)s) : (T)s;
   }
 }
 
@@ -1499,11 +1517,11 @@ cudaError_t spread_slots(T* fgrid, bool accumulate, const double* x_old, const d
       if (!ts.box || !ts.live || !rec) return cudaErrorInvalidValue;
       if (!ts.tmax || !ts.quirk) return cudaErrorInvalidValue;
       k_spread_home<<<ntiles, kHomeThreads, kHomeSmem, st>>>(tf, ts, rec);
-      bool full = true;  // every tile full: the row fold
+      bool full = true;  // every tile full: the column fold
       for (int ax = 0; ax < 3; ax++) full &= (bs.n[ax] % bs.tile[ax] == 0);
       if (full) {
-        k_spread_fold_rows<T><<<dim3((unsigned)ntiles, 3), kFoldThreads, 0, st>>>(fgrid, accumulate ? 1 : 0, ts.box,
-                                                                                 ts.live, bs);
+        k_spread_fold_cols<T><<<dim3((unsigned)ntiles, 3), kTX * kTY, 0, st>>>(fgrid, accumulate ? 1 : 0, ts.box,
+                                                                               bs);
         count_launches(2);
         return cudaGetLastError();
       }

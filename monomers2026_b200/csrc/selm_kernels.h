@@ -82,8 +82,9 @@ struct TileSlots {
   BinSpec bs{};               // the spread tiles (mode 2)
   // home mode (FP32 grids): a monomer is filed once, under the tile of its
   // cell floor((x - lo)/dx); the spread accumulates each tile's monomers into
-  // a box of the tile plus a 2-cell halo, written to box[], and a fold pass
-  // sums the boxes that cover each cell.  live[t] = tile t had monomers.
+  // a box of the tile plus a 2-cell halo, written to box[] (zeros for a tile
+  // without monomers), and a fold pass sums the boxes that cover each cell.
+  // live[t] = tile t had monomers.
   // The interpolation also leaves, per tile, the largest |impulse| of its
   // monomers (tmax: the bits of the FP64 value, which order as unsigned
   // integers for non-negative values, NaN above all) and whether a weight
