@@ -470,26 +470,23 @@ __device__ __forceinline__ int home_cell(double g, int n, bool& low_half) {
   return wrapi((int)fl, n);
 }
 
-// Home mode: the coordinates, in the home tile's box (the tile plus 2 cells
-// on each side), of the stencil bases that the thread of component d stores
-// in the record (axis d unshifted, axis d+1 shifted; record_store's split, so
-// the three threads write distinct bytes).  With home cell c (tile origin t0)
-// the unshifted base floor(g) - 1 sits at c - t0 + 1, the shifted base
-// floor(g - 1/2) - 1 at c - t0 or c - t0 + 1: always in [0, tile], and the
-// 4 stencil points stay inside the box.
-__device__ __forceinline__ void home_box_store(unsigned char (&hb)[3][2], int d, double gx, double gy, double gz,
-                                               const BinSpec& bs) {
+// Home mode: the slot, in the home tile's box (the tile plus 2 cells on each
+// side, x fastest), of component d's stencil base, from the thread of that
+// component.  With home cell c (tile origin t0) the unshifted base
+// floor(g) - 1 sits at box coordinate c - t0 + 1, the shifted base
+// floor(g - 1/2) - 1 at c - t0 or c - t0 + 1: always in [0, tile], and the 4
+// stencil points stay inside the box.
+__device__ __forceinline__ void home_slot_store(unsigned short (&hs)[3], int d, double gx, double gy, double gz,
+                                                const BinSpec& bs) {
   const double g[3] = {gx, gy, gz};
-  const int a1 = (d + 1) % 3;
+  int c[3];
 #pragma unroll
   for (int ax = 0; ax < 3; ax++) {
-    if (ax == d || ax == a1) {
-      bool low;
-      const int c = home_cell(g[ax], bs.n[ax], low);
-      const int l = c % bs.tile[ax];
-      hb[ax][ax == d ? 0 : 1] = (unsigned char)((ax == d) ? l + 1 : (low ? l : l + 1));
-    }
+    bool low;
+    const int l = home_cell(g[ax], bs.n[ax], low) % bs.tile[ax];
+    c[ax] = (ax == d) ? l + 1 : (low ? l : l + 1);
   }
+  hs[d] = (unsigned short)((c[2] * (bs.tile[1] + 4) + c[1]) * (bs.tile[0] + 4) + c[0]);
 }
 
 // Home mode: the tile of the monomer's cell.
@@ -608,7 +605,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_interp_update(c
   const T val = stencil_gather<T>(u + d * N, base, w, a);
   if (rec) {
     record_store<T>(rec[p], d, base, w, a);
-    if (ts.home) home_box_store(rec[p].hb, d, gx, gy, gz, ts.bs);
+    if (ts.home) home_slot_store(rec[p].hs, d, gx, gy, gz, ts.bs);
   }
   if (ts.count && d == 0) tile_append(ts, p, gx, gy, gz, err);  // the spread of this step reads x_old
   const double vg = v[g];
@@ -653,7 +650,7 @@ __global__ void __launch_bounds__(256) k_qs_prepare(const double* __restrict__ x
   T w[3][4];
   stencil_of<T>(gx, gy, gz, d, base, w);
   record_store<T>(rec[p], d, base, w, a);
-  if (ts.home) home_box_store(rec[p].hb, d, gx, gy, gz, ts.bs);
+  if (ts.home) home_slot_store(rec[p].hs, d, gx, gy, gz, ts.bs);
   if (ts.count && d == 0) tile_append(ts, p, gx, gy, gz, err);
   tf_out[gid] = -f[gid] * inv_dv;
   if (ts.home) home_scale_note<T>(ts, gx, gy, gz, tf_out[gid], w);
@@ -1089,7 +1086,22 @@ constexpr int kHomeThreads = 512;
 constexpr int kHomeWarps = kHomeThreads / 32;
 constexpr int kHomeSplitK = 11;  // single-word path for n <= 2^11
 static_assert(kHX % 32 == 20 && (kHX * kHY) % 32 == 16, "bank pattern of the box atomics");
-constexpr size_t kHomeSmem = sizeof(unsigned) * 3 * kHBox;  // 57,600 B
+static_assert(kHBox <= 65536, "box slots of the stencil records are 16-bit");
+constexpr int kHomeStage = 112;  // candidates staged in shared memory at a time (three blocks per SM)
+constexpr size_t kHomeBoxBytes = sizeof(unsigned) * 3 * kHBox;  // 57,600 B
+constexpr size_t kHomeSmem = kHomeBoxBytes + kHomeStage * (sizeof(WRec<float>) + 3 * sizeof(double));  // 74,624 B
+static_assert(sizeof(WRec<float>) % 16 == 0 && kHomeBoxBytes % 16 == 0, "16-byte staging copies");
+
+// 16- and 8-byte asynchronous copies global -> shared (LDGSTS), and the wait for all of this thread's
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <int SPLIT>
 __device__ __forceinline__ void home_add(const int* __restrict__ ids, int n_prim, int n_ovf, const TileSlots& ts, int tb,
@@ -1101,8 +1113,8 @@ __device__ __forceinline__ void home_add(const int* __restrict__ ids, int n_prim
   auto one2 = [&](int p0, int p1, bool two) {
     const WRec<float>& R0 = rec[p0];
     const WRec<float>& R1 = rec[two ? p1 : p0];
-    const uint2 h0 = *reinterpret_cast<const uint2*>(&R0.hb[0][0]);
-    const uint2 h1 = *reinterpret_cast<const uint2*>(&R1.hb[0][0]);
+    const uint2 h0 = *reinterpret_cast<const uint2*>(&R0.hs[0]);  // hs[0..2] and two bytes of padding
+    const uint2 h1 = *reinterpret_cast<const uint2*>(&R1.hs[0]);
     float wxa[2][2], wya[2][2], wza[2][2][2];
     float wxb[2][2], wyb[2][2], wzb[2][2][2];
 #pragma unroll
@@ -1118,15 +1130,14 @@ __device__ __forceinline__ void home_add(const int* __restrict__ ids, int n_prim
       t0[d] = tf[3L * p0 + d];
       t1[d] = two ? tf[3L * p1 + d] : 0.0;
     }
-    auto add = [&](const uint2 hbw, const float (&wx)[2][2], const float (&wy)[2][2], const float (&wz)[2][2][2],
+    auto add = [&](const uint2 hsw, const float (&wx)[2][2], const float (&wy)[2][2], const float (&wz)[2][2][2],
                    const double (&tv)[3]) {
-      const unsigned char* hb = reinterpret_cast<const unsigned char*>(&hbw);
+      const unsigned short* hs = reinterpret_cast<const unsigned short*>(&hsw);
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         const int sx = (d != 0), sy = (d != 1), sz = (d != 2);
-        const int bx = hb[0 + sx], by = hb[2 + sy], bz = hb[4 + sz];
         const float A = (float)(-tv[d] * scale) * wy[sy][0] * wx[sx][0];
-        const int slot = d * kHBox + (bz * kHY + by) * kHX + bx + loff;
+        const int slot = d * kHBox + hs[d] + loff;
         atomicAdd(acc + slot, (unsigned)round_small(A * wz[sz][0][0]));
         atomicAdd(acc + slot + 2 * kHY * kHX, (unsigned)round_small(A * wz[sz][0][1]));
       }
@@ -1136,17 +1147,16 @@ __device__ __forceinline__ void home_add(const int* __restrict__ ids, int n_prim
   };
   auto one = [&](int p) {
     const WRec<float>& R = rec[p];
-    const uint2 hbw = *reinterpret_cast<const uint2*>(&R.hb[0][0]);
-    const unsigned char* hb = reinterpret_cast<const unsigned char*>(&hbw);  // hb[ax * 2 + shifted]
+    const uint2 hsw = *reinterpret_cast<const uint2*>(&R.hs[0]);
+    const unsigned short* hs = reinterpret_cast<const unsigned short*>(&hsw);
 #pragma unroll
     for (int d = 0; d < 3; d++) {
       if (SPLIT && d != dsel) continue;
       const int sx = (d != 0), sy = (d != 1), sz = (d != 2);
-      const int bx = hb[0 + sx], by = hb[2 + sy], bz = hb[4 + sz];
       const float wx = R.w[0][sx][ix], wy = R.w[1][sy][jy];
       const float wz0 = R.w[2][sz][kz], wz1 = R.w[2][sz][kz + 2];
       const float A = (float)(-tf[3L * p + d] * scale) * wy * wx;
-      const int slot = (SPLIT ? 0 : d * kHBox) + (bz * kHY + by) * kHX + bx + loff;
+      const int slot = (SPLIT ? 0 : d * kHBox) + hs[d] + loff;
       if (!SPLIT) {
         atomicAdd(acc + slot, (unsigned)round_small(A * wz0));
         atomicAdd(acc + slot + 2 * kHY * kHX, (unsigned)round_small(A * wz1));
@@ -1170,14 +1180,16 @@ __device__ __forceinline__ void home_add(const int* __restrict__ ids, int n_prim
   if (!SPLIT) {
     // two candidates per pass (their loads overlap), the next pair's indices loaded ahead
     int c = wid;
-    int pa = (c < n_prim) ? ids[c] : 0;
-    int pb = (c + kHomeWarps < n_prim) ? ids[c + kHomeWarps] : 0;
+    // (ids null: the candidates are the records 0 .. n_prim-1 themselves, staged in shared memory)
+    auto id = [&](int q) { return ids ? ids[q] : q; };
+    int pa = (c < n_prim) ? id(c) : 0;
+    int pb = (c + kHomeWarps < n_prim) ? id(c + kHomeWarps) : 0;
     while (c < n_prim) {
       const int p0 = pa, p1 = pb;
       const bool two = c + kHomeWarps < n_prim;
       c += 2 * kHomeWarps;
-      if (c < n_prim) pa = ids[c];
-      if (c + kHomeWarps < n_prim) pb = ids[c + kHomeWarps];
+      if (c < n_prim) pa = id(c);
+      if (c + kHomeWarps < n_prim) pb = id(c + kHomeWarps);
       one2(p0, p1, two);
     }
   } else {
@@ -1192,6 +1204,9 @@ __device__ __forceinline__ void home_add(const int* __restrict__ ids, int n_prim
 __global__ void __launch_bounds__(kHomeThreads, 3) k_spread_home(const double* __restrict__ tf, TileSlots ts,
                                                                  const WRec<float>* __restrict__ rec) {
   extern __shared__ __align__(16) unsigned hacc[];  // [3][kHZ][kHY][kHX], or [2][kHZ][kHY][kHX] (split path)
+  // the staged candidates: their records and impulses
+  WRec<float>* srec = reinterpret_cast<WRec<float>*>(reinterpret_cast<unsigned char*>(hacc) + kHomeBoxBytes);
+  double* stf = reinterpret_cast<double*>(srec + kHomeStage);
   const int tb = blockIdx.x, tid = threadIdx.x;
   const int n = ts.count[tb];
   const int n_prim = min(n, ts.cap);
@@ -1208,14 +1223,41 @@ __global__ void __launch_bounds__(kHomeThreads, 3) k_spread_home(const double* _
       // a non-finite impulse makes the tile non-finite, as a floating-point sum would
       for (int i = tid; i < 3 * kHBox; i += kHomeThreads) out[i] = __int_as_float(0x7fc00000);
     } else {
-      for (int i = tid; i < 3 * kHBox / 4; i += kHomeThreads) z4[i] = make_uint4(0u, 0u, 0u, 0u);
-      __syncthreads();
       const int k = (n > 1) ? 32 - __clz(n - 1) : 1;  // ceil(log2 n)
       int em = 0;
       if (m > 0.0) frexp(m, &em);  // m < 2^em
       if (k <= kHomeSplitK) {
         const int S = max(-1000, min(1000, min(30 - k, 22) - em - ew));
-        home_add<0>(ids, n_prim, n_ovf, ts, tb, 0, ldexp(1.0, S), 0, hacc, tf, rec);
+        const double scale = ldexp(1.0, S);
+        // the candidates' records and impulses go to shared memory in chunks,
+        // each by asynchronous copies that every thread issues at once (the
+        // first chunk's while the box is zeroed), so that their load latency
+        // is paid once per chunk rather than once per candidate pair
+        auto stage = [&](int c0, int nc) {
+          for (int i = tid; i < nc * 8; i += kHomeThreads) {
+            const int c = i >> 3, q = i & 7;
+            cp_async16(reinterpret_cast<unsigned char*>(srec + c) + 16 * q,
+                       reinterpret_cast<const unsigned char*>(rec + ids[c0 + c]) + 16 * q);
+          }
+          for (int i = tid; i < nc * 3; i += kHomeThreads) {
+            const int c = i / 3, q = i - 3 * c;
+            cp_async8(stf + i, tf + 3L * ids[c0 + c] + q);
+          }
+        };
+        int c0 = 0, nc = min(kHomeStage, n_prim);
+        stage(0, nc);
+        for (int i = tid; i < 3 * kHBox / 4; i += kHomeThreads) z4[i] = make_uint4(0u, 0u, 0u, 0u);
+        for (;;) {
+          cp_async_wait_all();
+          __syncthreads();  // the chunk and the zeroed box are visible to every thread
+          home_add<0>(nullptr, nc, 0, ts, tb, 0, scale, 0, hacc, stf, srec);
+          c0 += nc;
+          if (c0 >= n_prim) break;
+          nc = min(kHomeStage, n_prim - c0);
+          __syncthreads();  // every warp is done with the chunk
+          stage(c0, nc);
+        }
+        if (n_ovf > 0) home_add<0>(ids, 0, n_ovf, ts, tb, 0, scale, 0, hacc, tf, rec);
         __syncthreads();
         if (S >= -100 && S <= 100) {
           // the integer rounded to FP32 once, then scaled by a power of two (exact)
@@ -1235,6 +1277,8 @@ __global__ void __launch_bounds__(kHomeThreads, 3) k_spread_home(const double* _
         const int L = 32 - k;
         const int S = max(-1000, min(1000, 62 - 2 * k - em - ew));
         const double inv = ldexp(1.0, -S);
+        for (int i = tid; i < 2 * kHBox / 4; i += kHomeThreads) z4[i] = make_uint4(0u, 0u, 0u, 0u);
+        __syncthreads();
         for (int d = 0; d < 3; d++) {
           if (d > 0) {
             __syncthreads();

@@ -99,8 +99,9 @@ struct TileSlots {
 template <typename T> struct alignas(16) WRec {
   T w[3][2][4];  // weight factors [axis][unshifted, shifted][point] (16-byte aligned rows)
   int b[3][2];   // stencil bases wrapped into [0, n): [axis][unshifted, shifted]
-  // home mode: the bases' coordinates in the home tile's box, [axis][unshifted, shifted]
-  unsigned char hb[3][2];
+  // home mode: per component, the slot of its stencil base in the home tile's
+  // box (the tile plus 2 cells on each side, x fastest), without the component offset
+  unsigned short hs[3];
 };
 // the bases of record 0 and the record stride in ints, for the binning kernels
 template <typename T> inline const int* wrec_bases(const WRec<T>* rec) {
