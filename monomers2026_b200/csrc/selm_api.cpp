@@ -305,11 +305,17 @@ static int alloc_bins(selm_sim* s, const BinSpec& bs, BinBuffers& bb, int M) {
 // Spread-tile slots: a tile holds four times its expected candidate count
 // (plus 64) before its further candidates go to the overflow list, which has
 // room for every entry a monomer can make.
-// FP32 grids file each monomer under its home tile only (home mode), with a
-// box buffer of the tiles' halo-extended boxes for the fold pass.
+// FP32 grids with many monomers file each monomer under its home tile only
+// (home mode), with a box buffer of the tiles' halo-extended boxes for the
+// fold pass.  With few monomers the spread costs its launches more than its
+// additions, and one kernel (k_spread_tiles) beats two: a batch of 256
+// replicas of 50-2000 monomers on 32^3-96^3 grids steps at 44k replica-steps/s
+// against 38k in home mode; at 128^3 with 1e5 monomers home mode takes the
+// spread from 73 to 56 us.
+constexpr int kHomeMinMonomers = 16384;
 static int alloc_slots(selm_sim* s, const BinSpec& bs, TileSlots& ts, int M) {
   const long ntiles = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
-  const bool home = (s->prm.form == SELM_FORM_FUSED32);
+  const bool home = (s->prm.form == SELM_FORM_FUSED32) && M >= kHomeMinMonomers;
   double per = 1.0;  // expected tiles a monomer is filed under (a union stencil is 5 cells per axis)
   if (!home)
     for (int a = 0; a < 3; a++) per *= (bs.nb[a] == 1) ? 1.0 : 1.0 + 4.0 / bs.tile[a];

@@ -36,6 +36,7 @@ from .selm import Batch, Selm
 
 _FP = {"fused32": 4, "fused64": 8, "plain64": 8}
 SPREAD_TILE = (16, 8, 16)  # cells of a spread tile (kTX, kTY, kTZ of the engine)
+HOME_MIN_MONOMERS = 16384  # FP32 simulations with at least this many monomers spread by home tiles
 
 
 def estimate_device_bytes(params, natoms: int, pairs: bool = True) -> int:
@@ -55,7 +56,8 @@ def estimate_device_bytes(params, natoms: int, pairs: bool = True) -> int:
     nb = [-(-n // t) for n, t in zip((nx, ny, nz), tile)]
     tiles = nb[0] * nb[1] * nb[2]
     M = max(1, int(natoms))
-    home = params.form == "fused32"  # FP32 grids: one filing per monomer, plus the tiles' halo boxes
+    # FP32 grids with at least HOME_MIN_MONOMERS: one filing per monomer, plus the tiles' halo boxes
+    home = params.form == "fused32" and M >= HOME_MIN_MONOMERS
     per = 1.0
     if not home:
         for b, t in zip(nb, tile):
