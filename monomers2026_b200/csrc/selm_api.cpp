@@ -90,8 +90,11 @@ int sim_alloc(selm_sim* s, void** p, size_t bytes) {
   cudaMemPool_t pool = nullptr;
   cudaError_t e = device_pool(&pool);
   if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes, pool, s->st);
+  // zero-filled on the simulation's stream, where everything that uses the
+  // memory is ordered after it (other streams join through events, a batch
+  // synchronises the stream on admission); no wait here, so that creating a
+  // simulation beside a running batch does not stall on every allocation
   if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, bytes, s->st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
   if (e != cudaSuccess) {
     cudaGetLastError();
     if (*p) cudaFreeAsync(*p, s->st);

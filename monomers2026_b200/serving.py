@@ -147,6 +147,32 @@ def run_sequential(workloads, steps: int, form: str = "plain64"):
             "replica_steps_per_s": len(workloads) * steps / (total_ms / 1e3)}
 
 
+def run_sequential_jobs(jobs, form: str = "plain64", sample_steps: int = 10):
+    """The serving jobs run one after another, each alone in ``form``: every
+    job's step is device-timed over ``sample_steps`` steps (after one
+    untimed step) and counted for all of its ``nsteps``.  Returns the
+    replica-steps/s of that sequence (creation and read-back not counted)."""
+    import torch
+
+    total_ms = 0.0
+    steps = 0
+    for j in jobs:
+        s = _make(j.workload, form)
+        st = torch.cuda.Stream()
+        s.set_stream(st.cuda_stream)
+        s.run(1)
+        s.synchronize()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s.run(sample_steps)
+        e.record(st)
+        e.synchronize()
+        total_ms += a.elapsed_time(e) / sample_steps * j.nsteps
+        steps += j.nsteps
+        s.final()
+    return {"jobs": len(jobs), "sample_steps": sample_steps, "replica_steps_per_s": steps / (total_ms / 1e3)}
+
+
 @dataclasses.dataclass
 class Job:
     jid: int
@@ -159,6 +185,7 @@ class Job:
     v: np.ndarray | None = None
     status: int = 0
     est_bytes: int = 0
+    left: int = 0  # batch steps still to take
 
 
 class Server:
@@ -167,7 +194,12 @@ class Server:
     ``run(jobs)`` plays the arrivals on the wall clock: between two batch
     steps it admits every arrived job whose estimated memory fits the budget
     (first come, first served), then steps the batch once; jobs whose steps
-    are done are read back and retired, freeing their memory for the queue."""
+    are done are read back and retired, freeing their memory for the queue.
+    When every admitted job has taken its steps and only their read-backs
+    are outstanding, the loop waits for those instead of stepping an empty
+    batch; the per-step latencies are those of steps with work."""
+
+    AHEAD = 3  # batch steps in flight at most
 
     def __init__(self, budget_bytes: int, form: str = "fused32"):
         self.budget = int(budget_bytes)
@@ -234,18 +266,29 @@ class Server:
                     if isinstance(s, Exception):
                         raise s
                     self.batch.add_job(s, j.nsteps)
+                    j.left = j.nsteps
                     j.admitted = time.perf_counter() - t0
                     active[s._h.value] = (j, s)
                 if not active:
                     time.sleep(0.0005)
                     continue
-                a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record(stream)
-                self.batch.run(1)
-                e.record(stream)
-                step_ev.append((a, e, len(active)))
+                stepping = [j for j, _ in active.values() if j.left > 0]
+                if stepping:
+                    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    self.batch.run(1)
+                    e.record(stream)
+                    step_ev.append((a, e, len(stepping)))
+                    for j in stepping:
+                        j.left -= 1
+                    # at most AHEAD steps in flight: the host does not queue
+                    # seconds of work ahead of the device, which kept the
+                    # creation of new jobs waiting behind the batch's streams
+                    if len(step_ev) > self.AHEAD:
+                        step_ev[-1 - self.AHEAD][1].synchronize()
                 # finished jobs: an event query, then a read-back on the job's own stream
-                for s in self.batch.poll():
+                retired = self.batch.poll()
+                for s in retired:
                     j, _ = active.pop(s._h.value)
                     j.x, j.v, _f = self.batch.retire(s)
                     j.status = s.status()
@@ -253,6 +296,8 @@ class Server:
                     s.final()
                     self.used -= j.est_bytes
                     finished.append(j)
+                if not stepping and not retired:
+                    time.sleep(0.0002)  # only read-backs outstanding
         finally:
             todo.put(None)
             th.join(timeout=30)
