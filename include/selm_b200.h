@@ -301,6 +301,41 @@ int selm_analysis_reset(selm_analysis* a);
 int selm_analysis_device_bytes(selm_analysis* a, unsigned long long* bytes);
 int selm_analysis_destroy(selm_analysis* a);
 
+/* ---- decomposed instance (z slabs over ranks) ----
+ * Replaces the reference's MPI slab decomposition of one instance: z slabs
+ * with FFTW-MPI transposed layouts (mpi/SELM_Eulerian_Period.cpp:18-51,
+ * 348-407) and the summed interpolation (mpi/SELM_Lagrangian_LAMMPS.cpp:102).
+ * selm_slab_create makes rank `rank`'s slab of an instance over `nranks`
+ * ranks (fused forms, inertial integrator, a grid of 16, 32, 48, 64, 96 or
+ * 128 cells per side with nz a multiple of 16 nranks): grid planes
+ * [rank nz/nranks, (rank+1) nz/nranks) and a block of the ny (nx/2+1)
+ * columns of the half spectrum (selm_slab_layout).  Every rank is given the
+ * same monomers and topology and keeps all of them; selm_set_particles,
+ * selm_set_topology, selm_initial, selm_get_particles work as for a whole
+ * instance.  A step is the four stages below, the same on every rank, with
+ * the caller's exchanges between them (buffers from selm_slab_buffers,
+ * device pointers, on the slab's stream, sizes in bytes):
+ *   selm_slab_gather   -> gather [3][M] (FP32/FP64) holds this slab's part of
+ *                         the interpolation; the caller replaces it by the
+ *                         sum over the ranks (an all-reduce);
+ *   selm_slab_advance  -> work [3][nzl][ny (nx/2+1)] complex: the xy spectrum
+ *                         of the slab's planes; the caller's all-to-all
+ *                         moves it to cols [3][nz][ncl] of every rank
+ *                         (rank r's columns c0..c0+ncl-1, planes in order);
+ *   selm_slab_solve    -> cols: the z pass, in place; the caller's
+ *                         all-to-all moves the columns back to work;
+ *   selm_slab_finish   -> the slab's velocity, the forces at x^{n+1}.
+ * selm_slab_velocity reads the slab's velocity [3][nzl][ny][nx].  A slab
+ * refuses selm_step and batches. */
+int selm_slab_create(const selm_params* params, int rank, int nranks, selm_sim** out);
+int selm_slab_layout(const selm_sim* s, int* z0, int* nzl, long long* c0, long long* ncl);
+int selm_slab_buffers(selm_sim* s, void** gather, void** work, void** cols, long long* sizes);
+int selm_slab_gather(selm_sim* s);
+int selm_slab_advance(selm_sim* s);
+int selm_slab_solve(selm_sim* s);
+int selm_slab_finish(selm_sim* s);
+int selm_slab_velocity(selm_sim* s, double* out);
+
 /* kernels this library has launched since it was loaded (all simulations) */
 unsigned long long selm_kernel_launches(void);
 

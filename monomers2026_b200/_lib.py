@@ -27,6 +27,8 @@ EXPORTED = [
     "selm_analysis_create", "selm_analysis_sample", "selm_analysis_msd", "selm_analysis_structure",
     "selm_analysis_kinetic", "selm_analysis_reset", "selm_analysis_device_bytes", "selm_analysis_destroy",
     "selm_get_coupling_impulse", "selm_host_register", "selm_host_unregister",
+    "selm_slab_create", "selm_slab_layout", "selm_slab_buffers", "selm_slab_gather", "selm_slab_advance",
+    "selm_slab_solve", "selm_slab_finish", "selm_slab_velocity",
 ]
 
 SELM_OK = 0
@@ -108,6 +110,13 @@ def load():
     L.selm_batch_add_job.argtypes = [vp, vp, C.c_longlong]
     L.selm_batch_poll.argtypes = [vp, C.POINTER(vp), C.c_int, C.POINTER(C.c_int)]
     L.selm_batch_retire.argtypes = [vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.selm_slab_create.argtypes = [C.POINTER(SelmParams), C.c_int, C.c_int, C.POINTER(vp)]
+    L.selm_slab_layout.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong),
+                                   C.POINTER(C.c_longlong)]
+    L.selm_slab_buffers.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(C.c_longlong)]
+    for name in ("selm_slab_gather", "selm_slab_advance", "selm_slab_solve", "selm_slab_finish"):
+        getattr(L, name).argtypes = [vp]
+    L.selm_slab_velocity.argtypes = [vp, C.POINTER(C.c_double)]
     L.selm_device_bytes.argtypes = [vp, C.POINTER(C.c_ulonglong)]
     L.selm_host_register.argtypes = [vp, C.c_ulonglong]
     L.selm_host_unregister.argtypes = [vp]

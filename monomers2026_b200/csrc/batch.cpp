@@ -169,6 +169,7 @@ static int batch_join(selm_batch* b, selm_sim* s, long long budget) {
   if (!b || !s) return selm_fail(SELM_ERR_INVALID, "NULL argument");
   if (s->batch) return selm_fail(SELM_ERR_STATE, "the simulation already belongs to a batch");
   if (!s->fz) return selm_fail(SELM_ERR_STATE, "only the fused forms step in a batch");
+  if (s->slab.nranks) return selm_fail(SELM_ERR_STATE, "a slab of a decomposed instance steps with its peers");
   if (!s->initialized) return selm_fail(SELM_ERR_STATE, "selm_initial has not been called");
   if (s->cb) return selm_fail(SELM_ERR_STATE, "a simulation with a host force callback steps alone");
   if (s->prof) return selm_fail(SELM_ERR_STATE, "profiling needs single steps");

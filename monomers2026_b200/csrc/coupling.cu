@@ -353,9 +353,12 @@ __device__ __forceinline__ void stencil_of(double gx, double gy, double gz, int 
 
 // Gamma_d u: the weighted sum over the 4^3 stencil of component d, in the
 // reference's loop and product order (cuda/SELM_Kernel.cu:375-422).
-template <typename T>
+// SLAB: ud holds only the planes [z0, z0 + nzl) of the grid (a decomposed
+// instance's slab); points on other planes are left out (the slabs' sums add
+// up to the whole gather)
+template <typename T, bool SLAB = false>
 __device__ __forceinline__ T stencil_gather(const T* __restrict__ ud, const int base[3], const T w[3][4],
-                                            const CouplingArgs& a) {
+                                            const CouplingArgs& a, int z0 = 0, int nzl = 0) {
   T val = T(0);
   // rows of 4 consecutive x-points: 16-byte vector loads over an aligned
   // window when the rows are 16-byte aligned (nx a multiple of the vector
@@ -381,7 +384,9 @@ __device__ __forceinline__ T stencil_gather(const T* __restrict__ ud, const int 
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       const T dk = T(1) * w[2][k];
-      const long zoff = (long)wrapi(base[2] + k, a.nz) * a.ny;
+      const int zk = wrapi(base[2] + k, a.nz);
+      if (SLAB && (unsigned)(zk - z0) >= (unsigned)nzl) continue;
+      const long zoff = (long)(SLAB ? zk - z0 : zk) * a.ny;
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         const T dj = dk * w[1][j];
@@ -404,7 +409,9 @@ __device__ __forceinline__ T stencil_gather(const T* __restrict__ ud, const int 
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       const T dk = T(1) * w[2][k];
-      const long zoff = (long)wrapi(base[2] + k, a.nz) * a.ny;
+      const int zk = wrapi(base[2] + k, a.nz);
+      if (SLAB && (unsigned)(zk - z0) >= (unsigned)nzl) continue;
+      const long zoff = (long)(SLAB ? zk - z0 : zk) * a.ny;
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         const T dj = dk * w[1][j];
@@ -545,6 +552,8 @@ __device__ __forceinline__ void tile_append(const TileSlots& ts, int p, double g
       else atomicOr(err, ERR_BUCKET_OVERFLOW);
     }
   };
+  // a slab of a decomposed instance files only under its own tile layers
+  auto zin = [&](int tz) { return ts.tz1 == 0 || (tz >= ts.tz0 && tz < ts.tz1); };
   if (nxs <= 2 && nys <= 2 && nzs <= 2) {
     // at most 2 x 2 x 2 tiles (tiles of at least 5 cells): all counters bumped
     // before any slot is written, so the atomics overlap
@@ -552,7 +561,7 @@ __device__ __forceinline__ void tile_append(const TileSlots& ts, int p, double g
 #pragma unroll
     for (int c = 0; c < 8; c++) {
       const int i = c & 1, j = (c >> 1) & 1, k = c >> 2;
-      const bool ok = i < nxs && j < nys && k < nzs;
+      const bool ok = i < nxs && j < nys && k < nzs && zin(k ? z1 : z0);
       tt[c] = ok ? ((k ? z1 : z0) * bs.nb[1] + (j ? y1 : y0)) * bs.nb[0] + (i ? x1 : x0) : -1;
       sl[c] = ok ? atomicAdd(&ts.count[tt[c]], 1) : 0;
     }
@@ -564,6 +573,7 @@ __device__ __forceinline__ void tile_append(const TileSlots& ts, int p, double g
 #pragma unroll 1
   for (int k = 0; k < nzs; k++) {
     const int tz = (k == 0) ? z0 : (k == 1) ? z1 : z2;
+    if (!zin(tz)) continue;
 #pragma unroll 1
     for (int j = 0; j < nys; j++) {
       const int ty = (j == 0) ? y0 : (j == 1) ? y1 : y2;
@@ -581,8 +591,10 @@ __device__ __forceinline__ void tile_append(const TileSlots& ts, int p, double g
 // (monomer, component); the spread part lives in k_spread_tiles.  The thread
 // of component d also stores, for the spread of the same step, the stencil
 // bases and weights of axis d (unshifted) and axis d+1 (shifted) in the
-// monomer's record, so the three threads together fill it.
-template <typename T>
+// monomer's record, so the three threads together fill it.  GATHERED: u is
+// the interpolated velocity itself, [3M] by monomer component (a decomposed
+// instance sums it over its slabs), and only the update and the filing run.
+template <typename T, bool GATHERED = false>
 // 256 threads, at least four blocks per SM in FP32 (64 registers): more warps in flight
 // for the latency-bound stencil gathers
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_interp_update(const T* __restrict__ u, const double* __restrict__ x_old,
@@ -602,7 +614,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) k_interp_update(c
   int base[3];
   T w[3][4];
   stencil_of<T>(gx, gy, gz, d, base, w);
-  const T val = stencil_gather<T>(u + d * N, base, w, a);
+  const T val = GATHERED ? u[g] : stencil_gather<T>(u + d * N, base, w, a);
   if (rec) {
     record_store<T>(rec[p], d, base, w, a);
     if (ts.home) home_slot_store(rec[p].hs, d, gx, gy, gz, ts.bs);
@@ -750,6 +762,55 @@ cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double
   count_launches(1);
   return cudaGetLastError();
 }
+
+// a decomposed instance's slab: the part of every monomer component's
+// interpolation that comes from the slab's planes [z0, z0 + nzl) (u: the
+// slab's velocity [3][nzl][ny][nx]), into out [3M]
+template <typename T>
+__global__ void __launch_bounds__(256) k_interp_partial(const T* __restrict__ u, const double* __restrict__ x, CouplingArgs a,
+                                                        int z0, int nzl, T* __restrict__ out) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 3L * a.M) return;
+  const int p = (int)(gid / 3), d = (int)(gid % 3);
+  const double gx = (x[3L * p] - a.lo) / a.dx, gy = (x[3L * p + 1] - a.lo) / a.dx, gz = (x[3L * p + 2] - a.lo) / a.dx;
+  int base[3];
+  T w[3][4];
+  stencil_of<T>(gx, gy, gz, d, base, w);
+  out[gid] = stencil_gather<T, true>(u + (long)d * nzl * a.ny * a.nx, base, w, a, z0, nzl);
+}
+
+template <typename T>
+cudaError_t interp_partial(const T* u_slab, const double* x, const CouplingArgs& a, int z0, int nzl, T* out,
+                           cudaStream_t st) {
+  if (a.M <= 0) return cudaSuccess;
+  const long nt = 3L * a.M;
+  k_interp_partial<T><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(u_slab, x, a, z0, nzl, out);
+  count_launches(1);
+  return cudaGetLastError();
+}
+template cudaError_t interp_partial<float>(const float*, const double*, const CouplingArgs&, int, int, float*,
+                                           cudaStream_t);
+template cudaError_t interp_partial<double>(const double*, const double*, const CouplingArgs&, int, int, double*,
+                                            cudaStream_t);
+
+// the update of a decomposed instance from the summed interpolation `gathered` [3M]
+template <typename T>
+cudaError_t interp_update_gathered(const T* gathered, const double* x_old, double* x_new, double* v, double* f,
+                                   const double* m, double* tf, WRec<T>* rec, const CouplingArgs& a, uint32_t* err,
+                                   cudaStream_t st, const TileSlots& ts) {
+  if (a.M <= 0) return cudaSuccess;
+  const long nt = 3L * a.M;
+  k_interp_update<T, true><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(gathered, x_old, x_new, v, f, m, tf, nullptr,
+                                                                         rec, a, err, ts);
+  count_launches(1);
+  return cudaGetLastError();
+}
+template cudaError_t interp_update_gathered<float>(const float*, const double*, double*, double*, double*,
+                                                   const double*, double*, WRec<float>*, const CouplingArgs&,
+                                                   uint32_t*, cudaStream_t, const TileSlots&);
+template cudaError_t interp_update_gathered<double>(const double*, const double*, double*, double*, double*,
+                                                    const double*, double*, WRec<double>*, const CouplingArgs&,
+                                                    uint32_t*, cudaStream_t, const TileSlots&);
 
 // ================================================================ spread (gather)
 // Tiles of kTX x kTY x kTZ cells.  bin_particles (mode 2) files every monomer
@@ -943,7 +1004,7 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
   const unsigned* acc_hi = acc_lo + kAccWords;
   const unsigned* acc_top = acc_lo + 2 * kAccWords;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const int tb = blockIdx.x;
+  const int tb = blockIdx.x + ts.tile0;
   const int tbx = tb % bs.nb[0], tby = (tb / bs.nb[0]) % bs.nb[1], tbz = tb / (bs.nb[0] * bs.nb[1]);
   SpreadTile tl;
   tl.t0x = tbx * kTX;
@@ -1027,7 +1088,8 @@ __global__ void __launch_bounds__(kSpreadThreads) k_spread_tiles(T* __restrict__
     const int row = idx / kTX, cx = idx % kTX;
     const int cy = row % kTY, cz = (row / kTY) % kTZ, d = row / (kTY * kTZ);
     if (cx < tl.ex && cy < tl.ey && cz < tl.ez) {
-      T* dst = fgrid + d * N + ((long)(tl.t0z + cz) * ny + (tl.t0y + cy)) * nx + tl.t0x + cx;
+      T* dst = fgrid + d * (ts.cstride ? ts.cstride : N) + ((long)(tl.t0z + cz - ts.z0) * ny + (tl.t0y + cy)) * nx +
+               tl.t0x + cx;
       const int slot = row * kTX + spread_rot(cx, cz, d);
       const long long sum =
           (tl.mode == kSplit3) ? (long long)(int)acc_top[slot] * (1ll << 42) + (long long)acc_hi[slot] * (1ll << 21) +
@@ -1550,7 +1612,7 @@ cudaError_t spread_slots(T* fgrid, bool accumulate, const double* x_old, const d
   const BinSpec& bs = ts.bs;
   const int ntiles = bs.nb[0] * bs.nb[1] * bs.nb[2];
   if (!accumulate && a.M == 0) {
-    return cudaMemsetAsync(fgrid, 0, sizeof(T) * 3L * a.nx * a.ny * a.nz, st);
+    return cudaMemsetAsync(fgrid, 0, sizeof(T) * 3L * (ts.cstride ? ts.cstride : (long)a.nx * a.ny * a.nz), st);
   }
   if (bs.mode != 2 || bs.tile[0] != kTX || bs.tile[1] != kTY || bs.tile[2] != kTZ || !ts.count)
     return cudaErrorInvalidValue;
@@ -1582,7 +1644,9 @@ cudaError_t spread_slots(T* fgrid, bool accumulate, const double* x_old, const d
     }
   }
   if (ts.home) return cudaErrorInvalidValue;
-  k_spread_tiles<T><<<ntiles, kSpreadThreads, spread_smem<T>(), st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, nullptr,
+  // a slab of a decomposed instance: its tile layers only
+  const int nlaunch = ts.tz1 ? (ts.tz1 - ts.tz0) * bs.nb[0] * bs.nb[1] : ntiles;
+  k_spread_tiles<T><<<nlaunch, kSpreadThreads, spread_smem<T>(), st>>>(fgrid, accumulate ? 1 : 0, x_old, tf, bs, nullptr,
                                                                   nullptr, ts, rec, a);
   count_launches(1);
   return cudaGetLastError();

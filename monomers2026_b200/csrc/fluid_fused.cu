@@ -520,6 +520,9 @@ static void fast_dispatch(int n, int split, int z_blocks_per_sm, const T* fp, cp
 
 using namespace selm;
 
+// grid sizes with compile-time four-step FFT kernels
+bool fused_fast_size(int n) { return fast_size(n); }
+
 struct FusedState {
   bool fp32 = false;
   void* u = nullptr;      // T [3][N]
@@ -597,16 +600,23 @@ template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
   const long N = s->N, N2 = s->N2;
   auto al = [&](void** p, size_t bytes) -> int { return sim_alloc(s, p, bytes); };
   int rc;
-  if ((rc = al(&z->u, sizeof(T) * 3 * N))) return rc;
-  if ((rc = al(&z->fp, sizeof(T) * 3 * N))) return rc;
-  if ((rc = al(&z->work, sizeof(C) * 3 * N2))) return rc;
-  if ((rc = al(&z->uhat, sizeof(C) * 3 * N2))) return rc;
+  // a decomposed instance holds its slab of planes (u, fp, work) and its
+  // block of columns (uhat, and the columns of the z pass)
+  const bool slab = s->slab.nranks > 0;
+  const long Nr = slab ? (long)s->slab.nzl * s->ny * s->nx : N;
+  const long N2r = slab ? (long)s->slab.nzl * s->ny * (s->nx / 2 + 1) : N2;
+  const long N2c = slab ? (long)s->nz * s->slab.ncl : N2;
+  if ((rc = al(&z->u, sizeof(T) * 3 * Nr))) return rc;
+  if ((rc = al(&z->fp, sizeof(T) * 3 * Nr))) return rc;
+  if ((rc = al(&z->work, sizeof(C) * 3 * N2r))) return rc;
+  if ((rc = al(&z->uhat, sizeof(C) * 3 * N2c))) return rc;
+  if (slab && (rc = al(&s->slab.cols, sizeof(C) * 3 * N2c))) return rc;
   if ((rc = al((void**)&z->symx, sizeof(double) * 2 * s->nx))) return rc;
   if ((rc = al((void**)&z->symy, sizeof(double) * 2 * s->ny))) return rc;
   if ((rc = al((void**)&z->symz, sizeof(double) * 2 * s->nz))) return rc;
   if ((rc = al((void**)&z->d_step, sizeof(uint64_t)))) return rc;
-  CUF(cudaMemsetAsync(z->u, 0, sizeof(T) * 3 * N, s->st));
-  CUF(cudaMemsetAsync(z->uhat, 0, sizeof(C) * 3 * N2, s->st));
+  CUF(cudaMemsetAsync(z->u, 0, sizeof(T) * 3 * Nr, s->st));
+  CUF(cudaMemsetAsync(z->uhat, 0, sizeof(C) * 3 * N2c, s->st));
   CUF(cudaMemsetAsync(z->d_step, 0, sizeof(uint64_t), s->st));
   const int nn[3] = {s->nx, s->ny, s->nz};
   double* tabs[3] = {z->symx, z->symy, z->symz};
@@ -684,6 +694,27 @@ static FusedGeom geom_of(selm_sim* s) {
   return g;
 }
 
+// the z kernel's geometry (all columns; a slab sets its block of columns)
+static ZGeom zgeom_of(selm_sim* s, const FusedGeom& g) {
+  ZGeom zg{};
+  zg.ny = s->ny;
+  zg.nx = s->nx;
+  zg.nxh = s->nx / 2 + 1;
+  zg.dx = g.dx;
+  zg.mu = g.mu;
+  zg.rho = g.rho;
+  zg.dt = g.dt;
+  zg.noise_amp = g.noise_amp;
+  zg.idx2 = 1.0 / (g.dx * g.dx);
+  zg.qs = (g.integrator == SELM_INTEGRATOR_QUASI_STEADY);
+  zg.stochastic = g.stochastic;
+  zg.noise_mode = g.noise_mode;
+  zg.seed = g.seed;
+  zg.step = g.step;
+  zg.rk = philox_keys(g.seed);
+  return zg;
+}
+
 template <typename T> static int fused_fluid_t(selm_sim* s) {
   using C = cpx<T>;
   FusedState* z = s->fz;
@@ -692,22 +723,7 @@ template <typename T> static int fused_fluid_t(selm_sim* s) {
   const FusedGeom g = geom_of(s);
   const unsigned planes = (unsigned)(3 * s->nz);
   if (z->fast) {
-    ZGeom zg{};
-    zg.ny = s->ny;
-    zg.nx = s->nx;
-    zg.nxh = s->nx / 2 + 1;
-    zg.dx = g.dx;
-    zg.mu = g.mu;
-    zg.rho = g.rho;
-    zg.dt = g.dt;
-    zg.noise_amp = g.noise_amp;
-    zg.idx2 = 1.0 / (g.dx * g.dx);
-    zg.qs = (g.integrator == SELM_INTEGRATOR_QUASI_STEADY);
-    zg.stochastic = g.stochastic;
-    zg.noise_mode = g.noise_mode;
-    zg.seed = g.seed;
-    zg.step = g.step;
-    zg.rk = philox_keys(g.seed);
+    const ZGeom zg = zgeom_of(s, g);
     fast_dispatch<T>(s->nx, z->tune_split, z->tune_z_blocks, (const T*)z->fp, (C*)z->work, (C*)z->uhat, (T*)z->u,
                      zg, tb, z->symx, z->symy, z->symz, s->ny, s->nz, s->st, s);
     CUF(cudaGetLastError());
@@ -737,9 +753,8 @@ template <typename T> static int fused_fluid_t(selm_sim* s) {
 
 // forces_done: set when the step also issued the conservative forces at the
 // new positions (on the side stream, beside the fluid solve, joined at the end)
-template <typename T> static int fused_step_t(selm_sim* s, bool* forces_done) {
-  *forces_done = false;
-  FusedState* z = s->fz;
+// the coupling kernels' arguments; *d_step is the step being taken
+static CouplingArgs coupling_args_of(selm_sim* s) {
   CouplingArgs a{};
   a.nx = s->nx;
   a.ny = s->ny;
@@ -753,8 +768,15 @@ template <typename T> static int fused_step_t(selm_sim* s, bool* forces_done) {
   a.stochastic = s->prm.flag_stochastic;
   a.seed = s->prm.seed;
   a.step = 0;
-  a.step_ptr = z->d_step;
+  a.step_ptr = s->fz->d_step;
   a.M = s->M;
+  return a;
+}
+
+template <typename T> static int fused_step_t(selm_sim* s, bool* forces_done) {
+  *forces_done = false;
+  FusedState* z = s->fz;
+  const CouplingArgs a = coupling_args_of(s);
   // *d_step is the step being taken; the inverse xy kernel advances it
   double* xo = s->x[s->cx];
   double* xn = s->x[s->cx ^ 1];
@@ -825,8 +847,11 @@ int fused_initial(selm_sim* s) {
   FusedState* z = s->fz;
   using std::size_t;
   const size_t es = z->fp32 ? sizeof(float) : sizeof(double);
-  CUF(cudaMemsetAsync(z->u, 0, es * 3 * s->N, s->st));
-  CUF(cudaMemsetAsync(z->uhat, 0, 2 * es * 3 * s->N2, s->st));
+  const bool slab = s->slab.nranks > 0;
+  const long Nr = slab ? (long)s->slab.nzl * s->ny * s->nx : s->N;
+  const long N2c = slab ? (long)s->nz * s->slab.ncl : s->N2;
+  CUF(cudaMemsetAsync(z->u, 0, es * 3 * Nr, s->st));
+  CUF(cudaMemsetAsync(z->uhat, 0, 2 * es * 3 * N2c, s->st));
   static const uint64_t kFirstStep = 1;
   CUF(cudaMemcpyAsync(z->d_step, &kFirstStep, sizeof(uint64_t), cudaMemcpyHostToDevice, s->st));
   return SELM_OK;
@@ -940,6 +965,7 @@ int fused_step(selm_sim* s) {
 }
 
 int fused_get_field(selm_sim* s, int which, double* out) {
+  if (s->slab.nranks) return selm_fail(SELM_ERR_STATE, "a slab holds part of the field: selm_slab_velocity");
   if (which != SELM_FIELD_U)
     return selm_fail(SELM_ERR_STATE, "the fused forms keep the forcing in the spectrum; only the velocity is readable");
   FusedState* z = s->fz;
@@ -957,6 +983,7 @@ int fused_get_field(selm_sim* s, int which, double* out) {
 }
 
 int fused_set_field(selm_sim* s, int which, const double* in) {
+  if (s->slab.nranks) return selm_fail(SELM_ERR_STATE, "a slab holds part of the field");
   if (which != SELM_FIELD_U)
     return selm_fail(SELM_ERR_STATE, "the fused forms keep the forcing in the spectrum; only the velocity is settable");
   FusedState* z = s->fz;
@@ -969,6 +996,171 @@ int fused_set_field(selm_sim* s, int which, const double* in) {
   } else {
     CUF(cudaMemcpyAsync(z->u, in, sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
     CUF(fft3_r2c<double>((const double*)z->u, (double2*)z->uhat, s->nx, s->ny, s->nz, 3, s->tb64, s->st));
+    CUF(cudaStreamSynchronize(s->st));
+  }
+  return SELM_OK;
+}
+
+// ---------------------------------------------------------------- decomposed instance (z slabs)
+// One instance spread over R ranks, a slab each: rank r holds the grid
+// planes [z0, z0 + nzl) (velocity, spread force, xy spectrum) and a block of
+// ncl columns of the flattened (y, x) half spectrum for the z pass (u_hat and
+// the z-pass columns); every monomer's state is replicated.  A step is four
+// stages with the caller's exchanges between them, the counterpart of the
+// reference's MPI path (slab layouts and transposed FFTs,
+// mpi/SELM_Eulerian_Period.cpp:18-51; the summed interpolation,
+// mpi/SELM_Lagrangian_LAMMPS.cpp:102):
+//   gather  - the slab's part of each monomer component's interpolation,
+//             into gather [3M];           caller: sum gather over the ranks
+//   advance - the monomer update from the summed interpolation (the same on
+//             every rank), the spread into the slab's tiles, the xy forward
+//             FFT of the slab's planes into work [3][nzl][ny*nxh];
+//                                         caller: all-to-all work -> cols
+//   solve   - the z pass (FFT, spectral update and noise, inverse FFT) on
+//             cols [3][nz][ncl] in place; caller: all-to-all cols -> work
+//   finish  - the xy inverse FFT of the slab's planes into u, the step
+//             count, the forces at the new positions.
+// Every stage is the whole-grid kernel on the slab's part: the spread of a
+// slab's tiles, the FFTs of its planes and the z pass of its columns give
+// the same values as in a single instance; only the interpolation is summed
+// in another order (slab by slab).
+enum SlabStage { kSlabXyForward = 0, kSlabZ = 1, kSlabXyInverse = 2 };
+
+template <typename T, int N, int N1>
+static void slab_launch(int stage, selm_sim* s, const ZGeom& zg, const FftTables<T>& tb) {
+  using C = cpx<T>;
+  using Z = ZShape<T, N>;
+  constexpr int RP = rows_per_chunk_fast<T, N>();
+  FusedState* z = s->fz;
+  const unsigned planes = (unsigned)(3 * s->slab.nzl);
+  if (stage == kSlabXyForward) {
+    k_xy_forward_fast<T, N, N1, RP><<<planes, 512, smem_xy_fast<T, N>(), s->st>>>((const T*)z->fp, (C*)z->work,
+                                                                                  tb.wx_f);
+  } else if (stage == kSlabZ) {
+    const unsigned nb = (unsigned)((s->slab.ncl + Z::WB - 1) / Z::WB);
+    k_z_update_fast<T, N, N1, Z::WB, Z::TPB, Z::MINB>
+        <<<nb, Z::TPB, smem_z_request(smem_z_need<T, N>(), z->tune_z_blocks), s->st>>>(
+            (C*)s->slab.cols, (C*)z->uhat, zg, tb.wz_f, z->symx, z->symy, z->symz);
+  } else {
+    k_xy_inverse_fast<T, N, N1, RP><<<planes, 512, smem_xy_fast<T, N>(), s->st>>>((const C*)z->work, (T*)z->u,
+                                                                                  tb.wx_f, (uint64_t*)zg.step);
+  }
+  count_launches(1);
+}
+
+template <typename T> static int slab_fluid(int stage, selm_sim* s) {
+  const FftTables<T>& tb = *reinterpret_cast<const FftTables<T>*>(s->fz->fp32 ? (const void*)&s->tb32
+                                                                                 : (const void*)&s->tb64);
+  ZGeom zg = zgeom_of(s, geom_of(s));
+  zg.c0 = s->slab.c0;
+  zg.ncol = s->slab.ncl;
+  switch (s->nx) {
+#define SELM_CASE(N)                                                        \
+  case N:                                                                   \
+    if (s->fz->tune_split == 1)                                             \
+      slab_launch<T, N, fftk::SplitBalanced<N>::N1>(stage, s, zg, tb);      \
+    else                                                                    \
+      slab_launch<T, N, fftk::Split<N>::N1>(stage, s, zg, tb);              \
+    break;
+    SELM_FAST_SIZES(SELM_CASE)
+#undef SELM_CASE
+    default:
+      return selm_fail(SELM_ERR_STATE, "a slab needs a grid size of the compile-time FFT kernels");
+  }
+  CUF(cudaGetLastError());
+  return SELM_OK;
+}
+
+static int slab_gather_buffer(selm_sim* s) {
+  if (s->M <= s->slab.gather_m) return SELM_OK;
+  const int rc = sim_alloc(s, &s->slab.gather, (s->fz->fp32 ? sizeof(float) : sizeof(double)) * 3 * (size_t)s->M);
+  if (rc == SELM_OK) s->slab.gather_m = s->M;
+  return rc;
+}
+
+template <typename T> static int slab_gather_t(selm_sim* s) {
+  if (s->M == 0) return SELM_OK;
+  const CouplingArgs a = coupling_args_of(s);
+  CUF(interp_partial<T>((const T*)s->fz->u, s->x[s->cx], a, s->slab.z0, s->slab.nzl, (T*)s->slab.gather, s->st));
+  return SELM_OK;
+}
+
+template <typename T> static int slab_advance_t(selm_sim* s) {
+  FusedState* z = s->fz;
+  const CouplingArgs a = coupling_args_of(s);
+  double* xo = s->x[s->cx];
+  double* xn = s->x[s->cx ^ 1];
+  if (s->M > 0) {
+    WRec<T>* rec = static_cast<WRec<T>*>(s->wrec);
+    CUF(interp_update_gathered<T>((const T*)s->slab.gather, xo, xn, s->v, s->f, s->m, s->tf, rec, a, s->err, s->st,
+                                  s->tslots));
+    CUF(spread_slots<T>((T*)z->fp, false, xo, s->tf, s->tslots, a, s->st, rec));
+  } else {
+    CUF(cudaMemsetAsync(z->fp, 0, sizeof(T) * 3 * (size_t)s->slab.nzl * s->ny * s->nx, s->st));
+  }
+  return slab_fluid<T>(kSlabXyForward, s);
+}
+
+static int slab_ready(selm_sim* s) {
+  if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  if (!s->slab.nranks) return selm_fail(SELM_ERR_STATE, "not a slab of a decomposed instance");
+  if (!s->initialized) return selm_fail(SELM_ERR_STATE, "selm_initial has not been called");
+  return slab_gather_buffer(s);
+}
+
+extern "C" int selm_slab_gather(selm_sim* s) {
+  int rc = slab_ready(s);
+  if (rc) return rc;
+  return s->fz->fp32 ? slab_gather_t<float>(s) : slab_gather_t<double>(s);
+}
+
+extern "C" int selm_slab_advance(selm_sim* s) {
+  int rc = slab_ready(s);
+  if (rc) return rc;
+  return s->fz->fp32 ? slab_advance_t<float>(s) : slab_advance_t<double>(s);
+}
+
+extern "C" int selm_slab_solve(selm_sim* s) {
+  int rc = slab_ready(s);
+  if (rc) return rc;
+  return s->fz->fp32 ? slab_fluid<float>(kSlabZ, s) : slab_fluid<double>(kSlabZ, s);
+}
+
+extern "C" int selm_slab_finish(selm_sim* s) {
+  int rc = slab_ready(s);
+  if (rc) return rc;
+  rc = s->fz->fp32 ? slab_fluid<float>(kSlabXyInverse, s) : slab_fluid<double>(kSlabXyInverse, s);
+  if (rc) return rc;
+  fused_step_taken(s);  // step count, positions x^{n+1}
+  return engine_forces(s);
+}
+
+extern "C" int selm_slab_buffers(selm_sim* s, void** gather, void** work, void** cols, long long* sizes) {
+  int rc = slab_ready(s);
+  if (rc) return rc;
+  const long long es = s->fz->fp32 ? 4 : 8;
+  if (gather) *gather = s->slab.gather;
+  if (work) *work = s->fz->work;
+  if (cols) *cols = s->slab.cols;
+  if (sizes) {
+    sizes[0] = 3LL * s->M * es;                                       // gather: T [3][M]
+    sizes[1] = 3LL * s->slab.nzl * s->ny * (s->nx / 2 + 1) * 2 * es;  // work: complex [3][nzl][ny*nxh]
+    sizes[2] = 3LL * s->nz * s->slab.ncl * 2 * es;                    // cols: complex [3][nz][ncl]
+  }
+  return SELM_OK;
+}
+
+extern "C" int selm_slab_velocity(selm_sim* s, double* out) {
+  int rc = slab_ready(s);
+  if (rc) return rc;
+  const long n = 3L * s->slab.nzl * s->ny * s->nx;
+  if (s->fz->fp32) {
+    std::vector<float> h(n);
+    CUF(cudaMemcpyAsync(h.data(), s->fz->u, sizeof(float) * n, cudaMemcpyDeviceToHost, s->st));
+    CUF(cudaStreamSynchronize(s->st));
+    for (long i = 0; i < n; i++) out[i] = h[i];
+  } else {
+    CUF(cudaMemcpyAsync(out, s->fz->u, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
     CUF(cudaStreamSynchronize(s->st));
   }
   return SELM_OK;

@@ -197,6 +197,10 @@ struct ZGeom {
   uint64_t seed;
   const uint64_t* step;
   PhiloxKeys rk;  // round keys of seed
+  // a decomposed instance's block of columns: work and uhat hold the columns
+  // c0 .. c0 + ncol - 1 of the flattened (y, x) half spectrum, ncol apart
+  // from one z plane to the next (ncol == 0: all ny * nxh columns)
+  long c0 = 0, ncol = 0;
 };
 
 // reference noise draw of a half-spectrum mode (cuda/SELM_Kernel.cu:56-79); the
@@ -261,12 +265,12 @@ __global__ void __launch_bounds__(TPB, MINB) k_z_update_fast(cpx<T>* __restrict_
   C* tw = A + N * NL;
   const int nxh = g.nxh, ny = g.ny;
   const long col0 = (long)blockIdx.x * WB;
-  const int wn = (int)min((long)WB, (long)nxh * ny - col0);
-  const long plane = (long)ny * nxh;
+  const long plane = g.ncol ? g.ncol : (long)ny * nxh;
+  const int wn = (int)min((long)WB, plane - col0);
   __shared__ int coli[WB], colj[WB];  // (i, j) of the block's columns
   for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twz[t];
   if (threadIdx.x < wn) {
-    const int col = (int)col0 + threadIdx.x;
+    const int col = (int)(g.c0 + col0) + threadIdx.x;
     colj[threadIdx.x] = col / nxh;
     coli[threadIdx.x] = col - colj[threadIdx.x] * nxh;
   }

@@ -260,6 +260,62 @@ extern "C" int selm_create(const selm_params* params, selm_sim** out) {
   return SELM_OK;
 }
 
+// One slab of an instance decomposed over nranks ranks (fused forms,
+// inertial integrator, a grid size of the compile-time FFT kernels): grid
+// planes [rank nz/nranks, (rank+1) nz/nranks), whole spread tiles of 16
+// planes each, and columns [rank C, (rank+1) C) of the ny (nx/2+1) columns of
+// the half spectrum, C = ceil(ny (nx/2+1) / nranks) (the last rank fewer).
+extern "C" int selm_slab_create(const selm_params* params, int rank, int nranks, selm_sim** out) {
+  if (!out) return selm_fail(SELM_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  int rc = validate(params);
+  if (rc) return rc;
+  if (nranks < 1 || rank < 0 || rank >= nranks) return selm_fail(SELM_ERR_INVALID, "rank must be in [0, nranks)");
+  if (params->form == SELM_FORM_PLAIN64 || params->integrator != SELM_INTEGRATOR_INERTIAL)
+    return selm_fail(SELM_ERR_INVALID, "a decomposed instance runs the fused forms with the inertial integrator");
+  const int n = params->num_mesh_pts[2];
+  if (!fused_fast_size(n) || n % (16 * nranks) != 0)
+    return selm_fail(SELM_ERR_INVALID, "a decomposed instance needs a compile-time FFT size that splits into "
+                                       "whole 16-plane tile layers per rank");
+  selm_sim* s = new selm_sim();
+  s->prm = *params;
+  s->nx = s->ny = s->nz = n;
+  s->N = (long)n * n * n;
+  s->N2 = (long)(n / 2 + 1) * n * n;
+  s->lo = params->box_lo;
+  s->hi = params->box_hi;
+  s->dx = (s->hi - s->lo) / s->nx;
+  const long ncol = (long)n * (n / 2 + 1), per = (ncol + nranks - 1) / nranks;
+  s->slab.rank = rank;
+  s->slab.nranks = nranks;
+  s->slab.nzl = n / nranks;
+  s->slab.z0 = rank * s->slab.nzl;
+  s->slab.c0 = std::min(ncol, rank * per);
+  s->slab.ncl = std::min(ncol, s->slab.c0 + per) - s->slab.c0;
+  if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete s;
+    return selm_fail(SELM_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  s->own_st = true;
+  rc = engine_allocate_grid(s);
+  if (rc) {
+    selm_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return SELM_OK;
+}
+
+extern "C" int selm_slab_layout(const selm_sim* s, int* z0, int* nzl, long long* c0, long long* ncl) {
+  if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
+  if (!s->slab.nranks) return selm_fail(SELM_ERR_STATE, "not a slab of a decomposed instance");
+  if (z0) *z0 = s->slab.z0;
+  if (nzl) *nzl = s->slab.nzl;
+  if (c0) *c0 = s->slab.c0;
+  if (ncl) *ncl = s->slab.ncl;
+  return SELM_OK;
+}
+
 int engine_allocate_grid(selm_sim* s) {
   int rc;
   const long N = s->N, N2 = s->N2;
@@ -318,7 +374,7 @@ static int alloc_bins(selm_sim* s, const BinSpec& bs, BinBuffers& bb, int M) {
 constexpr int kHomeMinMonomers = 16384;
 static int alloc_slots(selm_sim* s, const BinSpec& bs, TileSlots& ts, int M) {
   const long ntiles = (long)bs.nb[0] * bs.nb[1] * bs.nb[2];
-  const bool home = (s->prm.form == SELM_FORM_FUSED32) && M >= kHomeMinMonomers;
+  const bool home = (s->prm.form == SELM_FORM_FUSED32) && M >= kHomeMinMonomers && s->slab.nranks == 0;
   double per = 1.0;  // expected tiles a monomer is filed under (a union stencil is 5 cells per axis)
   if (!home)
     for (int a = 0; a < 3; a++) per *= (bs.nb[a] == 1) ? 1.0 : 1.0 + 4.0 / bs.tile[a];
@@ -330,6 +386,14 @@ static int alloc_slots(selm_sim* s, const BinSpec& bs, TileSlots& ts, int M) {
   ts.cap = (int)cap;
   ts.ovf_cap = (int)std::min<long>(2147483647L, (long)M * (home ? 1 : spread_entries_per_monomer(bs)) + 1024);
   ts.home = home ? 1 : 0;
+  if (s->slab.nranks) {
+    // a decomposed instance's slab: its tile layers only, written into the slab's planes
+    ts.tz0 = s->slab.z0 / bs.tile[2];
+    ts.tz1 = (s->slab.z0 + s->slab.nzl) / bs.tile[2];
+    ts.tile0 = ts.tz0 * bs.nb[0] * bs.nb[1];
+    ts.z0 = s->slab.z0;
+    ts.cstride = (long)s->slab.nzl * s->ny * s->nx;
+  }
   int rc;
   if (home) {
     const long box = 3L * (bs.tile[0] + 4) * (bs.tile[1] + 4) * (bs.tile[2] + 4);
@@ -835,6 +899,7 @@ extern "C" int selm_step(selm_sim* s, int nsteps) {
   if (!s) return selm_fail(SELM_ERR_INVALID, "sim is NULL");
   if (!s->initialized) return selm_fail(SELM_ERR_STATE, "selm_initial has not been called");
   if (s->batch) return selm_fail(SELM_ERR_STATE, "the simulation belongs to a batch: step it with selm_batch_step");
+  if (s->slab.nranks) return selm_fail(SELM_ERR_STATE, "a slab steps with its peers through the selm_slab_* stages");
   if (nsteps < 0) return selm_fail(SELM_ERR_INVALID, "nsteps < 0");
   if (nsteps > 0) s->ready_early = false;  // a graph step sets it again
   for (int i = 0; i < nsteps; i++) {

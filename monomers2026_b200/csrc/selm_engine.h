@@ -65,6 +65,16 @@ struct selm_sim {
   selm::BinBuffers fbb{};
   selm::TileSlots tslots{};  // spread-tile candidates, filed during the interpolation
   selm::NeighborList nlist{};  // Verlet list of the pair style
+  // z-slab of a decomposed instance (selm_slab_create): grid planes
+  // [z0, z0 + nzl) and columns [c0, c0 + ncl) of the flattened (y, x) half
+  // spectrum; nranks == 0 for a simulation of the whole grid
+  struct Slab {
+    int rank = 0, nranks = 0, z0 = 0, nzl = 0;
+    long c0 = 0, ncl = 0;
+    void* gather = nullptr;  // T [3][M]: this slab's part of the interpolation, then (after the caller's sum) all of it
+    int gather_m = 0;        // the monomers it has room for
+    void* cols = nullptr;    // C [3][nz][ncl]: the columns of the z pass
+  } slab;
   bool have_topo = false;
   selm::ForceTopo topo{};
   selm_force_fn cb = nullptr;
@@ -110,6 +120,7 @@ void fused_release(selm_sim* s);
 int fused_step_graph(selm_sim* s, int par, cudaGraph_t* graph, unsigned long long* kernels);
 // host bookkeeping of one step taken by a graph launched elsewhere
 void fused_step_taken(selm_sim* s);
+bool fused_fast_size(int n);
 
 // batches (batch.cpp)
 void batch_mark_dirty(selm_batch* b, selm_sim* s);  // member s has new graphs

@@ -95,6 +95,12 @@ struct TileSlots {
   int* live = nullptr;        // [ntiles]
   unsigned long long* tmax = nullptr;  // [ntiles]
   int* quirk = nullptr;                // [ntiles]
+  // z-slab of a decomposed instance: monomers are filed only under tiles of
+  // the layers [tz0, tz1) (tz1 == 0: all), the spread's block b takes tile
+  // tile0 + b, and the grid it writes holds planes z0.. with components
+  // cstride apart (0: the whole grid's N)
+  int tz0 = 0, tz1 = 0, tile0 = 0, z0 = 0;
+  long cstride = 0;
 };
 template <typename T> struct alignas(16) WRec {
   T w[3][2][4];  // weight factors [axis][unshifted, shifted][point] (16-byte aligned rows)
@@ -123,6 +129,15 @@ template <typename T>
 cudaError_t interp_update(const T* u, const double* x_old, double* x_new, double* v, double* f, const double* m,
                           double* tf, const int* order, WRec<T>* rec, const CouplingArgs& a, uint32_t* err,
                           cudaStream_t st, const TileSlots* ts = nullptr);
+// decomposed instance: the slab's part of the interpolation, and the update
+// from the interpolation summed over the slabs
+template <typename T>
+cudaError_t interp_partial(const T* u_slab, const double* x, const CouplingArgs& a, int z0, int nzl, T* out,
+                           cudaStream_t st);
+template <typename T>
+cudaError_t interp_update_gathered(const T* gathered, const double* x_old, double* x_new, double* v, double* f,
+                                   const double* m, double* tf, WRec<T>* rec, const CouplingArgs& a, uint32_t* err,
+                                   cudaStream_t st, const TileSlots& ts);
 template <typename T>
 cudaError_t interp_only(const T* u, const double* x, int M, int nx, int ny, int nz, double lo, double dx, double* out,
                         cudaStream_t st);

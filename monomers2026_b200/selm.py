@@ -90,12 +90,17 @@ class Selm:
     """One simulation: Eulerian_Period fluid + monomers, resident on the GPU."""
 
     def __init__(self, params: Params, x: np.ndarray, mass: np.ndarray, v: np.ndarray | None = None,
-                 topology: Topology | None = None):
+                 topology: Topology | None = None, slab: tuple[int, int] | None = None):
+        """``slab=(rank, nranks)``: rank's slab of an instance decomposed over
+        nranks ranks (``monomers2026_b200.decomposed``)."""
         L = _lib.load()
         self._L = L
         self.params = params
         h = C.c_void_p()
-        check(L.selm_create(C.byref(params.to_c()), C.byref(h)))
+        if slab is None:
+            check(L.selm_create(C.byref(params.to_c()), C.byref(h)))
+        else:
+            check(L.selm_slab_create(C.byref(params.to_c()), int(slab[0]), int(slab[1]), C.byref(h)))
         self._h = h
         self.M = int(len(mass))
         self._x = np.ascontiguousarray(x, np.float64).reshape(self.M, 3)
