@@ -57,6 +57,7 @@ extern "C" {
 #define SELM_STATUS_FENE_STRETCH 0x4u
 #define SELM_STATUS_FENE_BROKEN 0x8u
 #define SELM_STATUS_NLIST_OVERFLOW 0x20u /* a monomer had more pair partners in reach than its neighbour list holds */
+#define SELM_STATUS_COPY_TIMEOUT 0x40u /* an asynchronous copy into shared memory did not complete within its bound; the step's fluid result is invalid */
 
 /* Model.SELM keys (cuda/SELM.cu:17-48) plus the box and dt that the
  * reference takes from LAMMPS (domain->boxlo/hi, update->dt). */

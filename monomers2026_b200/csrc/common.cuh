@@ -24,6 +24,7 @@ enum : uint32_t {
   ERR_FENE_BROKEN = 1u << 3,      // FENE bond past the LAMMPS error limit
   ERR_BUCKET_OVERFLOW = 1u << 4,  // candidate list longer than the kernel bound
   ERR_NLIST_OVERFLOW = 1u << 5,   // more pair partners within the list radius than the list holds
+  ERR_COPY_TIMEOUT = 1u << 6,     // an asynchronous (TMA) copy did not complete within its wait bound
 };
 
 template <typename T> struct cpx_t;

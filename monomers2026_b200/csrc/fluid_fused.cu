@@ -31,6 +31,8 @@
 #include <mutex>
 #include <map>
 
+#include <cudaTypedefs.h>
+
 #include "common.cuh"
 #include "fluid_fused_fast.cuh"
 #include "selm_engine.h"
@@ -389,13 +391,15 @@ template <typename T, int N> constexpr size_t smem_xy_fast() { return smem_xy_fo
 
 // Shape of a z-kernel block: WB columns, TPB threads, at least MINB blocks
 // per SM (register bound), and the default cap on blocks per SM (0: none).
-// The 128^3 FP32 kernel takes 19 columns in blocks held to 80 registers:
-// its 438 blocks then all fit at once, three per SM, where 16 columns left a
-// second wave of 76 blocks (measured 64 us against 78; without the register
-// bound the 19-column block takes 96 registers, two per SM, and 81 us).
+// The 128^3 FP32 kernel takes 20 columns in blocks held to three per SM's
+// registers: its 416 blocks then all fit at once, where 16 columns left a
+// second wave of 76 blocks (measured 64 us against 78 with 19 columns; 20
+// makes the block's columns a whole number of 16-byte units, which its
+// tensor copies need: kTma).
 template <typename T, int N> struct ZShape {
   static constexpr bool kWide = sizeof(T) == 4 && N == 128;
-  static constexpr int WB = sizeof(T) == 8 ? 8 : (kWide ? 19 : 16);
+  static constexpr bool kTma = kWide;
+  static constexpr int WB = sizeof(T) == 8 ? 8 : (kWide ? 20 : 16);
   static constexpr int TPB = 256;
   static constexpr int MINB = kWide ? 3 : (sizeof(T) == 8 ? 2 : 1);
   static constexpr int CAP = 3;
@@ -406,7 +410,8 @@ template <typename T, int N> constexpr int wb_fast() { return ZShape<T, N>::WB; 
 // default at most three blocks share an SM: with the 128^3 FP32 kernel, four
 // resident blocks per SM measured slower than three.
 template <typename T, int N> constexpr size_t smem_z_need() {
-  return sizeof(cpx<T>) * ((size_t)N * 3 * wb_fast<T, N>() + N);
+  // the TMA form places its columns at a 128-byte boundary: up to 128 bytes more
+  return sizeof(cpx<T>) * ((size_t)N * 3 * wb_fast<T, N>() + N) + (ZShape<T, N>::kTma ? 128 : 0);
 }
 constexpr int kZDefaultBlocksPerSm = 3;
 // the default cap of a size (ZShape<T, N>::CAP)
@@ -439,6 +444,11 @@ template <typename T, int N, int N1> static cudaError_t fast_attrs_split() {
     return e;
   const size_t zmax = smem_z_need<T, N>() > kZSmemMax ? smem_z_need<T, N>() : kZSmemMax;
   using Z = ZShape<T, N>;
+  if constexpr (Z::kTma) {
+    if ((e = cudaFuncSetAttribute((const void*)k_z_update_fast<T, N, N1, Z::WB, Z::TPB, Z::MINB, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zmax)))
+      return e;
+  }
   return cudaFuncSetAttribute((const void*)k_z_update_fast<T, N, N1, Z::WB, Z::TPB, Z::MINB>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zmax);
 }
@@ -451,7 +461,7 @@ template <typename T, int N> static cudaError_t fast_attrs() {
 template <typename T, int N, int N1>
 static void fast_launch(const T* fp, cpx<T>* work, cpx<T>* uhat, T* u, const ZGeom& zg, const FftTables<T>& tb,
                         const double* symx, const double* symy, const double* symz, int ny, int nz, cudaStream_t st,
-                        selm_sim* s, int z_blocks_per_sm) {
+                        selm_sim* s, int z_blocks_per_sm, const CUtensorMap* zmap) {
   constexpr int RP = rows_per_chunk_fast<T, N>();
   using Z = ZShape<T, N>;
   const unsigned planes = (unsigned)(3 * nz);
@@ -460,9 +470,19 @@ static void fast_launch(const T* fp, cpx<T>* work, cpx<T>* uhat, T* u, const ZGe
   count_launches(1);
   prof_mark(s, "xy_forward", false);
   prof_mark(s, "z_update", true);
-  k_z_update_fast<T, N, N1, Z::WB, Z::TPB, Z::MINB><<<(unsigned)z_blocks<Z::WB>(zg.nxh, ny), Z::TPB,
-                                  smem_z_request(smem_z_need<T, N>(), z_blocks_per_sm), st>>>(
-      work, uhat, zg, tb.wz_f, symx, symy, symz);
+  const unsigned zb = (unsigned)z_blocks<Z::WB>(zg.nxh, ny);
+  const size_t zs = smem_z_request(smem_z_need<T, N>(), z_blocks_per_sm);
+  bool tma = false;
+  if constexpr (Z::kTma) {
+    if (zmap) {  // the block's columns by tensor copies (the map covers work)
+      k_z_update_fast<T, N, N1, Z::WB, Z::TPB, Z::MINB, true><<<zb, Z::TPB, zs, st>>>(work, uhat, zg, tb.wz_f, symx,
+                                                                                       symy, symz, *zmap);
+      tma = true;
+    }
+  }
+  if (!tma)
+    k_z_update_fast<T, N, N1, Z::WB, Z::TPB, Z::MINB><<<zb, Z::TPB, zs, st>>>(work, uhat, zg, tb.wz_f, symx, symy,
+                                                                              symz, CUtensorMap{});
   count_launches(1);
   prof_mark(s, "z_update", false);
   prof_mark(s, "xy_inverse", true);
@@ -498,16 +518,17 @@ template <typename T> static cudaError_t fast_attrs_for(int n) {
 template <typename T>
 static void fast_dispatch(int n, int split, int z_blocks_per_sm, const T* fp, cpx<T>* work, cpx<T>* uhat, T* u,
                           const ZGeom& zg, const FftTables<T>& tb, const double* symx, const double* symy,
-                          const double* symz, int ny, int nz, cudaStream_t st, selm_sim* s) {
+                          const double* symz, int ny, int nz, cudaStream_t st, selm_sim* s,
+                          const CUtensorMap* zmap) {
   switch (n) {
 #define SELM_CASE(N)                                                                                            \
   case N:                                                                                                       \
     if (split == 1)                                                                                             \
       fast_launch<T, N, fftk::SplitBalanced<N>::N1>(fp, work, uhat, u, zg, tb, symx, symy, symz, ny, nz, st, s, \
-                                                    z_blocks_per_sm);                                          \
+                                                    z_blocks_per_sm, zmap);                                          \
     else                                                                                                        \
       fast_launch<T, N, fftk::Split<N>::N1>(fp, work, uhat, u, zg, tb, symx, symy, symz, ny, nz, st, s,         \
-                                            z_blocks_per_sm);                                                  \
+                                            z_blocks_per_sm, zmap);                                                  \
     break;
     SELM_FAST_SIZES(SELM_CASE)
 #undef SELM_CASE
@@ -525,6 +546,9 @@ bool fused_fast_size(int n) { return fast_size(n); }
 
 struct FusedState {
   bool fp32 = false;
+  // tensor map of work for the z kernel's TMA staging (FP32 128^3 whole grids)
+  CUtensorMap zmap{};
+  bool zmap_ok = false;
   void* u = nullptr;      // T [3][N]
   void* fp = nullptr;     // T [3][N] spread impulse
   void* work = nullptr;   // C [3][nz][ny][nxh]
@@ -595,6 +619,34 @@ extern "C" int selm_tune_get(selm_sim* s, int knob, int* value) {
   return SELM_OK;
 }
 
+// The z kernel's tensor map over work [component][plane][column] of 8-byte
+// complex values, as dims (column, component, plane) and a box of the
+// kernel's WB columns x 3 x n; cuTensorMapEncodeTiled comes through the
+// runtime's driver entry point.  The host checks what TMA needs (16-byte
+// base, strides and box rows; the kernel's column origin is a multiple of WB,
+// WB * 8 bytes a multiple of 16); false: the kernel loads and stores itself.
+static bool encode_zmap(CUtensorMap* map, void* work, long ncol, int n, int wb) {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  if (!fn) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)ncol, 3, (cuuint64_t)n};
+  const cuuint64_t strides[2] = {(cuuint64_t)n * ncol * 8, (cuuint64_t)ncol * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)wb, 3, (cuuint32_t)n};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  if (((uintptr_t)work & 15) || (strides[0] & 15) || (strides[1] & 15) || ((size_t)wb * 8) % 16 || n > 256)
+    return false;
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, work, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
 template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
   using C = cpx<T>;
   const long N = s->N, N2 = s->N2;
@@ -633,6 +685,8 @@ template <typename T> static int fused_alloc_t(selm_sim* s, FusedState* z) {
   z->plan = plan_for<T>(s->nx, s->ny, s->nz);
   z->fast = fast_size(s->nx) && s->nx == s->ny && s->nx == s->nz;
   if (z->fast) CUF(fast_attrs_for<T>(s->nx));
+  if (z->fast && sizeof(T) == 4 && s->nx == 128 && !slab)
+    z->zmap_ok = encode_zmap(&z->zmap, z->work, (long)s->ny * (s->nx / 2 + 1), s->nz, ZShape<float, 128>::WB);
   const int prec = (int)(8 * sizeof(T));
   z->tune_split = tune_default_of(s->nx, prec, SELM_TUNE_FFT_SPLIT, 0);
   z->tune_z_blocks = tune_default_of(s->nx, prec, SELM_TUNE_Z_BLOCKS, z_default_blocks(s->nx, prec));
@@ -712,6 +766,7 @@ static ZGeom zgeom_of(selm_sim* s, const FusedGeom& g) {
   zg.seed = g.seed;
   zg.step = g.step;
   zg.rk = philox_keys(g.seed);
+  zg.err = s->err;
   return zg;
 }
 
@@ -725,7 +780,7 @@ template <typename T> static int fused_fluid_t(selm_sim* s) {
   if (z->fast) {
     const ZGeom zg = zgeom_of(s, g);
     fast_dispatch<T>(s->nx, z->tune_split, z->tune_z_blocks, (const T*)z->fp, (C*)z->work, (C*)z->uhat, (T*)z->u,
-                     zg, tb, z->symx, z->symy, z->symz, s->ny, s->nz, s->st, s);
+                     zg, tb, z->symx, z->symy, z->symz, s->ny, s->nz, s->st, s, z->zmap_ok ? &z->zmap : nullptr);
     CUF(cudaGetLastError());
     return SELM_OK;
   }
@@ -1040,7 +1095,7 @@ static void slab_launch(int stage, selm_sim* s, const ZGeom& zg, const FftTables
     const unsigned nb = (unsigned)((s->slab.ncl + Z::WB - 1) / Z::WB);
     k_z_update_fast<T, N, N1, Z::WB, Z::TPB, Z::MINB>
         <<<nb, Z::TPB, smem_z_request(smem_z_need<T, N>(), z->tune_z_blocks), s->st>>>(
-            (C*)s->slab.cols, (C*)z->uhat, zg, tb.wz_f, z->symx, z->symy, z->symz);
+            (C*)s->slab.cols, (C*)z->uhat, zg, tb.wz_f, z->symx, z->symy, z->symz, CUtensorMap{});
   } else {
     k_xy_inverse_fast<T, N, N1, RP><<<planes, 512, smem_xy_fast<T, N>(), s->st>>>((const C*)z->work, (T*)z->u,
                                                                                   tb.wx_f, (uint64_t*)zg.step);

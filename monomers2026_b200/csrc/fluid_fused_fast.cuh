@@ -12,6 +12,8 @@
 // Shared-memory lines are stored line-fastest (element t of line l at
 // t*stride + l), so threads of consecutive lines touch consecutive words.
 #pragma once
+#include <cuda.h>
+
 #include "common.cuh"
 #include "fft_fast.cuh"
 
@@ -201,6 +203,7 @@ struct ZGeom {
   // c0 .. c0 + ncol - 1 of the flattened (y, x) half spectrum, ncol apart
   // from one z plane to the next (ncol == 0: all ny * nxh columns)
   long c0 = 0, ncol = 0;
+  uint32_t* err = nullptr;  // status word (a TMA copy that timed out)
 };
 
 // reference noise draw of a half-spectrum mode (cuda/SELM_Kernel.cu:56-79); the
@@ -243,6 +246,48 @@ __device__ __forceinline__ void noise_draw_fast(const ZGeom& g, uint64_t step, i
   }
 }
 
+// ---- TMA staging of the z kernel's columns (single-CTA tensor copies, no
+// multicast): one thread loads a block's WB columns x 3 components x N
+// planes into shared memory on an mbarrier, and stores them back after the
+// inverse pass.  Every wait is bounded: a copy that does not complete sets
+// the status bit ERR_COPY_TIMEOUT and the block returns.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void zbar_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void zbar_load(void* dst, const CUtensorMap* map, unsigned long long* bar, unsigned bytes,
+                                          int x, int y, int z) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+// true once phase 0 of the barrier has completed, false after `limit` polls
+__device__ __forceinline__ bool zbar_wait(unsigned long long* bar, long limit) {
+  for (long i = 0; i < limit; i++) {
+    unsigned done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_u32(bar))
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void zbar_store(const CUtensorMap* map, const void* src, int x, int y, int z) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(map),
+               "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");  // shared memory read out: the block may end
+}
+constexpr long kZbarPolls = 1L << 22;
+
 // Column blocks of the z kernel: block b takes the WB consecutive columns
 // b*WB .. b*WB+WB-1 of the flattened (y, x) half-spectrum plane (column
 // index j*nxh + i, also its offset within a z plane), the last block fewer.
@@ -250,24 +295,38 @@ template <int WB> __host__ __device__ __forceinline__ int z_blocks(int nxh, int 
   return (nxh * ny + WB - 1) / WB;
 }
 
-template <typename T, int N, int N1_, int WB, int TPB, int MINB>
+// TMA: the block's columns of work come into shared memory and go back by
+// tensor copies (tmap: work as [plane][component][column], 3-D, box WB x 3
+// x N), instead of the passes' own global loads and stores.
+template <typename T, int N, int N1_, int WB, int TPB, int MINB, bool TMA = false>
 __global__ void __launch_bounds__(TPB, MINB) k_z_update_fast(cpx<T>* __restrict__ work, cpx<T>* __restrict__ uhat, ZGeom g,
                                                        const cpx<T>* __restrict__ twz,
                                                        const double* __restrict__ symx,
                                                        const double* __restrict__ symy,
-                                                       const double* __restrict__ symz) {
+                                                       const double* __restrict__ symz,
+                                                       const __grid_constant__ CUtensorMap tmap) {
   using C = cpx<T>;
   constexpr int N1 = N1_, N2 = N / N1_;
   static_assert(N1 * N2 == N && N1 <= 16 && N2 <= 16, "four-step split");
   constexpr int NL = 3 * WB;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* A = reinterpret_cast<C*>(smem_raw);  // element t of line (c, w) at t*NL + c*WB + w
+  extern __shared__ __align__(128) unsigned char zsmem_raw[];
+  // element t of line (c, w) at t*NL + c*WB + w; with TMA at a 128-byte
+  // boundary, the tensor copies' rule (the launch adds 128 bytes for it)
+  C* A = reinterpret_cast<C*>(TMA ? ((reinterpret_cast<uintptr_t>(zsmem_raw) + 127) & ~(uintptr_t)127)
+                                  : reinterpret_cast<uintptr_t>(zsmem_raw));
   C* tw = A + N * NL;
   const int nxh = g.nxh, ny = g.ny;
   const long col0 = (long)blockIdx.x * WB;
   const long plane = g.ncol ? g.ncol : (long)ny * nxh;
   const int wn = (int)min((long)WB, plane - col0);
   __shared__ int coli[WB], colj[WB];  // (i, j) of the block's columns
+  __shared__ __align__(8) unsigned long long zbar;
+  if constexpr (TMA) {
+    if (threadIdx.x == 0) {
+      zbar_init(&zbar);
+      zbar_load(A, &tmap, &zbar, (unsigned)(sizeof(C) * N * NL), (int)col0, 0, 0);
+    }
+  }
   for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = twz[t];
   if (threadIdx.x < wn) {
     const int col = (int)(g.c0 + col0) + threadIdx.x;
@@ -275,7 +334,17 @@ __global__ void __launch_bounds__(TPB, MINB) k_z_update_fast(cpx<T>* __restrict_
     coli[threadIdx.x] = col - colj[threadIdx.x] * nxh;
   }
   __syncthreads();
-  // pass A forward, loading straight from global: thread (line, n2)
+  if constexpr (TMA) {
+    // one thread polls (bounded) and tells the block, so that all of it goes on or stops
+    __shared__ int zok;
+    if (threadIdx.x == 0) {
+      zok = zbar_wait(&zbar, kZbarPolls);
+      if (!zok && g.err) atomicOr(g.err, (uint32_t)ERR_COPY_TIMEOUT);
+    }
+    __syncthreads();
+    if (!zok) return;  // the copy may still be in flight: its memory is left alone
+  }
+  // pass A forward, loading straight from global (or from the staged columns): thread (line, n2)
   for (int u = threadIdx.x; u < NL * N2; u += blockDim.x) {
     const int l = u % NL, n2 = u / NL;
     const int c = l / WB, w = l % WB;
@@ -283,7 +352,10 @@ __global__ void __launch_bounds__(TPB, MINB) k_z_update_fast(cpx<T>* __restrict_
     const long cb = (long)c * N * plane + col0 + w;
     C v[N1];
 #pragma unroll
-    for (int n1 = 0; n1 < N1; n1++) v[n1] = ok ? work[cb + (N2 * n1 + n2) * plane] : fftk::mk<C>(T(0), T(0));
+    for (int n1 = 0; n1 < N1; n1++) {
+      if constexpr (TMA) v[n1] = A[(N2 * n1 + n2) * NL + l];  // columns past the end arrive as zeros
+      else v[n1] = ok ? work[cb + (N2 * n1 + n2) * plane] : fftk::mk<C>(T(0), T(0));
+    }
     fftk::dft<N1, -1>(v);
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) A[(N2 * k1 + n2) * NL + l] = (k1 == 0) ? v[0] : cmul(v[k1], tw[n2 * k1]);
@@ -419,11 +491,19 @@ __global__ void __launch_bounds__(TPB, MINB) k_z_update_fast(cpx<T>* __restrict_
 #pragma unroll
     for (int k1 = 0; k1 < N1; k1++) v[k1] = A[(N2 * k1 + n2) * NL + l];
     fftk::dft<N1, +1>(v);
-    if (w < wn) {
+    if constexpr (TMA) {
+#pragma unroll
+      for (int n1 = 0; n1 < N1; n1++) A[(N2 * n1 + n2) * NL + l] = v[n1];  // the thread's own positions
+    } else if (w < wn) {
       const long cb = (long)c * N * plane + col0 + w;
 #pragma unroll
       for (int n1 = 0; n1 < N1; n1++) work[cb + (N2 * n1 + n2) * plane] = v[n1];
     }
+  }
+  if constexpr (TMA) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // this thread's writes, seen by the copy
+    __syncthreads();
+    if (threadIdx.x == 0) zbar_store(&tmap, A, (int)col0, 0, 0);  // columns past the end are not written
   }
 }
 
