@@ -353,6 +353,11 @@ def run_ours(args, rank, world, local_rank):
     batched = serving = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched, serving = batched_and_serving(args)
+    decomposed = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        log("decomposed instance (2 slabs, loopback)")
+        decomposed = decomposed_check(wl)
+        log(f"decomposed: {decomposed}")
 
     # ---- CPU baseline (rank 0 at N=1): the reference's CPU code on every host thread, a bounded sample
     cpu = None
@@ -401,6 +406,7 @@ def run_ours(args, rank, world, local_rank):
             "autotune": tuned,
             "batched": batched,
             "serving": serving,
+            "decomposed": decomposed,
             "gpu_launches": int(launches),
             "clocks": clocks,
             "status_word": status,
@@ -466,6 +472,45 @@ def batched_and_serving(args):
         f"step p50 {sv['step_ms']['p50']:.2f} p99 {sv['step_ms']['p99']:.2f} ms, "
         f"sequential plain64 {seq['replica_steps_per_s']:.0f} replica-steps/s")
     return b, sv
+
+
+def decomposed_check(wl, nranks=2, steps=5):
+    """The headline workload as one instance over `nranks` z slabs, all in this
+    process (loopback transport: the slabs run one after another, so the
+    time is an emulation, not a decomposed speed), against the whole
+    instance: the largest relative deviation of the monomer and fluid
+    velocities after `steps` steps (the interpolation is summed slab by slab;
+    everything else is the same kernels on the slabs' parts)."""
+    import torch
+
+    from monomers2026_b200.decomposed import Decomposed, LoopbackTransport
+    from monomers2026_b200.selm import Selm
+
+    whole = Selm(wl.params, wl.x, wl.mass, v=wl.v, topology=wl.topology)
+    whole.initial()
+    whole.run(steps)
+    _, vw, _ = whole.particles()
+    uw = whole.get_field(0)
+    whole.final()
+    dec = Decomposed(wl.params, wl.x, wl.mass, v=wl.v, topology=wl.topology, transport=LoopbackTransport(nranks))
+    dec.initial()
+    dec.step(1)  # untimed: first use of the exchange buffers
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dec.step(steps - 1)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) / (steps - 1) * 1e3
+    _, vd, _ = dec.particles()
+    ud = np.concatenate([a for _, a in sorted(dec.velocity().items())], axis=1)
+    status = dec.status()
+    dec.final()
+
+    def rel(a, b):
+        return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+    return {"slabs": nranks, "steps": steps, "loopback_ms_per_step": round(ms, 3),
+            "v_rel_dev": rel(vd, vw), "u_rel_dev": rel(ud, uw), "status": status,
+            "note": "slabs stepped one after another in one process; the exchanges are device copies"}
 
 
 def outputs_and_analysis(sim, lib, stream, dt, samples=20, frames=10):
