@@ -114,3 +114,27 @@ def test_gloo_ranks_exchange(world, n):
     assert all(ok for _, ok, _ in res)
     total = world * (world + 1) / 2
     assert all(g == [total] * 5 for _, _, g in res)
+
+
+def test_slab_create_refuses_what_it_cannot_decompose():
+    """The argument checks of selm_slab_create come before any device work."""
+    import ctypes as C
+
+    from monomers2026_b200 import _lib
+    from monomers2026_b200.selm import Params
+
+    L = _lib.load()
+    h = C.c_void_p()
+    cases = [
+        (dict(numMeshPtsPerDir=(64, 64, 64), form="fused32"), 2, 2),          # rank outside [0, nranks)
+        (dict(numMeshPtsPerDir=(64, 64, 64), form="fused32"), 0, 0),          # no ranks
+        (dict(numMeshPtsPerDir=(64, 64, 64), form="plain64"), 0, 2),          # the plain form
+        (dict(numMeshPtsPerDir=(64, 64, 64), form="fused32", integrator="quasi_steady"), 0, 2),
+        (dict(numMeshPtsPerDir=(64, 64, 64), form="fused64"), 0, 8),          # 64 planes: not 16 per rank
+        (dict(numMeshPtsPerDir=(30, 30, 30), form="fused32"), 0, 1),          # no whole 16-plane layers
+        (dict(numMeshPtsPerDir=(80, 80, 80), form="fused32"), 0, 1),          # not a compile-time FFT size
+    ]
+    for kw, rank, nranks in cases:
+        p = Params(**kw).to_c()
+        assert L.selm_slab_create(C.byref(p), rank, nranks, C.byref(h)) == 1, (kw, rank, nranks)  # SELM_ERR_INVALID
+        assert L.selm_last_error()
