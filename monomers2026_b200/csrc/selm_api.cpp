@@ -441,7 +441,7 @@ static int set_particles_host(selm_sim* s, int M, const double* x, const double*
 // trip): the positions and velocities go to device staging buffers and are
 // checked there on the copy stream (no host pass over them; a step still
 // running on the simulation's stream is not waited for); the call returns
-// the verdict and leaves the commit into the state queued on the
+// the checks' outcome and leaves the commit into the state queued on the
 // simulation's stream.  The rare upload with positions outside the box is
 // redone by the host path, which remaps them.
 static int set_particles_staged(selm_sim* s, int M, const double* x, const double* v, const double* mass) {
