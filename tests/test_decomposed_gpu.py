@@ -82,3 +82,56 @@ def test_four_slabs_fene_fp32_and_fp64():
 def test_bench_workload_over_eight_slabs_fp32():
     wl = W.config(3, form="fused32", seed=1003)  # 128^3, 1e5 FENE + WCA monomers, kT = 1
     _compare(wl, "fused32", 8, 3, 1e-5)
+
+
+def _nccl_one_rank(port, q):
+    import datetime
+    import os
+
+    import torch
+    import torch.distributed as dist
+
+    from monomers2026_b200.decomposed import TorchTransport
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        wl = W.config(1, kT=1.0, grid=32, nchains=12, length=20)
+        v0 = np.random.default_rng(2).normal(0.0, 0.3, wl.x.shape)
+        p = replace(wl.params, form="fused32")
+        whole = Selm(p, wl.x, wl.mass, v=v0, topology=wl.topology)
+        whole.initial()
+        whole.run(3)
+        dec = Decomposed(p, wl.x, wl.mass, v=v0, topology=wl.topology, transport=TorchTransport())
+        dec.initial()
+        dec.step(3)
+        a, b = _fields(whole, dec)
+        q.put(("ok", [float(np.abs(x - y).max()) for x, y in zip(a, b)], dec.status()))
+        whole.final()
+        dec.final()
+    except Exception as e:  # reported to the test
+        q.put(("error", repr(e), -1))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_nccl_transport_one_rank_is_the_whole_instance():
+    """The torch.distributed transport on NCCL (all_reduce, all_to_all) with
+    one rank, in a child process: bitwise the whole instance."""
+    import socket
+
+    import torch.multiprocessing as mp
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    proc = ctx.Process(target=_nccl_one_rank, args=(port, q))
+    proc.start()
+    kind, errs, status = q.get(timeout=300)
+    proc.join(timeout=60)
+    assert kind == "ok", errs
+    assert errs == [0.0, 0.0, 0.0, 0.0] and status == 0
